@@ -1,0 +1,184 @@
+/*
+ * warpsolve.h -- C ABI of the B200 (sm_100a) warp-field solver.
+ *
+ * Drop-in boundary for StarHub's per-frame non-rigid warp-field solve
+ * (changhaonan/StarHub).  Every entry point takes plain pointers and sizes
+ * (device pointers where noted), returns an int status (WS_OK = 0) and never
+ * aborts the process.  The reference interfaces each entry point replaces are
+ * cited beside it; paths are relative to the reference repository root.
+ *
+ * Threading: a ws_solver is used by one host thread at a time.  All device
+ * work of a solver is issued on the stream passed to ws_solve; nothing in a
+ * solve synchronises the host, so a solve can be captured in a CUDA graph.
+ */
+#ifndef STARHUB_B200_WARPSOLVE_H
+#define STARHUB_B200_WARPSOLVE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define WS_OK 0
+#define WS_ERR_INVALID_ARGUMENT (-1)
+#define WS_ERR_CAPACITY (-2)        /* input exceeds the capacity given at creation */
+#define WS_ERR_CUDA (-3)            /* a CUDA runtime call failed */
+#define WS_ERR_NAN (-4)             /* NaN in the right-hand side (WarpSolverPCG.cu:21-31 exits instead) */
+#define WS_ERR_TIMEOUT (-5)         /* a bounded device-side wait gave up */
+#define WS_ERR_NOT_READY (-6)       /* no inputs set / no solution yet */
+#define WS_ERR_NO_DEVICE (-7)
+
+/* Precision modes. */
+#define WS_PREC_MIXED 0             /* FP32 bulk, FP64 PCG reductions and FP64 6x6 Cholesky inverse */
+#define WS_PREC_FP32 1              /* FP32 everywhere, Gauss-Jordan inverse as the reference */
+
+typedef struct ws_solver ws_solver;
+
+/* Capacities of one solver object (cf. the reference's kMaxNumNodes,
+ * image-sized buffers and kMaxNumNodePairs, examples/mono_star/common/Constants.cpp:14-18). */
+typedef struct ws_config {
+    int max_scenes;             /* scenes per batched solve (1 for the plain path) */
+    int max_total_nodes;        /* sum of node counts over a batch */
+    int max_total_pixels;       /* sum of width*height over a batch */
+    int max_total_edges;        /* sum of node-graph edges over a batch */
+    int max_total_features;     /* sum of feature (keypoint) terms over a batch */
+    int precision;              /* WS_PREC_MIXED or WS_PREC_FP32 */
+    int device;                 /* CUDA device ordinal */
+} ws_config;
+
+/*
+ * One scene's solver inputs.  Replaces SetSolverInputs' seven structs
+ * (examples/mono_star/opt/WarpSolver.h:34-42): Measure4Solver, Render4Solver,
+ * OpticalFlow4Solver, KeyPoint4Solver (libs/star/opt/solver_types.h:21-89),
+ * Geometry4Solver (libs/star/geometry/surfel/SurfelGeometry.h:76-82),
+ * NodeGraph4Solver (libs/star/geometry/node_graph/NodeGraph.h:89-99),
+ * NodeFlow4Solver, the camera extrinsic, and the PenaltyConstants
+ * (examples/mono_star/opt/PenaltyConstants.cu:8-33).  Image maps are
+ * pitch-linear device arrays instead of texture objects; the C++ facade in
+ * include/starhub_b200/warp_solver.hpp converts texture objects.
+ * Every pointer is a device pointer and must stay valid until the solve ends.
+ */
+typedef struct ws_inputs {
+    int width, height;          /* image size */
+    int pitch;                  /* row pitch in texels (0 = width) */
+    float fx, fy, cx, cy;       /* pinhole intrinsics of the (downsampled) image */
+    float cam2world[16];        /* row-major 4x4 rigid transform */
+    const void *measure_vertex_confid;   /* float4 per texel, camera frame */
+    const void *measure_normal_radius;   /* float4 per texel, camera frame */
+    const void *reference_vertex;        /* float4 per texel, world frame */
+    const void *reference_normal;        /* float4 per texel, world frame */
+    const uint32_t *index_map;           /* surfel id per texel, 0xFFFFFFFF = none */
+    const void *opticalflow;             /* float2 per texel in pixels, NULL = zero flow */
+    int num_surfels;
+    const uint16_t *surfel_knn;          /* 4 node ids per surfel */
+    const float *surfel_knn_spatial_weight;  /* 4 per surfel */
+    const float *surfel_knn_connect_weight;  /* 4 per surfel */
+    int num_nodes;                       /* <= 65535, includes the two anchor nodes */
+    const float *reference_node_coords;  /* float4 per node */
+    int num_edges;
+    const uint16_t *node_graph;          /* (i, j, k) per edge, j = k-th neighbour of i */
+    int graph_k;                         /* neighbours per node (stride of the connect weights) */
+    const float *node_knn_connect_weight;/* graph_k per node */
+    float node_radius_square;
+    const float *node_motion_pred;       /* float4 per node, NULL = none */
+    int num_features;
+    const uint16_t *feature_knn;         /* 4 node ids per feature term, NULL if none */
+    float lambda_depth, lambda_optical_flow, lambda_reg, lambda_node_translation, lambda_feature;
+    const float *init_node_se3;          /* 8 floats per node (q0.xyzw, q1.xyzw), NULL = identity */
+} ws_inputs;
+
+/* Reference defaults for the penalty weights (PenaltyConstants.cu:8-33). */
+void ws_default_penalties(ws_inputs *in);
+
+/* WarpSolver::WarpSolver / AllocateBuffer (examples/mono_star/opt/WarpSolver.cu:50-103). */
+int ws_create(const ws_config *config, ws_solver **out);
+/* WarpSolver::~WarpSolver (WarpSolver.cu:75-80). */
+int ws_destroy(ws_solver *solver);
+
+/* WarpSolver::SetSolverInputs (WarpSolver.cu:125-155): one scene. */
+int ws_set_inputs(ws_solver *solver, const ws_inputs *inputs);
+/* Batched form: num_scenes independent scenes solved together (no reference counterpart;
+ * each scene's result equals the single-scene result bit for bit). */
+int ws_set_batch(ws_solver *solver, const ws_inputs *scenes, int num_scenes);
+
+/* WarpSolver::SolveStreamed (WarpSolver.cu:260-279) with the Gauss-Newton and PCG
+ * iteration counts as parameters (reference: 6 and 10, Constants.cpp:33, WarpSolver.cu:303).
+ * Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
+int ws_solve(ws_solver *solver, int gn_iters, int pcg_iters, void *stream);
+/* Same solve launched through a CUDA graph that is captured on first use and replayed. */
+int ws_solve_graph(ws_solver *solver, int gn_iters, int pcg_iters, void *stream);
+
+/* Synchronises the solver's last stream and reports device-side errors
+ * (timeouts, NaN right-hand side, capacity overflow found on the device). */
+int ws_sync_status(ws_solver *solver);
+
+/* WarpSolver::SolvedNodeSE3 / OptimizationProcessorWarpSolver::SolvedSE3
+ * (WarpSolver.h:45, OptimizationProcessorWarpSolver.h:28-30): device pointer to
+ * 8 floats per node of `scene`, valid until the next ws_set_* on this solver. */
+int ws_get_solution(ws_solver *solver, int scene, const float **dev_node_se3, int *num_nodes);
+
+/* Counts of the last index build (host copies; synchronises). */
+int ws_get_counts(ws_solver *solver, int scene, int *num_dense_terms, int *num_half_pairs, int *num_n2t_kv);
+
+/* Copies of the index structures of one scene to host memory (synchronise), for parity tests.
+ * ImageTermKNNFetcher::GetImageTermPixelAndKNN (ImageTermKNNFetcher.h:55-83). */
+int ws_get_dense_terms(ws_solver *solver, int scene, uint16_t *pixels, uint16_t *knn,
+                       float *spatial_w, float *connect_w, int capacity, int *count);
+/* Node2TermsIndex::GetNode2TermMap (examples/mono_star/opt/Node2TermsIndex.h:79-94). */
+int ws_get_node2term(ws_solver *solver, int scene, uint32_t *offsets, uint32_t *term_index,
+                     int capacity, int *count);
+/* NodePair2TermsIndex::GetNodePair2TermMap (NodePair2TermsIndex.h:44-55): unique (i<j) pairs,
+ * their term ranges into term_index, and the sorted pair->term list. */
+int ws_get_node_pairs(ws_solver *solver, int scene, uint32_t *rows, uint32_t *cols,
+                      uint32_t *begin, uint32_t *end, int capacity, int *count,
+                      uint32_t *term_index, int term_capacity, int *term_count);
+/* The assembled block system of the last Gauss-Newton iteration: block-CSR with the
+ * diagonal block first in every row; A[6*row+r][6*col+c] = blocks[36*k + 6*r + c].
+ * JtJMaterializer::AssembleBinBlockCSR (JtJMaterializerBinBlockCSR.cu:44-75). */
+int ws_get_system(ws_solver *solver, int scene, uint32_t *rowptr, uint32_t *cols, float *blocks,
+                  int block_capacity, int *num_blocks, float *inv_diag, float *jtr, float *step);
+/* Dense term residuals (3 per term) and gradients (18 per term) of the last iteration
+ * (DenseImageHandler::Term2JacobianMap, DenseImageHandler.cu:384-398). */
+int ws_get_dense_jacobian(ws_solver *solver, int scene, float *residual, float *gradient,
+                          int capacity, int *count);
+
+/* ---- Node graph, skinning and warp (bit-exact to the reference's integer outputs) ---- */
+
+/* NodeGraph::InitializeNodeGraphFromVertex (libs/star/geometry/node_graph/NodeGraph.cu:460-498):
+ * voxel subsample on the GPU (VoxelSubsamplerSorting.cu:8-96), greedy host dedup
+ * (NodeGraph.cu:652-704), two anchor nodes prepended.  `surfels` is a device float4 array;
+ * `nodes_host` receives float4 nodes.  Synchronises `stream`. */
+int ws_init_nodes(const float *surfels, int num_surfels, float node_radius, float *nodes_host,
+                  int capacity, int *num_nodes, void *stream);
+/* UpdateNodeDistanceKernel + BuildNodeGraphKernel + BuildNodeGraphPairKernel
+ * (NodeGraph.cu:10-118): device in/out; k = 4 or 8; edges gets (i, knn[i][k], k). */
+int ws_build_node_graph(const float *nodes, int num_nodes, int k, float node_radius,
+                        uint16_t *knn, float *spatial_w, uint16_t *edges, void *stream);
+/* SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94): device in/out. */
+int ws_skinning(const float *nodes, int num_nodes, const float *verts, int num_verts,
+                float node_radius, uint16_t *knn, float *spatial_w, float *connect_w, void *stream);
+/* ForwardWarpVertexAndNodeKernel (libs/star/geometry/surfel/SurfelNodeDeformer.cu:13-79):
+ * warps float4 vertices (and optional normals) by the normalized-DQ blend of `num_nodes` node DQs. */
+int ws_forward_warp(const float *node_se3, int num_nodes, const float *verts, const float *normals, int num_verts,
+                    const uint16_t *knn, const float *spatial_w, const float *connect_w,
+                    float *out_verts, float *out_normals, void *stream);
+/* Solver-map producer: z-buffered point splat of surfels into index / vertex / normal maps
+ * (replaces the OpenGL solver maps, RendererDraw.cu:167-230 with shaders/solver_map.vert:21-53;
+ * index = surfel id, vertex/normal copied from `attr_verts`/`attr_normals`).  `verts` are
+ * positions in the camera frame used for projection.  `footprint` is the splat half-width in
+ * pixels.  Writes width*height texels of every output; empty texels get index 0xFFFFFFFF and
+ * zero vectors. */
+int ws_splat_maps(const float *verts, const float *attr_verts, const float *attr_normals,
+                  int num_verts, int width, int height, float fx, float fy, float cx, float cy,
+                  int footprint, uint32_t *index_map, float *vertex_map, float *normal_map,
+                  void *stream);
+
+/* Library version / build identification. */
+int ws_version(void);
+const char *ws_error_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,446 @@
+// Index build of the B200 warp-field solver: pixel-term compaction,
+// node->term and node-pair->term maps, and the block-CSR sparsity pattern.
+//
+// All scenes of a batch are processed by the same launches; per-scene counts
+// live in device memory (Plan), so nothing here waits on the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ws_common.cuh"
+#include "ws_prims.cuh"
+#include "ws_workspace.h"
+
+namespace ws {
+
+constexpr int kPixTileThreads = 256;
+constexpr int kPixPerThread = 4;
+constexpr int kPixTile = kPixTileThreads * kPixPerThread;   // 1024 pixels per tile
+
+__device__ __forceinline__ void set_error(int *flag, int code) { atomicCAS(flag, 0, code); }
+
+// markPotentialValidImageTermPixelKernel (examples/mono_star/opt/ImageTermKNNFetcher.cu:9-29):
+// a pixel is a potential term iff its index map holds a surfel id.
+// A pixel counts only when its surfel id is in range (out-of-range ids are treated as empty,
+// which keeps every later gather inside the caller's arrays).
+__device__ __forceinline__ bool valid_surfel(uint32_t id, const Scene &sc) {
+    return id != kInvalidIndex && id < (uint32_t)sc.num_surfels;
+}
+
+__global__ void k_pixel_count(const Scene *scenes, const uint32_t *tile_scene, int num_tiles, uint32_t *tile_count) {
+    __shared__ uint32_t sm[32];
+    const int t = blockIdx.x;
+    if (t >= num_tiles) return;
+    const Scene &sc = scenes[tile_scene[t]];
+    const uint32_t npix = (uint32_t)sc.width * (uint32_t)sc.height;
+    const uint32_t p0 = (uint32_t)(t - sc.tile_base) * kPixTile + threadIdx.x * kPixPerThread;
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < kPixPerThread; ++i) {
+        const uint32_t p = p0 + i;
+        if (p < npix) {
+            const uint32_t y = p / (uint32_t)sc.width, x = p - y * (uint32_t)sc.width;
+            c += valid_surfel(sc.index_map[(size_t)y * sc.pitch + x], sc) ? 1u : 0u;
+        }
+    }
+    uint32_t total;
+    block_excl_scan_u32(c, &total, sm);
+    if (threadIdx.x == 0) tile_count[t] = total;
+}
+
+// compactPontentialImageTermPixelsKernel (ImageTermKNNFetcher.cu:56-88) fused with
+// queryPixelKNNKernel (WarpSolver.cu:7-47): raster-order compaction of
+// (x, y, x + flow_x, y + flow_y) and the surfel's 4-NN and weights.
+__global__ void k_pixel_compact(const Scene *scenes, const uint32_t *tile_scene, int num_tiles,
+                                const uint32_t *tile_offset, ushort4 *pixels, ushort4 *knn,
+                                float4 *sw, float4 *cw, uint32_t *term_scene, uint32_t cap, int *err) {
+    __shared__ uint32_t sm[32];
+    const int t = blockIdx.x;
+    if (t >= num_tiles) return;
+    const uint32_t s = tile_scene[t];
+    const Scene &sc = scenes[s];
+    const uint32_t npix = (uint32_t)sc.width * (uint32_t)sc.height;
+    const uint32_t p0 = (uint32_t)(t - sc.tile_base) * kPixTile + threadIdx.x * kPixPerThread;
+    uint32_t ids[kPixPerThread];
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < kPixPerThread; ++i) {
+        const uint32_t p = p0 + i;
+        ids[i] = kInvalidIndex;
+        if (p < npix) {
+            const uint32_t y = p / (uint32_t)sc.width, x = p - y * (uint32_t)sc.width;
+            ids[i] = sc.index_map[(size_t)y * sc.pitch + x];
+            if (!valid_surfel(ids[i], sc)) ids[i] = kInvalidIndex;
+            c += (ids[i] != kInvalidIndex) ? 1u : 0u;
+        }
+    }
+    uint32_t pos = tile_offset[t] + block_excl_scan_u32(c, nullptr, sm);
+#pragma unroll
+    for (int i = 0; i < kPixPerThread; ++i) {
+        if (ids[i] == kInvalidIndex) continue;
+        const uint32_t p = p0 + i;
+        const uint32_t y = p / (uint32_t)sc.width, x = p - y * (uint32_t)sc.width;
+        float2 fl = make_float2(0.f, 0.f);
+        if (sc.flow) fl = sc.flow[(size_t)y * sc.pitch + x];
+        const unsigned tx = __float2uint_rn(fl.x + float(x));
+        const unsigned ty = __float2uint_rn(fl.y + float(y));
+        if (pos < cap) {
+            pixels[pos] = make_ushort4((unsigned short)x, (unsigned short)y, (unsigned short)tx, (unsigned short)ty);
+            ushort4 k4 = sc.surfel_knn[ids[i]];
+            const unsigned nn = (unsigned)sc.num_nodes;
+            if (k4.x >= nn || k4.y >= nn || k4.z >= nn || k4.w >= nn) {   // node id out of range
+                set_error(err, WS_ERR_INVALID_ARGUMENT);
+                k4 = make_ushort4(0, 0, 0, 0);
+            }
+            knn[pos] = k4;
+            sw[pos] = sc.surfel_sw[ids[i]];
+            cw[pos] = sc.surfel_cw[ids[i]];
+            term_scene[pos] = s;
+        }
+        ++pos;
+    }
+}
+
+// Per-scene counts and key/value ranges (term_offset_types.h:62-82 size2offset),
+// computed after the compaction scan.
+__global__ void k_plan(const Scene *scenes, int num_scenes, const uint32_t *tile_offset, int total_tiles,
+                       Plan *plan, uint32_t *counts, uint32_t cap_n2t, uint32_t cap_pair, int *err) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t n2t = 0, pair = 0;
+    for (int s = 0; s < num_scenes; ++s) {
+        const Scene &sc = scenes[s];
+        Plan p;
+        p.dense_begin = tile_offset[sc.tile_base];
+        p.dense_count = tile_offset[sc.tile_base + sc.num_tiles] - p.dense_begin;
+        p.n2t_base = n2t;
+        p.n2t_count = 4u * p.dense_count + 2u * sc.num_edges + sc.num_nodes + 4u * sc.num_features;
+        p.pair_base = pair;
+        p.pair_count = 6u * p.dense_count + sc.num_edges + 6u * sc.num_features;
+        p.pad[0] = p.pad[1] = 0;
+        n2t += p.n2t_count;
+        pair += p.pair_count;
+        plan[s] = p;
+    }
+    if (n2t > cap_n2t || pair > cap_pair) {
+        set_error(err, WS_ERR_CAPACITY);
+        n2t = min(n2t, cap_n2t);
+        pair = min(pair, cap_pair);
+    }
+    counts[kCntDense] = tile_offset[total_tiles];
+    counts[kCntN2T] = n2t;
+    counts[kCntPairKV] = pair;
+}
+
+// Node-graph edge endpoints clamped into the scene (an out-of-range id flags WS_ERR_INVALID_ARGUMENT).
+__device__ __forceinline__ void edge_ends(const Scene &sc, uint32_t e, uint16_t &x, uint16_t &y, int *err) {
+    x = sc.edges[3 * e];
+    y = sc.edges[3 * e + 1];
+    const uint16_t last = (uint16_t)(sc.num_nodes - 1);
+    if (x > last || y > last) {
+        set_error(err, WS_ERR_INVALID_ARGUMENT);
+        x = min(x, last);
+        y = min(y, last);
+    }
+}
+
+__device__ __forceinline__ ushort4 clamp_knn(ushort4 k, const Scene &sc, int *err) {
+    const uint16_t last = (uint16_t)(sc.num_nodes - 1);
+    if (k.x > last || k.y > last || k.z > last || k.w > last) {
+        set_error(err, WS_ERR_INVALID_ARGUMENT);
+        k = make_ushort4(min(k.x, last), min(k.y, last), min(k.z, last), min(k.w, last));
+    }
+    return k;
+}
+
+__device__ __forceinline__ int find_scene_n2t(const Plan *plan, int num_scenes, uint32_t i) {
+    int lo = 0, hi = num_scenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (plan[mid].n2t_base <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int find_scene_pair(const Plan *plan, int num_scenes, uint32_t i) {
+    int lo = 0, hi = num_scenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (plan[mid].pair_base <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// buildTermKeyValueKernel (examples/mono_star/opt/Node2TermsIndex.cu:6-76): keys are global
+// node ids, values are the scene-local term ids of the reference's term space
+// [dense | reg | node-motion | feature]; self edges get the invalid key.
+__global__ void k_n2t_kv(const Scene *scenes, const Plan *plan, int num_scenes, const uint32_t *counts,
+                         const ushort4 *dense_knn, uint32_t *keys, uint32_t *vals, uint32_t invalid_key, int *err) {
+    const uint32_t n = counts[kCntN2T];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int s = find_scene_n2t(plan, num_scenes, i);
+        const Scene &sc = scenes[s];
+        const Plan &p = plan[s];
+        uint32_t j = i - p.n2t_base;
+        const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
+        uint32_t key, val;
+        if (j < 4u * nd) {
+            const uint32_t t = j >> 2;
+            const ushort4 k4 = dense_knn[p.dense_begin + t];
+            const uint32_t slot = j & 3u;
+            const uint16_t id = slot == 0 ? k4.x : slot == 1 ? k4.y : slot == 2 ? k4.z : k4.w;
+            key = sc.node_base + id;
+            val = t;
+        } else if ((j -= 4u * nd) < 2u * ne) {
+            const uint32_t e = j >> 1;
+            uint16_t x, y;
+            edge_ends(sc, e, x, y, err);
+            key = (x != y) ? sc.node_base + ((j & 1u) ? y : x) : invalid_key;
+            val = nd + e;
+        } else if ((j -= 2u * ne) < nn) {
+            key = sc.node_base + j;
+            val = nd + ne + j;
+        } else {
+            j -= nn;
+            const uint32_t f = j >> 2;
+            const ushort4 k4 = clamp_knn(sc.feature_knn[f], sc, err);
+            const uint32_t slot = j & 3u;
+            const uint16_t id = slot == 0 ? k4.x : slot == 1 ? k4.y : slot == 2 ? k4.z : k4.w;
+            key = sc.node_base + id;
+            val = nd + ne + nn + f;
+        }
+        keys[i] = key;
+        vals[i] = val;
+    }
+}
+
+// computeTermOffsetKernel (Node2TermsIndex.cu:78-121) as a lower bound per node.
+__global__ void k_n2t_offsets(const uint32_t *sorted_keys, const uint32_t *counts, uint32_t total_nodes,
+                              uint32_t *offsets) {
+    const uint32_t n = counts[kCntN2T];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g <= total_nodes; g += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sorted_keys[mid] < g) lo = mid + 1; else hi = mid;
+        }
+        offsets[g] = lo;
+    }
+}
+
+// computeKVNodePairKNN / buildKeyValuePairKernel (NodePair2TermsIndex.cu:11-92): 6 (i<j) pairs per
+// dense term in i-major order, one per non-self reg edge, feature terms like dense terms.
+__device__ __forceinline__ unsigned long long knn_pair_key(const ushort4 k4, uint32_t q, uint32_t base, int bits,
+                                                            unsigned long long invalid) {
+    const uint16_t a[4] = {k4.x, k4.y, k4.z, k4.w};
+    uint32_t off = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (a[i] < a[j]) {
+                if (off == q) return ((unsigned long long)(base + a[i]) << bits) | (unsigned long long)(base + a[j]);
+                ++off;
+            }
+    return invalid;
+}
+
+__global__ void k_pair_kv(const Scene *scenes, const Plan *plan, int num_scenes, const uint32_t *counts,
+                          const ushort4 *dense_knn, unsigned long long *keys, uint32_t *vals, int bits,
+                          unsigned long long invalid, int *err) {
+    const uint32_t n = counts[kCntPairKV];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int s = find_scene_pair(plan, num_scenes, i);
+        const Scene &sc = scenes[s];
+        const Plan &p = plan[s];
+        uint32_t j = i - p.pair_base;
+        const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
+        unsigned long long key;
+        uint32_t val;
+        if (j < 6u * nd) {
+            const uint32_t t = j / 6u;
+            key = knn_pair_key(dense_knn[p.dense_begin + t], j - 6u * t, sc.node_base, bits, invalid);
+            val = t;
+        } else if ((j -= 6u * nd) < ne) {
+            uint16_t x, y;
+            edge_ends(sc, j, x, y, err);
+            const uint32_t lo = min(x, y), hi = max(x, y);
+            key = (x != y) ? (((unsigned long long)(sc.node_base + lo) << bits) | (unsigned long long)(sc.node_base + hi))
+                           : invalid;
+            val = nd + j;
+        } else {
+            j -= ne;
+            const uint32_t f = j / 6u;
+            key = knn_pair_key(clamp_knn(sc.feature_knn[f], sc, err), j - 6u * f, sc.node_base, bits, invalid);
+            val = nd + ne + nn + f;
+        }
+        keys[i] = key;
+        vals[i] = val;
+    }
+}
+
+// segmentNodePairKernel (NodePair2TermsIndex.cu:94-128): 1 at the first key of every unique pair;
+// also records the number of valid (non-invalid) keys.
+__global__ void k_pair_marks(const unsigned long long *keys, const uint32_t *counts, uint32_t *marks,
+                             unsigned long long invalid, uint32_t *counts_out) {
+    const uint32_t n = counts[kCntPairKV];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[i];
+        const bool valid = k != invalid;
+        marks[i] = (valid && (i == 0 || keys[i - 1] != k)) ? 1u : 0u;
+        if (valid && (i + 1 == n || keys[i + 1] == invalid)) counts_out[kCntPairValid] = i + 1;
+        if (i == 0 && !valid) counts_out[kCntPairValid] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n == 0) counts_out[kCntPairValid] = 0;
+}
+
+// compactNodePairKeyKernel (NodePair2TermsIndex.cu:130-169): unique pairs and their term ranges.
+__global__ void k_half_fill(const unsigned long long *keys, const uint32_t *head_off,
+                            uint32_t *counts, int bits, uint32_t cap_half, uint32_t *half_row, uint32_t *half_col,
+                            uint32_t *half_begin, uint32_t *half_end, uint32_t *row_cnt_up, uint32_t *row_cnt_lo,
+                            int *err) {
+    const uint32_t n = counts[kCntPairKV];
+    const uint32_t nhalf = head_off[n];
+    const uint32_t nvalid = counts[kCntPairValid];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[kCntHalf] = min(nhalf, cap_half);
+        if (nhalf > cap_half) set_error(err, WS_ERR_CAPACITY);
+    }
+    const unsigned long long mask = (1ull << bits) - 1ull;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t h = head_off[i];
+        if (head_off[i + 1] == h) continue;        // not the first key of a unique pair
+        if (h >= cap_half) continue;
+        const unsigned long long k = keys[i];
+        const uint32_t row = (uint32_t)(k >> bits), col = (uint32_t)(k & mask);
+        half_row[h] = row;
+        half_col[h] = col;
+        half_begin[h] = i;
+        if (h > 0 && h - 1 < cap_half) half_end[h - 1] = i;
+        if (h + 1 == nhalf) half_end[h] = nvalid;
+        atomicAdd(&row_cnt_up[row], 1u);
+        atomicAdd(&row_cnt_lo[col], 1u);
+    }
+}
+
+__global__ void k_row_first(const uint32_t *half_row, const uint32_t *counts, uint32_t *row_first) {
+    const uint32_t n = counts[kCntHalf];
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x)
+        if (h == 0 || half_row[h - 1] != half_row[h]) row_first[half_row[h]] = h;
+}
+
+__global__ void k_row_len(const uint32_t *up, const uint32_t *lo, uint32_t total_nodes, uint32_t *len) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x)
+        len[g] = 1u + up[g] + lo[g];
+}
+
+__global__ void k_col_kv(const uint32_t *half_col, const uint32_t *counts, uint32_t *keys, uint32_t *vals) {
+    const uint32_t n = counts[kCntHalf];
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
+        keys[h] = half_col[h];
+        vals[h] = h;
+    }
+}
+
+// Block-CSR slots: every row is [diagonal, columns < row ascending, columns > row ascending],
+// which is the sorted symmetric pair order of computeSymmetricNodePairKernel + sort
+// (NodePair2TermsIndex.cu:171-192, 656-675) with the diagonal block placed first as in the
+// Bin-Blocked CSR (NodePairRowColumnIndex.cu:110-124).
+__global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, const uint32_t *counts,
+                        const uint32_t *half_row, const uint32_t *half_col, const uint32_t *row_first,
+                        const uint32_t *row_cnt_lo, const uint32_t *rowptr, uint32_t cap_blocks,
+                        uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx, int *err) {
+    const uint32_t n = counts[kCntHalf];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t col = sorted_col[k];
+        uint32_t lo = 0, hi = k;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sorted_col[mid] < col) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t rank_lo = k - lo;
+        const uint32_t h = sorted_h[k];
+        const uint32_t row = half_row[h];
+        const uint32_t s_lo = rowptr[col] + 1u + rank_lo;
+        const uint32_t s_up = rowptr[row] + 1u + row_cnt_lo[row] + (h - row_first[row]);
+        if (s_lo >= cap_blocks || s_up >= cap_blocks) {
+            set_error(err, WS_ERR_CAPACITY);
+            slot_lo[h] = slot_up[h] = kInvalidIndex;
+            continue;
+        }
+        slot_lo[h] = s_lo;
+        slot_up[h] = s_up;
+        colidx[s_lo] = row;
+        colidx[s_up] = half_col[h];
+    }
+}
+
+__global__ void k_diag_cols(const uint32_t *rowptr, uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx,
+                            int *err) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
+        const uint32_t s = rowptr[g];
+        if (s < cap_blocks) colidx[s] = g;
+        if (g + 1 == total_nodes && rowptr[total_nodes] > cap_blocks) set_error(err, WS_ERR_CAPACITY);
+    }
+}
+
+static inline int grid_for(uint32_t n, int threads, int num_sms) {
+    const uint32_t want = (n + threads - 1) / threads;
+    const uint32_t cap = (uint32_t)num_sms * 8u;
+    return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, cap));
+}
+
+void index_build(Workspace &w, cudaStream_t st) {
+    const int S = w.num_scenes;
+    const int T = (int)w.total_tiles;
+    const uint32_t N = w.total_nodes;
+    // 1. compaction of potential pixels
+    k_pixel_count<<<T, kPixTileThreads, 0, st>>>(w.scenes, w.tile_scene, T, w.tile_count);
+    exclusive_scan(w.tile_count, w.tile_count, nullptr, (uint32_t)T, w.cap_tiles, w.scan_tmp, st);
+    k_plan<<<1, 32, 0, st>>>(w.scenes, S, w.tile_count, T, w.plan, w.counts, w.cap_n2t, w.cap_pair_kv, w.error_flag);
+    k_pixel_compact<<<T, kPixTileThreads, 0, st>>>(w.scenes, w.tile_scene, T, w.tile_count, w.d_pixels, w.d_knn,
+                                                   w.d_sw, w.d_cw, w.d_scene, w.cap_pixels, w.error_flag);
+    // 2. node -> term
+    const uint32_t n2t_invalid = (1u << w.node_bits) - 1u;
+    k_n2t_kv<<<grid_for(w.cap_n2t, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, S, w.counts, w.d_knn, w.n2t_key,
+                                                                    w.n2t_val, n2t_invalid, w.error_flag);
+    const bool n2t_alt = radix_sort<uint32_t>(w.n2t_key, w.n2t_val, w.n2t_key_alt, w.n2t_val_alt, w.counts + kCntN2T, 0,
+                                              w.cap_n2t, w.node_bits, w.sort_hist, w.sort_digit, st);
+    w.n2t_sorted_key = n2t_alt ? w.n2t_key_alt : w.n2t_key;
+    w.n2t_sorted_val = n2t_alt ? w.n2t_val_alt : w.n2t_val;
+    k_n2t_offsets<<<grid_for(N + 1, 256, w.num_sms), 256, 0, st>>>(w.n2t_sorted_key, w.counts, N, w.n2t_offset);
+    // 3. node pair -> term
+    const int pbits = 2 * w.node_bits;
+    const unsigned long long pinvalid = (pbits >= 64) ? ~0ull : ((1ull << pbits) - 1ull);
+    k_pair_kv<<<grid_for(w.cap_pair_kv, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, S, w.counts, w.d_knn,
+                                                                         w.pair_key, w.pair_val, w.node_bits, pinvalid,
+                                                                         w.error_flag);
+    const bool pair_alt = radix_sort<unsigned long long>(w.pair_key, w.pair_val, w.pair_key_alt, w.pair_val_alt,
+                                                         w.counts + kCntPairKV, 0, w.cap_pair_kv, pbits, w.sort_hist,
+                                                         w.sort_digit, st);
+    w.pair_sorted_key = pair_alt ? w.pair_key_alt : w.pair_key;
+    w.pair_sorted_val = pair_alt ? w.pair_val_alt : w.pair_val;
+    const int pg = grid_for(w.cap_pair_kv, 256, w.num_sms);
+    k_pair_marks<<<pg, 256, 0, st>>>(w.pair_sorted_key, w.counts, w.pair_head, pinvalid, w.counts);
+    exclusive_scan(w.pair_head, w.pair_head, w.counts + kCntPairKV, 0, w.cap_pair_kv, w.scan_tmp, st);
+    // pair_head now holds exclusive offsets; a unique pair starts where two consecutive offsets differ
+    cudaMemsetAsync(w.row_cnt_up, 0, sizeof(uint32_t) * w.cap_nodes, st);
+    cudaMemsetAsync(w.row_cnt_lo, 0, sizeof(uint32_t) * w.cap_nodes, st);
+    k_half_fill<<<pg, 256, 0, st>>>(w.pair_sorted_key, w.pair_head, w.counts, w.node_bits, w.cap_half,
+                                    w.half_row, w.half_col, w.half_begin, w.half_end, w.row_cnt_up, w.row_cnt_lo,
+                                    w.error_flag);
+    // 4. block CSR
+    k_row_first<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_row, w.counts, w.row_first);
+    k_row_len<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.row_cnt_up, w.row_cnt_lo, N, w.rowptr);
+    exclusive_scan(w.rowptr, w.rowptr, nullptr, N, w.cap_nodes, w.scan_tmp, st);
+    k_col_kv<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_col, w.counts, w.col_key, w.col_val);
+    const bool col_alt = radix_sort<uint32_t>(w.col_key, w.col_val, w.col_key_alt, w.col_val_alt, w.counts + kCntHalf,
+                                              0, w.cap_half, w.node_bits, w.sort_hist, w.sort_digit, st);
+    const uint32_t *scol = col_alt ? w.col_key_alt : w.col_key;
+    const uint32_t *sh = col_alt ? w.col_val_alt : w.col_val;
+    k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,
+                                                                    w.row_first, w.row_cnt_lo, w.rowptr, w.cap_blocks,
+                                                                    w.half_slot_up, w.half_slot_lo, w.colidx,
+                                                                    w.error_flag);
+    k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, N, w.cap_blocks, w.colidx, w.error_flag);
+}
+
+}  // namespace ws

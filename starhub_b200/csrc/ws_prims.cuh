@@ -1,0 +1,245 @@
+// Deterministic scan and stable LSD radix sort with device-resident counts.
+//
+// Every launch is sized from a host-known capacity and reads the live element
+// count from device memory, so the index build needs no host synchronisation
+// and can be captured in a CUDA graph.  The sort is stable (equal keys keep
+// their input order), which is what the reference's cub::DeviceRadixSort
+// calls rely on (libs/star/common/algorithm_types.cuh:37-83).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ws {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;   // 4096 keys per tile
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;    // 2048 elements per tile
+
+__device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024, multiple of 32).
+__device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t *total, uint32_t *smem32) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t inc = warp_incl_scan_u32(v);
+    __syncthreads();
+    if (lane == 31) smem32[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? smem32[lane] : 0u;
+        w = warp_incl_scan_u32(w);
+        if (lane < nw) smem32[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t warp_off = warp > 0 ? smem32[warp - 1] : 0u;
+    if (total) *total = smem32[nw - 1];
+    return warp_off + inc - v;
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan: out[i] = sum_{j<i} in[i]; out[n] = total.  n read from n_dev
+// (or n_static when n_dev is null).  Three launches: tile sums, scan of tile
+// sums (one block), tile scans.
+// ---------------------------------------------------------------------------
+static __global__ void k_scan_tile_sums(const uint32_t *in, const uint32_t *n_dev, uint32_t n_static, uint32_t *tile_sums) {
+    __shared__ uint32_t sm[32];
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    const uint32_t base = blockIdx.x * kScanTile;
+    uint32_t s = 0;
+    if (base < n) {
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            const uint32_t idx = base + threadIdx.x * kScanItems + i;
+            if (idx < n) s += in[idx];
+        }
+    }
+    uint32_t total;
+    block_excl_scan_u32(s, &total, sm);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+static __global__ void k_scan_tile_offsets(uint32_t *tile_sums, int num_tiles) {
+    __shared__ uint32_t sm[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < num_tiles; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < num_tiles ? tile_sums[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_excl_scan_u32(v, &total, sm);
+        if (i < num_tiles) tile_sums[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tile_sums[num_tiles] = carry;
+}
+
+static __global__ void k_scan_apply(const uint32_t *in, const uint32_t *n_dev, uint32_t n_static,
+                             const uint32_t *tile_offsets, int num_tiles, uint32_t *out) {
+    __shared__ uint32_t sm[32];
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    const uint32_t base = blockIdx.x * kScanTile;
+    if (base > n) return;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        const uint32_t idx = base + threadIdx.x * kScanItems + i;
+        v[i] = idx < n ? in[idx] : 0u;
+        s += v[i];
+    }
+    uint32_t ex = block_excl_scan_u32(s, nullptr, sm) + tile_offsets[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        const uint32_t idx = base + threadIdx.x * kScanItems + i;
+        if (idx < n) out[idx] = ex;
+        ex += v[i];
+    }
+    if (base <= n && n < base + kScanTile && threadIdx.x == 0) out[n] = tile_offsets[num_tiles];
+}
+
+// Host driver.  `in` and `out` may alias.  tile_sums needs cap/2048 + 2 entries.
+inline void exclusive_scan(const uint32_t *in, uint32_t *out, const uint32_t *n_dev, uint32_t n_static,
+                           uint32_t cap, uint32_t *tile_sums, cudaStream_t st) {
+    const int tiles = (int)((cap + kScanTile) / kScanTile);
+    k_scan_tile_sums<<<tiles, kScanThreads, 0, st>>>(in, n_dev, n_static, tile_sums);
+    k_scan_tile_offsets<<<1, 1024, 0, st>>>(tile_sums, tiles);
+    k_scan_apply<<<tiles, kScanThreads, 0, st>>>(in, n_dev, n_static, tile_sums, tiles, out);
+}
+
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort of (key, u32 value), 8 bits per pass.
+// hist layout: hist[digit * max_tiles + tile].
+// ---------------------------------------------------------------------------
+template <class K>
+__global__ void k_radix_upsweep(const K *keys, const uint32_t *n_dev, uint32_t n_static, int shift,
+                                uint32_t *hist, int max_tiles) {
+    __shared__ uint32_t h[256];
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * (uint32_t)kSortTile;
+    if (base < n) {
+#pragma unroll 4
+        for (int r = 0; r < kSortRounds; ++r) {
+            const uint32_t idx = base + r * kSortThreads + threadIdx.x;
+            if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 255u], 1u);
+        }
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * max_tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+static __global__ void k_radix_scan(uint32_t *hist, int max_tiles, uint32_t *digit_total) {
+    __shared__ uint32_t sm[32];
+    uint32_t *row = hist + (size_t)blockIdx.x * max_tiles;
+    const int per = (max_tiles + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per;
+    const int e = min(b + per, max_tiles);
+    uint32_t local = 0;
+    for (int i = b; i < e; ++i) local += row[i];
+    uint32_t total;
+    uint32_t run = block_excl_scan_u32(local, &total, sm);
+    for (int i = b; i < e; ++i) {
+        const uint32_t v = row[i];
+        row[i] = run;
+        run += v;
+    }
+    if (threadIdx.x == 0) digit_total[blockIdx.x] = total;
+}
+
+template <class K>
+__global__ void __launch_bounds__(kSortThreads)
+k_radix_scatter(const K *keys_in, const uint32_t *vals_in, K *keys_out, uint32_t *vals_out,
+                const uint32_t *n_dev, uint32_t n_static, int shift,
+                const uint32_t *hist, int max_tiles, const uint32_t *digit_total) {
+    __shared__ uint32_t digit_base[256];
+    __shared__ uint32_t run[256];
+    __shared__ uint16_t wcount[kSortThreads / 32][256];
+    __shared__ uint32_t sm[32];
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    const uint32_t base = blockIdx.x * (uint32_t)kSortTile;
+    if (base >= n) return;                      // uniform for the whole block
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t ex = block_excl_scan_u32(digit_total[t], nullptr, sm);
+    digit_base[t] = ex + hist[(size_t)t * max_tiles + blockIdx.x];
+    run[t] = 0;
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint32_t idx = base + r * kSortThreads + t;
+        const bool valid = idx < n;
+        K key = 0;
+        uint32_t val = 0;
+        uint32_t d = 256u;
+        if (valid) {
+            key = keys_in[idx];
+            val = vals_in[idx];
+            d = (uint32_t)(key >> shift) & 255u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < kSortThreads / 32; ++w) wcount[w][t] = 0;
+        __syncthreads();
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int rank_w = __popc(peers & ((1u << lane) - 1u));
+        if (valid && rank_w == 0) wcount[warp][d] = (uint16_t)__popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t pre = 0;
+            for (int w = 0; w < warp; ++w) pre += wcount[w][d];
+            const uint32_t pos = digit_base[d] + run[d] + pre + (uint32_t)rank_w;
+            keys_out[pos] = key;
+            vals_out[pos] = val;
+        }
+        __syncthreads();
+        uint32_t tot = 0;
+#pragma unroll
+        for (int w = 0; w < kSortThreads / 32; ++w) tot += wcount[w][t];
+        run[t] += tot;
+        if (base + (uint32_t)(r + 1) * kSortThreads >= n) break;   // uniform
+    }
+}
+
+inline int sort_max_tiles(uint32_t cap) { return (int)((cap + kSortTile - 1) / kSortTile) + 1; }
+
+// Sorts `bits` low bits of the keys.  Buffers a/b ping-pong; returns true when
+// the result ended in the `alt` buffers.  hist needs 256 * sort_max_tiles(cap)
+// entries, digit_total 256.
+template <class K>
+inline bool radix_sort(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt,
+                       const uint32_t *n_dev, uint32_t n_static, uint32_t cap, int bits,
+                       uint32_t *hist, uint32_t *digit_total, cudaStream_t st) {
+    const int max_tiles = sort_max_tiles(cap);
+    bool in_alt = false;
+    for (int shift = 0; shift < bits; shift += 8) {
+        K *ki = in_alt ? keys_alt : keys;
+        uint32_t *vi = in_alt ? vals_alt : vals;
+        K *ko = in_alt ? keys : keys_alt;
+        uint32_t *vo = in_alt ? vals : vals_alt;
+        k_radix_upsweep<K><<<max_tiles, kSortThreads, 0, st>>>(ki, n_dev, n_static, shift, hist, max_tiles);
+        k_radix_scan<<<256, 256, 0, st>>>(hist, max_tiles, digit_total);
+        k_radix_scatter<K><<<max_tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_dev, n_static, shift, hist,
+                                                                max_tiles, digit_total);
+        in_alt = !in_alt;
+    }
+    return in_alt;
+}
+
+inline int bits_for(uint64_t max_value) {
+    int b = 1;
+    while (b < 64 && (max_value >> b) != 0) ++b;
+    return b;
+}
+
+}  // namespace ws

@@ -1,0 +1,819 @@
+// Gauss-Newton iteration of the B200 warp-field solver: term evaluation,
+// J^T J / J^T r assembly as warp-segmented reductions over the term lists, and a
+// persistent cooperative block-PCG with fused SpMV + dot + axpy.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ws_common.cuh"
+#include "ws_workspace.h"
+
+namespace ws {
+
+__device__ __forceinline__ void set_err(int *flag, int code) { atomicCAS(flag, 0, code); }
+
+// ---------------------------------------------------------------------------
+// Warp-field initialisation (SolverIterationData::SetWarpFieldInitialValue,
+// examples/mono_star/opt/SolverIterationData.cu:8-17, 112-125).
+// ---------------------------------------------------------------------------
+__global__ void k_init_warp(const Scene *scenes, const uint32_t *node_scene, uint32_t total_nodes, float *se3) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
+        const Scene &sc = scenes[node_scene[g]];
+        (void)sc;
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 1.f), q1 = make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float4 *>(se3 + 8ull * g)[0] = q0;
+        reinterpret_cast<float4 *>(se3 + 8ull * g)[1] = q1;
+    }
+}
+
+__global__ void k_copy_init_warp(const float *init, uint32_t node_base, uint32_t num_nodes, float *se3) {
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nodes; n += gridDim.x * blockDim.x) {
+        const float4 *src = reinterpret_cast<const float4 *>(init + 8ull * n);
+        float4 *dst = reinterpret_cast<float4 *>(se3 + 8ull * (node_base + n));
+        dst[0] = src[0];
+        dst[1] = src[1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dense depth + optical-flow term (computeDenseImageJacobianKernel,
+// examples/mono_star/opt/DenseImageJacobianResidual.cu:164-308, with :12-25 and :77-115).
+// One thread per compacted term; writes a 128-byte record:
+//   [0,18) gradient (3 channels x [rotation | translation]), [18,21) residual,
+//   [22,26) knn weights (spatial * connect), [26,30) global knn node ids.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const uint32_t *counts,
+                                                     const ushort4 *pixels, const ushort4 *knn, const float4 *sw,
+                                                     const float4 *cw, const uint32_t *term_scene, const float *se3,
+                                                     float *record) {
+    const uint32_t n = counts[kCntDense];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const Scene &sc = scenes[term_scene[t]];
+        const ushort4 k4 = knn[t];
+        const float4 s4 = sw[t], c4 = cw[t];
+        const uint32_t nb = (uint32_t)sc.node_base;
+        const uint32_t g[4] = {nb + k4.x, nb + k4.y, nb + k4.z, nb + k4.w};
+        const float w[4] = {s4.x * c4.x, s4.y * c4.y, s4.z * c4.z, s4.w * c4.w};
+        // averageDualQuaternion, pointer overload (libs/star/math/DualQuaternion.hpp:244-261)
+        DQf avg;
+        avg.q0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        avg.q1 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const DQf d = load_dq(se3 + 8ull * g[k]);
+            avg.q0 = make_float4(avg.q0.x + w[k] * d.q0.x, avg.q0.y + w[k] * d.q0.y, avg.q0.z + w[k] * d.q0.z,
+                                 avg.q0.w + w[k] * d.q0.w);
+            avg.q1 = make_float4(avg.q1.x + w[k] * d.q1.x, avg.q1.y + w[k] * d.q1.y, avg.q1.z + w[k] * d.q1.z,
+                                 avg.q1.w + w[k] * d.q1.w);
+        }
+        const SE3f T = dq_se3(avg);
+        const ushort4 px = pixels[t];
+        const size_t spix = (size_t)px.y * sc.pitch + px.x;
+        const float4 cv4 = sc.rvert[spix], cn4 = sc.rnorm[spix];
+        const float3 vw = mul(T.rot, f3(cv4.x, cv4.y, cv4.z)) + T.t;
+        const float3 nw = mul(T.rot, f3(cn4.x, cn4.y, cn4.z));
+        M33 W;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) W.m[i][j] = sc.w2c[4 * i + j];
+        const float3 wt = f3(sc.w2c[3], sc.w2c[7], sc.w2c[11]);
+        const float3 vc = mul(W, vw) + wt;
+        const float3 nc = mul(W, nw);
+        float gr[18];
+        float res[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < 18; ++i) gr[i] = 0.f;
+        if (px.z < (unsigned)sc.width && px.w < (unsigned)sc.height) {
+            const size_t tpix = (size_t)px.w * sc.pitch + px.z;
+            const float4 tv4 = sc.mvert[tpix], tn4 = sc.mnorm[tpix];
+            const float3 tv = f3(tv4.x, tv4.y, tv4.z), tn = f3(tn4.x, tn4.y, tn4.z);
+            bool ok = true;
+            if (fabsf(tv4.x) < 1e-3 && fabsf(tv4.y) < 1e-3 && fabsf(tv4.z) < 1e-3) ok = false;   // is_zero_vertex
+            if (dot3(tn, nc) < 0.7f) ok = false;                                                  // global_configs.h:57
+            if (fabsf(tv.z - vc.z) > 0.03f) ok = false;                                           // global_configs.h:58
+            if (ok) {
+                const float3 tvw = tmul(W, tv - wt);   // apply_inversed_se3
+                const float3 tnw = tmul(W, tn);        // rot.transpose_dot
+                res[0] = dot3(tnw, vw - tvw);
+                const float3 rr = cross3(vw, tnw);
+                gr[0] = rr.x; gr[1] = rr.y; gr[2] = rr.z;
+                gr[3] = tnw.x; gr[4] = tnw.y; gr[5] = tnw.z;
+                const float3 diff = vw - tvw;
+                const float3 row0 = f3(W.m[0][0], W.m[0][1], W.m[0][2]);
+                const float3 row1 = f3(W.m[1][0], W.m[1][1], W.m[1][2]);
+                const float ex = dot3(row0, diff), ey = dot3(row1, diff);
+                if (!(sqrtf(ex * ex + ey * ey) < 1e-6f)) {
+                    res[1] = ex;
+                    res[2] = ey;
+                    const float3 mv = f3(-vw.x, -vw.y, -vw.z);
+                    gr[6] = row0.y * mv.z - row0.z * mv.y;
+                    gr[7] = -row0.x * mv.z + row0.z * mv.x;
+                    gr[8] = row0.x * mv.y - row0.y * mv.x;
+                    gr[9] = row0.x; gr[10] = row0.y; gr[11] = row0.z;
+                    gr[12] = row1.y * mv.z - row1.z * mv.y;
+                    gr[13] = -row1.x * mv.z + row1.z * mv.x;
+                    gr[14] = row1.x * mv.y - row1.y * mv.x;
+                    gr[15] = row1.x; gr[16] = row1.y; gr[17] = row1.z;
+                }
+            }
+        }
+        float4 *out = reinterpret_cast<float4 *>(record + (size_t)kDenseRecord * t);
+        out[0] = make_float4(gr[0], gr[1], gr[2], gr[3]);
+        out[1] = make_float4(gr[4], gr[5], gr[6], gr[7]);
+        out[2] = make_float4(gr[8], gr[9], gr[10], gr[11]);
+        out[3] = make_float4(gr[12], gr[13], gr[14], gr[15]);
+        out[4] = make_float4(gr[16], gr[17], res[0], res[1]);
+        out[5] = make_float4(res[2], 0.f, w[0], w[1]);
+        out[6] = make_float4(w[2], w[3], __uint_as_float(g[0]), __uint_as_float(g[1]));
+        out[7] = make_float4(__uint_as_float(g[2]), __uint_as_float(g[3]), 0.f, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ARAP smoothness term (forwardWarpSmootherNodeKernel,
+// examples/mono_star/opt/NodeGraphHandler.cu:7-45).  Record (48 B):
+//   [0,3) Ti xj, [3,6) Tj xj, [6] connect weight, [7] validity, [8] i, [9] j (global ids).
+// ---------------------------------------------------------------------------
+__global__ void k_eval_reg(const Scene *scenes, const uint32_t *edge_scene, uint32_t total_edges, const float *se3,
+                           float *record) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total_edges; e += gridDim.x * blockDim.x) {
+        const Scene &sc = scenes[edge_scene[e]];
+        const uint32_t el = e - sc.edge_base;
+        // out-of-range ids were flagged by the index build; clamp so every read stays in bounds
+        const uint16_t last = (uint16_t)(sc.num_nodes - 1);
+        const uint16_t i = min(sc.edges[3 * el], last), j = min(sc.edges[3 * el + 1], last);
+        const uint16_t k = min(sc.edges[3 * el + 2], (uint16_t)(sc.graph_k - 1));
+        const float4 xi = sc.node_coords[i], xj = sc.node_coords[j];
+        const SE3f Ti = dq_se3(load_dq(se3 + 8ull * (sc.node_base + i)));
+        const SE3f Tj = dq_se3(load_dq(se3 + 8ull * (sc.node_base + j)));
+        const float3 vj = f3(xj.x, xj.y, xj.z);
+        const float3 a = mul(Ti.rot, vj) + Ti.t;
+        const float3 b = mul(Tj.rot, vj) + Tj.t;
+        const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        const float valid = (d2 > 64 * sc.node_r2) ? 0.f : 1.f;   // CLIP_FARAWAY_NODEGRAPH_PAIR
+        const float c = sc.node_cw[(size_t)i * sc.graph_k + k];
+        float4 *out = reinterpret_cast<float4 *>(record + (size_t)kRegRecord * e);
+        out[0] = make_float4(a.x, a.y, a.z, b.x);
+        out[1] = make_float4(b.y, b.z, c, valid);
+        out[2] = make_float4(__uint_as_float(sc.node_base + i), __uint_as_float(sc.node_base + j), 0.f, 0.f);
+    }
+}
+
+// Reg Jacobian rows without the connect weight (libs/star/opt/node_graph_reg_jacobian.cuh:85-106).
+__device__ __forceinline__ void reg_unit_jacobian(float3 a, float3 b, bool is_i, float J[3][6]) {
+    if (is_i) {
+        J[0][0] = 0.f;  J[0][1] = a.z;  J[0][2] = -a.y; J[0][3] = 1.f; J[0][4] = 0.f; J[0][5] = 0.f;
+        J[1][0] = -a.z; J[1][1] = 0.f;  J[1][2] = a.x;  J[1][3] = 0.f; J[1][4] = 1.f; J[1][5] = 0.f;
+        J[2][0] = a.y;  J[2][1] = -a.x; J[2][2] = 0.f;  J[2][3] = 0.f; J[2][4] = 0.f; J[2][5] = 1.f;
+    } else {
+        J[0][0] = 0.f;  J[0][1] = -b.z; J[0][2] = b.y;  J[0][3] = -1.f; J[0][4] = 0.f;  J[0][5] = 0.f;
+        J[1][0] = b.z;  J[1][1] = 0.f;  J[1][2] = -b.x; J[1][3] = 0.f;  J[1][4] = -1.f; J[1][5] = 0.f;
+        J[2][0] = -b.y; J[2][1] = b.x;  J[2][2] = 0.f;  J[2][3] = 0.f;  J[2][4] = 0.f;  J[2][5] = -1.f;
+    }
+}
+
+__device__ __forceinline__ int tri_index(int a, int c) {   // upper triangle (a <= c), row-major
+    return a * 6 - (a * (a - 1)) / 2 + (c - a);
+}
+
+// ---------------------------------------------------------------------------
+// 6x6 block inverses.
+// ---------------------------------------------------------------------------
+// DenseGaussian<6>::Inverse with partial pivoting (libs/star/math/DenseGaussian.hpp:33-112), FP32.
+__device__ void gauss_jordan6(const float *in, float *out) {
+    float m[36];
+    for (int i = 0; i < 36; ++i) m[i] = in[i];
+    int perm[6], reloc[6];
+    for (int i = 0; i < 6; ++i) perm[i] = i;
+    for (int i = 0; i < 6; ++i) {
+        int piv = i;
+        float pv = fabsf(m[6 * i + i]);
+        for (int j = i + 1; j < 6; ++j)
+            if (pv < fabsf(m[6 * j + i])) { pv = fabsf(m[6 * j + i]); piv = j; }
+        for (int k = 0; k < 6; ++k) { const float t = m[6 * i + k]; m[6 * i + k] = m[6 * piv + k]; m[6 * piv + k] = t; }
+        { const int t = perm[i]; perm[i] = perm[piv]; perm[piv] = t; }
+        reloc[i] = perm[i];
+        const float inv = 1.0f / m[6 * i + i];
+        for (int k = 0; k < 6; ++k) m[6 * i + k] *= inv;
+        m[6 * i + i] = inv;
+        for (int r = 0; r < 6; ++r) {
+            if (r == i) continue;
+            const float a = m[6 * r + i];
+            for (int k = 0; k < 6; ++k) m[6 * r + k] -= a * m[6 * i + k];
+            m[6 * r + i] = -a * m[6 * i + i];
+        }
+    }
+    for (int j = 0; j < 6; ++j)
+        for (int i = 0; i < 6; ++i) out[6 * reloc[j] + i] = m[6 * i + j];
+}
+
+// Symmetric positive definite 6x6 inverse by Cholesky in FP64.
+__device__ void cholesky6_fp64(const float *in, float *out) {
+    double L[21];   // packed lower triangle, row i holds i+1 entries
+#define LI(i, j) L[(i) * ((i) + 1) / 2 + (j)]
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double s = (double)in[6 * i + j];
+            for (int k = 0; k < j; ++k) s -= LI(i, k) * LI(j, k);
+            if (i == j) LI(i, i) = sqrt(s > 0.0 ? s : 1e-300);
+            else LI(i, j) = s / LI(j, j);
+        }
+    double Linv[21];
+#define LV(i, j) Linv[(i) * ((i) + 1) / 2 + (j)]
+    for (int i = 0; i < 6; ++i) {
+        LV(i, i) = 1.0 / LI(i, i);
+        for (int j = 0; j < i; ++j) {
+            double s = 0.0;
+            for (int k = j; k < i; ++k) s -= LI(i, k) * LV(k, j);
+            LV(i, j) = s / LI(i, i);
+        }
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = i; j < 6; ++j) {
+            double s = 0.0;
+            for (int k = j; k < 6; ++k) s += LV(k, i) * LV(k, j);
+            out[6 * i + j] = (float)s;
+            out[6 * j + i] = (float)s;
+        }
+#undef LI
+#undef LV
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal blocks, preconditioner and right-hand side: one warp per node over
+// its node->term list (computeBlockDiagonalPreconditionerKernel,
+// examples/mono_star/opt/PreconditionerRhsBuilder.cu:110-261, and
+// computeJtResidualWithIndexKernel, JtDotResidualIndexed.cu:40-149).
+// Lane l takes list positions l, l+32, ...; a fixed butterfly combines lanes.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, const Plan *plan,
+                                                        const uint32_t *node_scene, uint32_t total_nodes,
+                                                        const uint32_t *n2t_offset, const uint32_t *n2t_val,
+                                                        const float *drec, const float *rrec, const float *se3,
+                                                        const uint32_t *rowptr, uint32_t cap_blocks, float *blocks,
+                                                        float *inv_diag, float *jtr, int precision, int *err) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total_nodes; g += warps) {
+        const uint32_t s = node_scene[g];
+        const Scene &sc = scenes[s];
+        const Plan &p = plan[s];
+        const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
+        const float lam2[3] = {sc.lam_depth * sc.lam_depth, sc.lam_of * sc.lam_of, sc.lam_of * sc.lam_of};
+        const float reg2 = sc.lam_reg * sc.lam_reg;
+        const float node2 = sc.lam_node * sc.lam_node;
+        float D[21], b[6];
+#pragma unroll
+        for (int i = 0; i < 21; ++i) D[i] = 0.f;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) b[i] = 0.f;
+        const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
+        for (uint32_t it = beg + lane; it < end; it += 32) {
+            const uint32_t term = n2t_val[it];
+            if (term < nd) {
+                const float4 *rec = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * (p.dense_begin + term));
+                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4], r5 = rec[5], r6 = rec[6],
+                             r7 = rec[7];
+                const float gv[18] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x,
+                                      r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y};
+                const float res[3] = {r4.z, r4.w, r5.x};
+                const float wk[4] = {r5.z, r5.w, r6.x, r6.y};
+                const uint32_t ids[4] = {__float_as_uint(r6.z), __float_as_uint(r6.w), __float_as_uint(r7.x),
+                                         __float_as_uint(r7.y)};
+                int slot = 0;   // last matching slot (libs/star/opt/dense_image_jacobian.cuh:9-20)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) if (ids[k] == g) slot = k;
+                const float w = wk[slot];
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    float J[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) J[q] = gv[6 * ch + q] * w;
+#pragma unroll
+                    for (int a = 0; a < 6; ++a)
+#pragma unroll
+                        for (int c = a; c < 6; ++c) D[tri_index(a, c)] += (lam2[ch] * J[a]) * J[c];
+                    const float ow = lam2[ch] * (w * w);
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) b[q] -= (ow * res[ch]) * gv[6 * ch + q];
+                }
+            } else if (term < nd + ne) {
+                const float4 *rec = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * (sc.edge_base + term - nd));
+                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2];
+                if (r1.w == 0.f) continue;
+                const float3 a3 = f3(r0.x, r0.y, r0.z), b3 = f3(r0.w, r1.x, r1.y);
+                const float c = r1.z;
+                const bool is_i = (__float_as_uint(r2.x) == g);
+                float J[3][6];
+                reg_unit_jacobian(a3, b3, is_i, J);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    float Jc[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) Jc[q] = J[ch][q] * c;
+#pragma unroll
+                    for (int a = 0; a < 6; ++a)
+#pragma unroll
+                        for (int cc = a; cc < 6; ++cc) D[tri_index(a, cc)] += (reg2 * Jc[a]) * Jc[cc];
+                }
+                // computeRegTermJtResidual (node_graph_reg_jacobian.cuh:193-233)
+                const float c2 = c * c;
+                const float rv[3] = {(a3.x - b3.x) * c2, (a3.y - b3.y) * c2, (a3.z - b3.z) * c2};
+#pragma unroll
+                for (int q = 0; q < 6; ++q) b[q] -= reg2 * (rv[0] * J[0][q] + rv[1] * J[1][q] + rv[2] * J[2][q]);
+            } else if (term < nd + ne + nn) {
+                // node-motion term (node_motion_jacobian.cuh:7-36), lambda_node = 0 by default
+                if (node2 != 0.f && sc.node_motion) {
+                    const uint32_t nl = term - nd - ne;
+                    const float4 pred = sc.node_motion[nl];
+                    const SE3f T = dq_se3(load_dq(se3 + 8ull * (sc.node_base + nl)));
+                    const float conf = pred.w, c2 = pred.w * pred.w;
+                    D[tri_index(3, 3)] += (node2 * conf) * conf;
+                    D[tri_index(4, 4)] += (node2 * conf) * conf;
+                    D[tri_index(5, 5)] += (node2 * conf) * conf;
+                    b[3] -= node2 * ((T.t.x - pred.x) * c2);
+                    b[4] -= node2 * ((T.t.y - pred.y) * c2);
+                    b[5] -= node2 * ((T.t.z - pred.z) * c2);
+                }
+            }
+            // feature terms: zero Jacobian (PreconditionerRhsBuilder.cu:214-219)
+        }
+#pragma unroll
+        for (int i = 0; i < 21; ++i) D[i] = warp_sum(D[i]);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) b[i] = warp_sum(b[i]);
+        // full block with +1e-3 on the diagonal (PreconditionerRhsBuilder.cu:249-252)
+        float full[36];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) full[6 * a + c] = (a <= c) ? D[tri_index(a, c)] : D[tri_index(c, a)];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) full[7 * a] += 1e-3f;
+        const uint32_t slot = rowptr[g];
+        if (slot < cap_blocks && lane < 9) {
+            float4 v = make_float4(full[4 * lane], full[4 * lane + 1], full[4 * lane + 2], full[4 * lane + 3]);
+            reinterpret_cast<float4 *>(blocks + 36ull * slot)[lane] = v;
+        }
+        if (lane < 2) {
+            reinterpret_cast<float4 *>(jtr + 8ull * g)[lane] =
+                lane == 0 ? make_float4(b[0], b[1], b[2], b[3]) : make_float4(b[4], b[5], 0.f, 0.f);
+        }
+        if (lane == 0) {
+            bool bad = false;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) bad |= isnan(b[i]);
+            if (bad) set_err(err, WS_ERR_NAN);
+            float inv[36];
+            if (precision == WS_PREC_FP32) gauss_jordan6(full, inv);
+            else cholesky6_fp64(full, inv);
+            float4 *o = reinterpret_cast<float4 *>(inv_diag + 36ull * g);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) o[i] = make_float4(inv[4 * i], inv[4 * i + 1], inv[4 * i + 2], inv[4 * i + 3]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Off-diagonal blocks, once per unordered node pair (computeJtJNonDiagonalBlockKernel,
+// examples/mono_star/opt/JtJMaterializer.cu:66-174): A_ij goes to the (i, j) slot and
+// its transpose to the (j, i) slot.  A[6*i+a][6*j+c] = sum lambda^2 (J_i^T J_j)[a][c].
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, const Plan *plan,
+                                                        const uint32_t *node_scene, const uint32_t *counts,
+                                                        const uint32_t *half_row, const uint32_t *half_col,
+                                                        const uint32_t *half_begin, const uint32_t *half_end,
+                                                        const uint32_t *pair_val, const uint32_t *slot_up,
+                                                        const uint32_t *slot_lo, const float *drec, const float *rrec,
+                                                        float *blocks) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nhalf = counts[kCntHalf];
+    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < nhalf; h += warps) {
+        const uint32_t row = half_row[h], col = half_col[h];
+        const uint32_t s = node_scene[row];
+        const Scene &sc = scenes[s];
+        const Plan &p = plan[s];
+        const uint32_t nd = p.dense_count, ne = sc.num_edges;
+        const float lam2[3] = {sc.lam_depth * sc.lam_depth, sc.lam_of * sc.lam_of, sc.lam_of * sc.lam_of};
+        const float reg2 = sc.lam_reg * sc.lam_reg;
+        float A[36];
+#pragma unroll
+        for (int i = 0; i < 36; ++i) A[i] = 0.f;
+        for (uint32_t it = half_begin[h] + lane; it < half_end[h]; it += 32) {
+            const uint32_t term = pair_val[it];
+            if (term < nd) {
+                const float4 *rec = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * (p.dense_begin + term));
+                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4], r5 = rec[5], r6 = rec[6],
+                             r7 = rec[7];
+                const float gv[18] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x,
+                                      r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y};
+                const float wk[4] = {r5.z, r5.w, r6.x, r6.y};
+                const uint32_t ids[4] = {__float_as_uint(r6.z), __float_as_uint(r6.w), __float_as_uint(r7.x),
+                                         __float_as_uint(r7.y)};
+                int si = 0, sj = 0;   // computeDenseImageJtJBlockJacobian (dense_image_jacobian.cuh:82-126)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (ids[k] == row) si = k;
+                    if (ids[k] == col) sj = k;
+                }
+                const float wij = wk[si] * wk[sj];
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    const float f = lam2[ch] * wij;
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) {
+                        const float fa = f * gv[6 * ch + a];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) A[6 * a + c] += fa * gv[6 * ch + c];
+                    }
+                }
+            } else if (term < nd + ne) {
+                // computeRegJtJLocalBlock (libs/star/opt/node_graph_reg_jacobian.cuh:273-358)
+                const float4 *rec = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * (sc.edge_base + term - nd));
+                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2];
+                if (r1.w == 0.f) continue;
+                const float3 a3 = f3(r0.x, r0.y, r0.z), b3 = f3(r0.w, r1.x, r1.y);
+                const float c = r1.z;
+                const uint32_t ei = __float_as_uint(r2.x);
+                float Jr[3][6], Jc[3][6];
+                reg_unit_jacobian(a3, b3, row == ei, Jr);
+                reg_unit_jacobian(a3, b3, col == ei, Jc);
+                const float ws = reg2 * (c * c);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) {
+                        const float fa = ws * Jr[ch][a];
+#pragma unroll
+                        for (int cc = 0; cc < 6; ++cc) A[6 * a + cc] += fa * Jc[ch][cc];
+                    }
+            }
+            // node-motion terms own no pairs; feature terms have zero Jacobian
+        }
+#pragma unroll
+        for (int i = 0; i < 36; ++i) A[i] = warp_sum(A[i]);
+        const uint32_t su = slot_up[h], sl = slot_lo[h];
+        if (su == kInvalidIndex) continue;
+        if (lane < 9) {
+            reinterpret_cast<float4 *>(blocks + 36ull * su)[lane] =
+                make_float4(A[4 * lane], A[4 * lane + 1], A[4 * lane + 2], A[4 * lane + 3]);
+        } else if (lane < 18) {
+            const int q = lane - 9;
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int idx = 4 * q + e, a = idx / 6, c = idx % 6;
+                v[e] = A[6 * c + a];
+            }
+            reinterpret_cast<float4 *>(blocks + 36ull * sl)[q] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent block PCG (BlockPCG<6>::SolveNoConvergeCheck,
+// libs/star/pcg_solver/BlockPCG.cuh:67-190, 325-484) for every scene of the batch.
+//
+// Rows (nodes) are grouped in scene-aligned chunks of 8, one warp per row.
+// Per iteration: phase A  d = s + beta d (recomputed for neighbours), q = A d,
+// partial <d, q>;  phase B  alpha, x += alpha d, r -= alpha q, s = M^-1 r,
+// partial <r, s>.  The last chunk of a scene to finish a phase reduces that
+// scene's chunk partials in chunk order and publishes alpha / beta, so every
+// scene's arithmetic is independent of the rest of the batch.  Two bounded
+// grid barriers per iteration; a timed-out wait sets WS_ERR_TIMEOUT and every
+// block leaves.
+// ---------------------------------------------------------------------------
+constexpr int kPcgThreads = 256;   // 8 warps: one chunk of 8 rows per block round
+
+struct PcgArgs {
+    const Scene *scenes;
+    const uint32_t *chunk_scene, *chunk_row;
+    uint32_t total_chunks;
+    const uint32_t *rowptr, *colidx;
+    const float *blocks, *inv_diag, *jtr;
+    float *x, *r, *s, *q, *d0, *d1;
+    double *chunk_partial;
+    double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
+    uint32_t *scene_counter;  // per scene: [0] phase A, [1] phase B
+    uint32_t *barrier;        // [0] arrive count, [1] generation
+    uint32_t cap_blocks, total_nodes;
+    int *err;
+    float *se3;
+    int pcg_iters;
+    int fp64;
+};
+
+__device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile uint32_t *gen = bar + 1;
+        const uint32_t my_gen = *gen;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*gen == my_gen) {
+                if (++spins > kSpinLimit) { set_err(err, WS_ERR_TIMEOUT); ok = 0; break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (*reinterpret_cast<volatile int *>(err) == WS_ERR_TIMEOUT) ok = 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
+
+// CTA-level chunk partial: warps write row partials to smem, thread 0 sums in warp order,
+// publishes the chunk partial, and the last chunk of the scene reduces the scene.
+// Returns nothing; `mode` 0 = phase A (alpha), 1 = phase B (beta), 2 = init (delta only).
+__device__ void publish_partial(const PcgArgs &A, uint32_t chunk, uint32_t scene, double *wpart, int mode) {
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < kPcgThreads / 32; ++w) sum += wpart[w];
+        A.chunk_partial[chunk] = sum;
+        __threadfence();
+        const Scene &sc = A.scenes[scene];
+        const uint32_t ctr = (mode == 0) ? 0u : 1u;
+        const uint32_t ticket = atomicAdd(&A.scene_counter[2 * scene + ctr], 1u);
+        last = (ticket == (uint32_t)sc.num_chunks - 1u) ? 1 : 0;
+        if (last) atomicExch(&A.scene_counter[2 * scene + ctr], 0u);
+        __threadfence();
+    }
+    __syncthreads();
+    if (last && threadIdx.x < 32) {
+        const Scene &sc = A.scenes[scene];
+        double v = 0.0;
+        for (int c = threadIdx.x; c < sc.num_chunks; c += 32) v += ldcg(A.chunk_partial + sc.chunk_base + c);
+        v = warp_sum(v);
+        if (threadIdx.x == 0) {
+            double *S = A.scalars + 8ull * scene;
+            if (!A.fp64) v = (double)(float)v;
+            if (mode == 0) {
+                const double delta = ldcg(S + 0);
+                double alpha = (v != 0.0) ? delta / v : 0.0;
+                if (!A.fp64) alpha = (double)((float)delta / (float)v);
+                if (v == 0.0) alpha = 0.0;
+                S[1] = alpha;
+            } else {
+                const double delta_old = ldcg(S + 0);
+                double beta = (delta_old != 0.0) ? v / delta_old : 0.0;
+                if (!A.fp64 && delta_old != 0.0) beta = (double)((float)v / (float)delta_old);
+                S[2] = (mode == 2) ? 0.0 : beta;
+                S[0] = v;
+            }
+            S[3] = v;
+            __threadfence();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ double wpart[kPcgThreads / 32];
+    const int slot = lane / 6, a = lane % 6;      // SpMV lane mapping: 5 block slots x 6 rows
+    // ---- init: r = b, s = M^-1 b, x = 0, d = 0, delta = <r, s> ----
+    for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
+        const uint32_t scene = A.chunk_scene[ch];
+        const Scene &sc = A.scenes[scene];
+        const uint32_t row = A.chunk_row[ch] + warp;
+        const bool active = row < (uint32_t)(sc.node_base + sc.num_nodes);
+        double part = 0.0;
+        if (active && lane < 6) {
+            float bv[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) bv[c] = A.jtr[8ull * row + c];
+            const float *M = A.inv_diag + 36ull * row + 6 * lane;
+            float sv = 0.f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) sv += M[c] * bv[c];
+            A.r[8ull * row + lane] = bv[lane];
+            A.s[8ull * row + lane] = sv;
+            A.x[8ull * row + lane] = 0.f;
+            A.d0[8ull * row + lane] = 0.f;
+            A.d1[8ull * row + lane] = 0.f;
+            part = A.fp64 ? (double)bv[lane] * (double)sv : (double)(bv[lane] * sv);
+        }
+        if (!A.fp64) {
+            float pf = (float)part;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
+            part = pf;
+        } else {
+            part = warp_sum(part);
+        }
+        if (lane == 0) wpart[warp] = part;
+        publish_partial(A, ch, scene, wpart, 2);
+    }
+    if (!grid_barrier(A.barrier, A.err)) return;
+
+    for (int it = 0; it < A.pcg_iters; ++it) {
+        const float *d_old = (it & 1) ? A.d1 : A.d0;
+        float *d_new = (it & 1) ? A.d0 : A.d1;
+        // ---- phase A ----
+        for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
+            const uint32_t scene = A.chunk_scene[ch];
+            const Scene &sc = A.scenes[scene];
+            const uint32_t row = A.chunk_row[ch] + warp;
+            const bool active = row < (uint32_t)(sc.node_base + sc.num_nodes);
+            const float beta = (float)ldcg(A.scalars + 8ull * scene + 2);
+            double part = 0.0;
+            if (active) {
+                float acc = 0.f;
+                // bounds hold by construction; the clamps keep a capacity overflow (already
+                // flagged as WS_ERR_CAPACITY) from reading outside the buffers
+                const uint32_t b1 = min(A.rowptr[row + 1], A.cap_blocks);
+                const uint32_t b0 = min(A.rowptr[row], b1);
+                if (slot < 5) {
+                    for (uint32_t k = b0 + slot; k < b1; k += 5) {
+                        const uint32_t col = min(A.colidx[k], A.total_nodes - 1);
+                        const float2 *blk = reinterpret_cast<const float2 *>(A.blocks + 36ull * k + 6 * a);
+                        const float2 m0 = __ldg(blk), m1 = __ldg(blk + 1), m2 = __ldg(blk + 2);
+                        const float *sp = A.s + 8ull * col, *dp = d_old + 8ull * col;
+                        float dv[6];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) dv[c] = ldcg(sp + c) + beta * ldcg(dp + c);
+                        acc += m0.x * dv[0] + m0.y * dv[1] + m1.x * dv[2] + m1.y * dv[3] + m2.x * dv[4] + m2.y * dv[5];
+                    }
+                }
+                // combine the 5 slots for matrix row a in fixed order
+                const float t1 = __shfl_sync(0xffffffffu, acc, (a + 6) & 31);
+                const float t2 = __shfl_sync(0xffffffffu, acc, (a + 12) & 31);
+                const float t3 = __shfl_sync(0xffffffffu, acc, (a + 18) & 31);
+                const float t4 = __shfl_sync(0xffffffffu, acc, (a + 24) & 31);
+                if (lane < 6) {
+                    const float qa = (((acc + t1) + t2) + t3) + t4;
+                    const float dn = ldcg(A.s + 8ull * row + lane) + beta * ldcg(d_old + 8ull * row + lane);
+                    d_new[8ull * row + lane] = dn;
+                    A.q[8ull * row + lane] = qa;
+                    part = A.fp64 ? (double)dn * (double)qa : (double)(dn * qa);
+                }
+            }
+            if (!A.fp64) {
+                float pf = (float)part;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
+                part = pf;
+            } else {
+                part = warp_sum(part);
+            }
+            if (lane == 0) wpart[warp] = part;
+            publish_partial(A, ch, scene, wpart, 0);
+        }
+        if (!grid_barrier(A.barrier, A.err)) return;
+        // ---- phase B ----
+        for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
+            const uint32_t scene = A.chunk_scene[ch];
+            const Scene &sc = A.scenes[scene];
+            const uint32_t row = A.chunk_row[ch] + warp;
+            const bool active = row < (uint32_t)(sc.node_base + sc.num_nodes);
+            const float alpha = (float)ldcg(A.scalars + 8ull * scene + 1);
+            double part = 0.0;
+            float rn = 0.f;
+            if (active && lane < 6) {
+                const float dn = ldcg(d_new + 8ull * row + lane);
+                const float qa = ldcg(A.q + 8ull * row + lane);
+                A.x[8ull * row + lane] += alpha * dn;
+                rn = A.r[8ull * row + lane] - alpha * qa;
+                A.r[8ull * row + lane] = rn;
+            }
+            float rv[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rv[c] = __shfl_sync(0xffffffffu, rn, c);
+            if (active && lane < 6) {
+                const float *M = A.inv_diag + 36ull * row + 6 * lane;
+                float sv = 0.f;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) sv += M[c] * rv[c];
+                A.s[8ull * row + lane] = sv;
+                part = A.fp64 ? (double)rn * (double)sv : (double)(rn * sv);
+            }
+            if (!A.fp64) {
+                float pf = (float)part;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
+                part = pf;
+            } else {
+                part = warp_sum(part);
+            }
+            if (lane == 0) wpart[warp] = part;
+            publish_partial(A, ch, scene, wpart, 1);
+        }
+        if (!grid_barrier(A.barrier, A.err)) return;
+    }
+    // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
+    //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
+    for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
+        const uint32_t scene = A.chunk_scene[ch];
+        const Scene &sc = A.scenes[scene];
+        const uint32_t row = A.chunk_row[ch] + warp;
+        if (row >= (uint32_t)(sc.node_base + sc.num_nodes) || lane != 0) continue;
+        float xv[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) xv[c] = A.x[8ull * row + c];
+        const float3 w = f3(xv[0], xv[1], xv[2]);
+        SE3f inc;
+        if (fabsf(w.x) + fabsf(w.y) + fabsf(w.z) < 1e-4f) {
+            inc.rot = M33{{{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}}};
+        } else {
+            const float angle = sqrtf(w.x * w.x + w.y * w.y + w.z * w.z);
+            const float3 ax = (1.0f / angle) * w;
+            const float c = cosf(angle), sn = sinf(angle), t = 1.0f - c;
+            inc.rot.m[0][0] = t * ax.x * ax.x + c;
+            inc.rot.m[0][1] = t * ax.x * ax.y - ax.z * sn;
+            inc.rot.m[0][2] = t * ax.x * ax.z + ax.y * sn;
+            inc.rot.m[1][0] = t * ax.x * ax.y + ax.z * sn;
+            inc.rot.m[1][1] = t * ax.y * ax.y + c;
+            inc.rot.m[1][2] = t * ax.y * ax.z - ax.x * sn;
+            inc.rot.m[2][0] = t * ax.x * ax.z - ax.y * sn;
+            inc.rot.m[2][1] = t * ax.y * ax.z + ax.x * sn;
+            inc.rot.m[2][2] = t * ax.z * ax.z + c;
+        }
+        inc.t = f3(xv[3], xv[4], xv[5]);
+        const SE3f prev = dq_to_mat34(load_dq(A.se3 + 8ull * row));
+        SE3f nw;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                nw.rot.m[i][j] = inc.rot.m[i][0] * prev.rot.m[0][j] + inc.rot.m[i][1] * prev.rot.m[1][j] +
+                                 inc.rot.m[i][2] * prev.rot.m[2][j];
+        nw.t = mul(inc.rot, prev.t) + inc.t;
+        store_dq(A.se3 + 8ull * row, dq_from_mat34(nw));
+    }
+}
+
+int pcg_max_blocks(int device) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return std::max(1, per_sm) * std::max(1, sms);
+}
+
+static inline int grid_for(uint32_t n, int threads, int num_sms, int per_sm = 8) {
+    const uint32_t want = (n + threads - 1) / threads;
+    const uint32_t cap = (uint32_t)num_sms * (uint32_t)per_sm;
+    return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, cap));
+}
+
+void init_warp(Workspace &w, cudaStream_t st) {
+    k_init_warp<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.node_scene, w.total_nodes, w.se3);
+}
+
+cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {
+    k_eval_dense<<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
+        w.scenes, w.counts, w.d_pixels, w.d_knn, w.d_sw, w.d_cw, w.d_scene, w.se3, w.d_record);
+    if (w.total_edges > 0)
+        k_eval_reg<<<grid_for(w.total_edges, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.edge_scene, w.total_edges,
+                                                                            w.se3, w.r_record);
+    k_assemble_node<<<grid_for(w.total_nodes * 32u, 256, w.num_sms, 16), 256, 0, st>>>(
+        w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
+        w.rowptr, w.cap_blocks, w.blocks, w.inv_diag, w.jtr, w.precision, w.error_flag);
+    k_assemble_pair<<<grid_for(w.cap_half * 32u, 256, w.num_sms, 16), 256, 0, st>>>(
+        w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
+        w.half_slot_up, w.half_slot_lo, w.d_record, w.r_record, w.blocks);
+    PcgArgs a;
+    a.scenes = w.scenes;
+    a.chunk_scene = w.chunk_scene;
+    a.chunk_row = w.chunk_row;
+    a.total_chunks = w.total_chunks;
+    a.rowptr = w.rowptr;
+    a.colidx = w.colidx;
+    a.blocks = w.blocks;
+    a.inv_diag = w.inv_diag;
+    a.jtr = w.jtr;
+    a.x = w.x; a.r = w.r; a.s = w.s; a.q = w.q; a.d0 = w.d0; a.d1 = w.d1;
+    a.chunk_partial = w.chunk_partial;
+    a.scalars = w.scene_scalars;
+    a.scene_counter = w.scene_counter;
+    a.barrier = w.barrier;
+    a.cap_blocks = w.cap_blocks;
+    a.total_nodes = w.total_nodes;
+    a.err = w.error_flag;
+    a.se3 = w.se3;
+    a.pcg_iters = pcg_iters;
+    a.fp64 = (w.precision == WS_PREC_MIXED) ? 1 : 0;
+    const int grid = (int)std::min<uint32_t>(w.total_chunks, (uint32_t)w.pcg_grid);
+    // a barrier or counter left half-way by an earlier timed-out launch must not leak into this one
+    cudaMemsetAsync(w.barrier, 0, 4 * sizeof(uint32_t), st);
+    cudaMemsetAsync(w.scene_counter, 0, 2 * sizeof(uint32_t) * (size_t)w.num_scenes, st);
+    void *args[] = {&a};
+    return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, 0, st);
+}
+
+}  // namespace ws

@@ -1,0 +1,116 @@
+// Device workspace of one solver object: every buffer the solve touches is
+// allocated once at creation, sized by the ws_config capacities, and reused by
+// every solve (the reference preallocates at kMaxNumNodes and image size the
+// same way, examples/mono_star/opt/WarpSolver.cu:82-103).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "ws_common.cuh"
+
+namespace ws {
+
+struct Workspace {
+    // capacities
+    int cap_scenes = 0;
+    uint32_t cap_nodes = 0, cap_pixels = 0, cap_edges = 0, cap_features = 0;
+    uint32_t cap_tiles = 0, cap_chunks = 0;
+    uint32_t cap_n2t = 0, cap_pair_kv = 0, cap_half = 0, cap_blocks = 0;
+    int precision = WS_PREC_MIXED;
+    int device = 0;
+    int num_sms = 0;
+    int pcg_grid = 0;           // co-resident blocks for the persistent PCG kernel
+
+    // current batch (host mirror)
+    int num_scenes = 0;
+    uint32_t total_nodes = 0, total_edges = 0, total_tiles = 0, total_chunks = 0, total_features = 0;
+    int node_bits = 1;
+    std::vector<Scene> h_scenes;
+    bool have_inputs = false;
+    bool have_solution = false;
+
+    // scene tables
+    Scene *scenes = nullptr;            // [cap_scenes]
+    Plan *plan = nullptr;               // [cap_scenes]
+    uint32_t *counts = nullptr;         // [8]: dense total, n2t kv total, pair kv total, half total, ...
+    uint32_t *tile_scene = nullptr;     // [cap_tiles]
+    uint32_t *tile_count = nullptr;     // [cap_tiles + 1] (exclusive offsets after the scan)
+    uint32_t *node_scene = nullptr;     // [cap_nodes]
+    uint32_t *edge_scene = nullptr;     // [cap_edges]
+    uint32_t *chunk_scene = nullptr;    // [cap_chunks]
+    uint32_t *chunk_row = nullptr;      // [cap_chunks] first global row of the chunk
+    uint32_t *scan_tmp = nullptr;       // scan tile sums
+    uint32_t *sort_hist = nullptr;      // radix histograms
+    uint32_t *sort_digit = nullptr;     // [256]
+
+    // dense terms (compacted pixels)
+    ushort4 *d_pixels = nullptr;        // [cap_pixels]
+    ushort4 *d_knn = nullptr;           // [cap_pixels]
+    float4 *d_sw = nullptr, *d_cw = nullptr;
+    uint32_t *d_scene = nullptr;        // [cap_pixels]
+    float *d_record = nullptr;          // [cap_pixels * kDenseRecord]
+    float *r_record = nullptr;          // [cap_edges * kRegRecord]
+
+    // node->term
+    uint32_t *n2t_key = nullptr, *n2t_val = nullptr;         // [cap_n2t]
+    uint32_t *n2t_key_alt = nullptr, *n2t_val_alt = nullptr;
+    uint32_t *n2t_offset = nullptr;                          // [cap_nodes + 1]
+    const uint32_t *n2t_sorted_val = nullptr;                // points into val or val_alt
+    const uint32_t *n2t_sorted_key = nullptr;
+
+    // pair->term
+    unsigned long long *pair_key = nullptr, *pair_key_alt = nullptr;   // [cap_pair_kv]
+    uint32_t *pair_val = nullptr, *pair_val_alt = nullptr;
+    const unsigned long long *pair_sorted_key = nullptr;
+    const uint32_t *pair_sorted_val = nullptr;
+    uint32_t *pair_head = nullptr;                           // [cap_pair_kv + 1] marks, then offsets
+    uint32_t *half_row = nullptr, *half_col = nullptr;       // [cap_half]
+    uint32_t *half_begin = nullptr, *half_end = nullptr;
+    uint32_t *half_slot_up = nullptr, *half_slot_lo = nullptr;
+
+    // block CSR
+    uint32_t *row_cnt_up = nullptr, *row_cnt_lo = nullptr;   // [cap_nodes]
+    uint32_t *row_first = nullptr;                           // [cap_nodes]
+    uint32_t *rowptr = nullptr;                              // [cap_nodes + 1]
+    uint32_t *col_key = nullptr, *col_val = nullptr, *col_key_alt = nullptr, *col_val_alt = nullptr; // [cap_half]
+    uint32_t *colidx = nullptr;                              // [cap_blocks]
+    float *blocks = nullptr;                                 // [cap_blocks * 36]
+
+    // per-node system and PCG state (stride kVecStride)
+    float *inv_diag = nullptr;          // [cap_nodes * 36]
+    float *jtr = nullptr, *x = nullptr, *r = nullptr, *s = nullptr, *q = nullptr;
+    float *d0 = nullptr, *d1 = nullptr;
+    float *se3 = nullptr;               // [cap_nodes * 8] current warp
+    double *chunk_partial = nullptr;    // [cap_chunks]
+    double *scene_scalars = nullptr;    // [cap_scenes * 8]: delta, alpha, beta, dq ...
+    uint32_t *scene_counter = nullptr;  // [cap_scenes * 2]
+    uint32_t *barrier = nullptr;        // [4] count, generation
+    int *error_flag = nullptr;          // [4]
+
+    // pinned host staging of the scene tables (uploaded at the start of every solve)
+    void *h_tables = nullptr;
+    size_t h_tables_bytes = 0;
+    std::vector<const float *> init_ptrs;     // per-scene initial warp (device) or null
+
+    // graph capture cache
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<uint64_t> graph_key;
+    std::vector<const float *> graph_init;
+    cudaStream_t last_stream = nullptr;
+};
+
+// Index build (ws_index.cu): compaction, node->term, pair->term, block CSR.
+void index_build(Workspace &w, cudaStream_t st);
+// One Gauss-Newton iteration (ws_solve.cu): term evaluation, assembly, PCG, update.
+cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st);
+// Initialise the warp field of every scene (identity or the given initial warp).
+void init_warp(Workspace &w, cudaStream_t st);
+// Occupancy of the persistent PCG kernel.
+int pcg_max_blocks(int device);
+
+// Counters slot indices.
+enum { kCntDense = 0, kCntN2T = 1, kCntPairKV = 2, kCntHalf = 3, kCntPairValid = 4 };
+
+}  // namespace ws

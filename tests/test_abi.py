@@ -1,0 +1,60 @@
+"""CPU checks of the C ABI library: it loads without a GPU and exports every
+entry point include/warpsolve.h declares; host-side argument checks."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from starhub_b200 import build as b
+    b.build()
+    from starhub_b200 import _lib
+    return _lib.load()
+
+
+def declared_functions():
+    text = (ROOT / "include" / "warpsolve.h").read_text()
+    return sorted(set(re.findall(r"\b(ws_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "ws_solve" in names and "ws_create" in names and len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol(lib):
+    from starhub_b200 import _lib
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    assert sorted(_lib.EXPORTED) == declared_functions()
+
+
+def test_error_strings(lib):
+    from starhub_b200 import _lib
+    assert _lib.error_string(0) == "ok"
+    assert "capacity" in _lib.error_string(_lib.WS_ERR_CAPACITY)
+
+
+def test_create_rejects_bad_config(lib):
+    from starhub_b200._lib import WsConfig
+    h = C.c_void_p()
+    cfg = WsConfig()
+    cfg.max_scenes = 0
+    assert lib.ws_create(C.byref(cfg), C.byref(h)) == -1
+    assert lib.ws_create(None, C.byref(h)) == -1
+    assert lib.ws_destroy(None) == -1
+    assert lib.ws_solve(None, 1, 1, None) == -1
+
+
+def test_default_penalties_match_reference(lib):
+    from starhub_b200._lib import WsInputs
+    s = WsInputs()
+    lib.ws_default_penalties(C.byref(s))
+    # PenaltyConstants::setDefaultValue (examples/mono_star/opt/PenaltyConstants.cu:8-15)
+    assert (round(s.lambda_depth, 6), s.lambda_optical_flow, s.lambda_reg, s.lambda_node_translation,
+            s.lambda_feature) == (0.1, 0.0, 1.0, 0.0, 1.0)

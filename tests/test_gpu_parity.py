@@ -1,0 +1,121 @@
+"""GPU parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Integer / index outputs must be bit-exact; floating-point outputs are checked
+against the FP64 oracle with the tolerances stated at each assertion.  The
+north-star bar for a full solve is <= 1e-4 relative twist error and <= 1e-5 m
+warped-position error against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TWIST_TOL = 1e-4       # relative twist error vs the FP64 oracle (mixed precision path)
+POS_TOL = 1e-5         # metres, warped surfel positions vs the FP64 oracle
+
+
+def solve_gpu(ws, scene, gn, pcg, precision=0, graph=False):
+    import torch
+    from starhub_b200.solver import DeviceScene, WarpSolver
+    ds = DeviceScene.from_scene(scene)
+    s = WarpSolver(max_nodes=ds.num_nodes, max_pixels=ds.num_pixels, max_edges=ds.num_edges, precision=precision)
+    s.SetSolverInputs(ds)
+    stream = torch.cuda.Stream()
+    s.SolveStreamed(gn, pcg, stream=stream, graph=graph)
+    s.Sync()
+    return s, ds, s.SolvedNodeSE3(0).cpu().numpy().copy()
+
+
+def test_index_bit_exact(ws, orc, small_scene):
+    sc = small_scene
+    s, ds, _ = solve_gpu(ws, sc, 1, 1)
+    # dense terms (compaction)
+    pix, knn, sw, cw = s.dense_terms()
+    opix, oknn, osw, ocw = orc.compact_pixels(sc)
+    np.testing.assert_array_equal(pix, opix)
+    np.testing.assert_array_equal(knn, oknn)
+    np.testing.assert_array_equal(sw, osw)
+    np.testing.assert_array_equal(cw, ocw)
+    # node -> term
+    off, ti = s.node2term()
+    ooff, oti = orc.node2term(oknn, sc.edges, sc.num_nodes)
+    np.testing.assert_array_equal(off, ooff)
+    np.testing.assert_array_equal(ti, oti[: ooff[-1]])
+    # node pair -> term
+    p = s.node_pairs()
+    m = orc.nodepair2term(oknn, sc.edges, sc.num_nodes)
+    np.testing.assert_array_equal(p["rows"], m["half_rows"])
+    np.testing.assert_array_equal(p["cols"], m["half_cols"])
+    np.testing.assert_array_equal(p["begin"], m["half_begin"])
+    np.testing.assert_array_equal(p["end"], m["half_end"])
+    np.testing.assert_array_equal(p["term_index"], m["term_index"][: m["half_end"][-1]])
+    # block CSR: the symmetric pair list with the diagonal first in every row
+    sysm = s.system()
+    rp, cols = sysm["rowptr"], sysm["cols"]
+    np.testing.assert_array_equal(np.diff(rp.astype(np.int64)) - 1, np.diff(m["blkrow_offset"].astype(np.int64)))
+    for n in range(sc.num_nodes):
+        assert cols[rp[n]] == n
+        np.testing.assert_array_equal(cols[rp[n] + 1:rp[n + 1]], m["sym_cols"][m["blkrow_offset"][n]:m["blkrow_offset"][n + 1]])
+
+
+def test_first_iteration_terms_and_system(ws, orc, small_scene):
+    sc = small_scene
+    s, ds, _ = solve_gpu(ws, sc, 1, 20)
+    _, info = orc.solve(sc, gn_iters=1, pcg_iters=20, debug=True)
+    res, grad = s.dense_jacobian()
+    # FP32 device arithmetic vs FP64: residuals to 1e-6 m, gradients relative 1e-5
+    np.testing.assert_allclose(res, info["residual"], atol=2e-6, rtol=0)
+    np.testing.assert_allclose(grad, info["gradient"], atol=2e-5 * np.abs(info["gradient"]).max(), rtol=0)
+    sysm = s.system()
+    rp, cols, blocks = sysm["rowptr"], sysm["cols"], sysm["blocks"]
+    diag = blocks[rp[:-1]]
+    scale = np.abs(info["diag"]).max()
+    np.testing.assert_allclose(diag, info["diag"], atol=2e-5 * scale, rtol=0)
+    np.testing.assert_allclose(sysm["jtr"], info["jtr"], atol=2e-5 * np.abs(info["jtr"]).max(), rtol=0)
+    lookup = {(r, c): k for k, (r, c) in enumerate(zip(info["sym_rows"], info["sym_cols"]))}
+    for n in range(sc.num_nodes):
+        for k in range(rp[n] + 1, rp[n + 1]):
+            ok = lookup[(n, cols[k])]
+            np.testing.assert_allclose(blocks[k], info["offdiag"][ok], atol=2e-5 * scale, rtol=0)
+    # preconditioner (FP64 Cholesky on the device vs FP64 Cholesky on the host)
+    np.testing.assert_allclose(sysm["inv_diag"], info["inv_diag"], rtol=1e-3,
+                               atol=1e-4 * np.abs(info["inv_diag"]).max())
+    # first Gauss-Newton step
+    step_scale = np.abs(info["step"]).max()
+    np.testing.assert_allclose(sysm["step"], info["step"], atol=1e-4 * step_scale, rtol=0)
+
+
+def test_full_solve_mixed_precision(ws, orc, small_scene):
+    from starhub_b200.scenes import position_error, twist_error
+    sc = small_scene
+    _, _, dq = solve_gpu(ws, sc, sc.gn_iters, sc.pcg_iters)
+    ref = orc.solve(sc)
+    assert np.isfinite(dq).all()
+    te = twist_error(dq, ref)
+    pe = position_error(sc, dq, ref)
+    assert te <= TWIST_TOL, f"twist error {te}"
+    assert pe <= POS_TOL, f"position error {pe}"
+
+
+def test_full_solve_fp32_mode(ws, orc, small_scene):
+    from starhub_b200.scenes import twist_error
+    sc = small_scene
+    _, _, dq = solve_gpu(ws, sc, sc.gn_iters, sc.pcg_iters, precision=1)
+    ref32 = orc.solve(sc, precision=orc.ORC_PREC_FP32_REFERENCE)
+    ref64 = orc.solve(sc)
+    # FP32 everywhere as the reference: agreement bounded by FP32 PCG drift
+    assert twist_error(dq, ref64) < 5e-3
+    assert twist_error(dq, ref32) < 5e-3
+
+
+def test_graph_replay_matches_stream_solve(ws, small_scene):
+    sc = small_scene
+    _, _, a = solve_gpu(ws, sc, 3, 10, graph=False)
+    _, _, b = solve_gpu(ws, sc, 3, 10, graph=True)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_solve_is_deterministic(ws, small_scene):
+    _, _, a = solve_gpu(ws, small_scene, 2, 10)
+    _, _, b = solve_gpu(ws, small_scene, 2, 10)
+    np.testing.assert_array_equal(a, b)

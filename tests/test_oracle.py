@@ -1,0 +1,229 @@
+"""CPU checks of the oracle: known-answer tests derived from the reference's
+definitions, independent Python restatements of its integer rules, and
+properties of the assembled system.  No GPU."""
+import numpy as np
+import pytest
+
+
+# ---------------------------------------------------------------------------
+# Node graph: half-precision distances + strict-< heap + Lomuto quicksort
+# (libs/star/geometry/node_graph/NodeGraph.cu:10-101, brute_force_knn.cuh:52-135)
+# ---------------------------------------------------------------------------
+def py_knn(dist_row, k, init):
+    d = [init] * k
+    idx = [0] * k
+
+    def refresh():
+        m = 0
+        for i in range(1, k):
+            if d[i] > d[m]:
+                m = i
+        return m
+
+    m = refresh()
+    for j, v in enumerate(dist_row):
+        if v < d[m]:
+            d[m] = v
+            idx[m] = j
+        m = refresh()
+
+    def qs(lo, hi):
+        if lo < hi:
+            piv = d[hi]
+            i = lo - 1
+            for j in range(lo, hi):
+                if d[j] < piv:
+                    i += 1
+                    d[i], d[j] = d[j], d[i]
+                    idx[i], idx[j] = idx[j], idx[i]
+            d[i + 1], d[hi] = d[hi], d[i + 1]
+            idx[i + 1], idx[hi] = idx[hi], idx[i + 1]
+            qs(lo, i)
+            qs(i + 2, hi)
+
+    qs(0, k - 1)
+    return idx, d
+
+
+def half_sq_dist(a, b):
+    hi, lo = (a, b)
+    dx = np.float32(hi[0] - lo[0])
+    dy = np.float32(hi[1] - lo[1])
+    dz = np.float32(hi[2] - lo[2])
+    # fma(dz, dz, fma(dy, dy, dx*dx)) evaluated exactly in float64 then rounded once per fma
+    t = np.float32(dx * dx)
+    t = np.float32(np.float64(dy) * np.float64(dy) + np.float64(t))
+    t = np.float32(np.float64(dz) * np.float64(dz) + np.float64(t))
+    return float(np.float32(np.float16(t)))
+
+
+@pytest.mark.parametrize("k", [4, 8])
+def test_node_graph_matches_python_restatement(orc, k):
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(-0.1, 0.1, size=(40, 3)).astype(np.float32)
+    pts[5] = pts[6]          # exact duplicates -> ties
+    pts[7] = pts[6]
+    nodes = np.concatenate([np.zeros((2, 3), np.float32), pts])
+    nodes4 = np.concatenate([nodes, np.ones((len(nodes), 1), np.float32)], 1)
+    knn, w, edges = orc.OracleGeometry().node_graph(nodes4, k, 0.025)
+    for a in range(len(nodes)):
+        row = [half_sq_dist(nodes[max(a, b)], nodes[min(a, b)]) for b in range(len(nodes))]
+        idx, d = py_knn(row, k, 1e3)
+        assert list(knn[a]) == idx, f"node {a}"
+        ww = np.exp(-np.array(d, np.float32) / np.float32(2 * np.float32(0.025) * np.float32(0.025)))
+        np.testing.assert_allclose(w[a], ww / ww.sum(), rtol=1e-5)
+    assert (edges[:, 0] == np.repeat(np.arange(len(nodes)), k)).all()
+    assert (edges[:, 2] == np.tile(np.arange(k), len(nodes))).all()
+
+
+def test_node_graph_self_is_first(orc):
+    rng = np.random.default_rng(4)
+    nodes4 = np.concatenate([rng.uniform(-1, 1, (50, 3)), np.ones((50, 1))], 1).astype(np.float32)
+    knn, _, _ = orc.OracleGeometry().node_graph(nodes4, 4, 0.025)
+    assert (knn[:, 0] == np.arange(50)).all()
+
+
+def test_skinning_matches_python(orc):
+    rng = np.random.default_rng(8)
+    nodes = np.concatenate([rng.uniform(-0.2, 0.2, (30, 3)), np.ones((30, 1))], 1).astype(np.float32)
+    verts = np.concatenate([rng.uniform(-0.2, 0.2, (200, 3)), np.ones((200, 1))], 1).astype(np.float32)
+    knn, sw, cw = orc.OracleGeometry().skinning(nodes, verts, 0.025)
+    for v in range(200):
+        diff = (verts[v, :3] - nodes[:, :3]).astype(np.float32)
+        row = []
+        for d in diff:
+            t = np.float32(d[0] * d[0])
+            t = np.float32(np.float64(d[1]) ** 2 + np.float64(t))
+            t = np.float32(np.float64(d[2]) ** 2 + np.float64(t))
+            row.append(float(t))
+        idx, _ = py_knn(row, 4, 1e6)
+        assert list(knn[v]) == idx
+    assert (cw == 1.0).all()
+    np.testing.assert_allclose(sw.sum(1), 1.0, rtol=1e-6)
+
+
+def test_voxel_subsample_kat(orc):
+    v = 0.01
+    pts = np.array([[0.0012, 0.0011, 0.0010, 1], [0.0049, 0.0051, 0.0050, 1],   # voxel (0,0,0): 2nd is nearer the centre
+                    [0.0150, 0.0010, 0.0010, 1],                                 # voxel (1,0,0)
+                    [-0.0050, 0.0050, 0.0050, 1],                                # voxel (-1,0,0)
+                    [0.0052, 0.0049, 0.0050, 1]], np.float32)                    # ties with point 1? farther
+    out = orc.OracleGeometry().voxel_subsample(pts, v)
+    # keys sort (x+512) + (y+512)*1024 + ...: voxel x = -1 first, then 0, then 1
+    np.testing.assert_array_equal(out[:, :3], pts[[3, 1, 2], :3])
+
+
+def test_init_nodes_prepends_anchors_and_dedups(orc):
+    rng = np.random.default_rng(1)
+    pts = np.concatenate([rng.uniform(0, 0.2, (5000, 3)), np.ones((5000, 1))], 1).astype(np.float32)
+    nodes = orc.OracleGeometry().init_nodes(pts, 0.025)
+    np.testing.assert_array_equal(nodes[:2], [[0, 0, 0, 1], [0, 0, 0, 1]])
+    real = nodes[2:, :3].astype(np.float64)
+    d2 = ((real[:, None] - real[None]) ** 2).sum(-1)
+    np.fill_diagonal(d2, 1.0)
+    assert d2.min() > (0.85 * 0.025) ** 2 * (1 - 1e-5)
+
+
+# ---------------------------------------------------------------------------
+# Index build KATs (ImageTermKNNFetcher.cu:56-88, Node2TermsIndex.cu:6-121,
+# NodePair2TermsIndex.cu:11-193)
+# ---------------------------------------------------------------------------
+def test_compact_pixels_kat(orc):
+    from starhub_b200.scenes import Camera
+
+    class S:
+        pass
+    s = S()
+    s.camera = Camera(4, 3, 1, 1, 0, 0)
+    idx = np.full((3, 4), 0xFFFFFFFF, np.uint32)
+    idx[0, 1] = 2
+    idx[1, 0] = 0
+    idx[2, 3] = 1
+    s.index_map = idx
+    flow = np.zeros((3, 4, 2), np.float32)
+    flow[0, 1] = [0.5, 1.5]      # 1.5 -> 2 (ties to even), 1.5 -> 2
+    flow[1, 0] = [-3.0, 0.49]    # negative saturates to 0; 1.49 -> 1
+    flow[2, 3] = [2.5, -0.5]     # 5.5 -> 6, 1.5 -> 2
+    s.flow = flow
+    s.surfel_knn = np.array([[0, 1, 2, 3], [4, 5, 6, 7], [8, 9, 10, 11]], np.uint16)
+    s.surfel_sw = np.arange(12, dtype=np.float32).reshape(3, 4)
+    s.surfel_cw = np.ones((3, 4), np.float32)
+    pix, knn, sw, cw = orc.compact_pixels(s)
+    np.testing.assert_array_equal(pix, [[1, 0, 2, 2], [0, 1, 0, 1], [3, 2, 6, 2]])
+    np.testing.assert_array_equal(knn, s.surfel_knn[[2, 0, 1]])
+    np.testing.assert_array_equal(sw, s.surfel_sw[[2, 0, 1]])
+
+
+def test_node2term_kat(orc):
+    dense = np.array([[0, 1, 2, 3], [2, 3, 4, 1]], np.uint16)
+    edges = np.array([[0, 0, 0], [0, 4, 1], [2, 3, 1]], np.uint16)
+    off, ti = orc.node2term(dense, edges, 5)
+    # term ids: dense 0,1 | reg 2,3,4 | node-motion 5..9 ; self edge 2 -> invalid keys at the end
+    expect = {0: [0, 3, 5], 1: [0, 1, 6], 2: [0, 1, 4, 7], 3: [0, 1, 4, 8], 4: [1, 3, 9]}
+    for n, lst in expect.items():
+        assert list(ti[off[n]:off[n + 1]]) == lst
+    assert off[5] == sum(len(v) for v in expect.values())
+    assert list(ti[off[5]:]) == [2, 2]
+
+
+def test_nodepair2term_kat(orc):
+    dense = np.array([[3, 1, 2, 0], [2, 3, 4, 1]], np.uint16)
+    edges = np.array([[0, 0, 0], [4, 0, 1], [1, 3, 1]], np.uint16)
+    m = orc.nodepair2term(dense, edges, 5)
+    pairs = list(zip(m["half_rows"], m["half_cols"]))
+    # dense 0 -> (1,3),(2,3),(0,3),(1,2),(0,1),(0,2); dense 1 -> (2,3),(2,4),(3,4),(1,2),(1,3),(1,4)
+    # reg: (0,4) term 3, (1,3) term 4, self edge term 2 -> no pair
+    expect = {(0, 1): [0], (0, 2): [0], (0, 3): [0], (0, 4): [3], (1, 2): [0, 1], (1, 3): [0, 1, 4],
+              (1, 4): [1], (2, 3): [0, 1], (2, 4): [1], (3, 4): [1]}
+    assert pairs == sorted(expect)
+    for k, (b, e) in enumerate(zip(m["half_begin"], m["half_end"])):
+        assert list(m["term_index"][b:e]) == expect[pairs[k]]
+    sym = list(zip(m["sym_rows"], m["sym_cols"]))
+    assert sym == sorted(sym) and len(sym) == 2 * len(pairs)
+    assert list(m["blkrow_offset"]) == [0, 4, 8, 12, 16, 20]
+
+
+def test_binblock_csr_structure(orc):
+    m = orc.nodepair2term(np.array([[0, 1, 2, 3]], np.uint16), np.zeros((0, 3), np.uint16), 4)
+    rp, col = orc.binblock_csr(4, m["sym_rows"], m["sym_cols"])
+    # 24 scalar rows in one bin; every block row has 4 blocks -> bin length 24, 32 rows * 24 entries
+    assert list(rp[:33]) == list(range(32)) + [32 * 24]
+    nblk = rp[32] // 6
+    used = col[:nblk]
+    # row 0 of block-row 0 lists the diagonal (0) then columns 6, 12, 18
+    assert [used[0 + 32 * s] for s in range(4)] == [0, 6, 12, 18]
+    assert [used[6 + 32 * s] for s in range(4)] == [6, 0, 12, 18]
+    assert (used[24:32] == -1).all()
+
+
+# ---------------------------------------------------------------------------
+# Solve properties
+# ---------------------------------------------------------------------------
+def test_aligned_scene_gives_identity(orc, tiny_scene):
+    """Measurement equal to the rendered reference: zero residuals, zero step."""
+    import dataclasses
+    sc = dataclasses.replace(tiny_scene, meas_vertex=tiny_scene.ref_vertex.copy(),
+                             meas_normal=tiny_scene.ref_normal.copy())
+    dq = orc.solve(sc, gn_iters=3, pcg_iters=10)
+    ident = np.tile(np.array([0, 0, 0, 1, 0, 0, 0, 0], np.float32), (sc.num_nodes, 1))
+    np.testing.assert_allclose(dq, ident, atol=1e-6)
+
+
+def test_system_symmetric_and_preconditioner(orc, tiny_scene):
+    _, info = orc.solve(tiny_scene, gn_iters=1, pcg_iters=10, debug=True)
+    rows, cols, off = info["sym_rows"], info["sym_cols"], info["offdiag"].reshape(-1, 6, 6)
+    lookup = {(r, c): k for k, (r, c) in enumerate(zip(rows, cols))}
+    for k, (r, c) in enumerate(zip(rows, cols)):
+        np.testing.assert_allclose(off[k], off[lookup[(c, r)]].T, rtol=1e-5, atol=1e-9)
+    D = info["diag"].reshape(-1, 6, 6)
+    M = info["inv_diag"].reshape(-1, 6, 6)
+    eye = np.einsum("nij,njk->nik", D.astype(np.float64), M.astype(np.float64))
+    np.testing.assert_allclose(eye, np.broadcast_to(np.eye(6), eye.shape), atol=2e-3)
+    assert (np.diagonal(D, axis1=1, axis2=2) >= 1e-3 * (1 - 1e-6)).all()
+
+
+def test_fp32_reference_mode_close_to_fp64(orc, tiny_scene):
+    from starhub_b200.scenes import twist_error
+    d64 = orc.solve(tiny_scene, precision=orc.ORC_PREC_FP64)
+    d32 = orc.solve(tiny_scene, precision=orc.ORC_PREC_FP32_REFERENCE)
+    assert twist_error(d32, d64) < 5e-3
