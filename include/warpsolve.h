@@ -174,6 +174,18 @@ int ws_splat_maps(const float *verts, const float *attr_verts, const float *attr
                   int footprint, uint32_t *index_map, float *vertex_map, float *normal_map,
                   void *stream);
 
+/* ---- Measurement hooks ---- */
+
+/* Enables (1) or disables (0) per-phase CUDA-event timing of ws_solve on the solve stream
+ * (disabled inside graph capture).  Phases: 0 index build, 1 term evaluation, 2 diagonal
+ * blocks + right-hand side, 3 off-diagonal blocks, 4 persistent PCG + warp update. */
+int ws_set_profiling(ws_solver *solver, int enable);
+/* Milliseconds per phase of the last profiled solve, summed over its Gauss-Newton
+ * iterations (synchronises).  `launches` (optional) gets the launches of each phase. */
+int ws_get_phase_times(ws_solver *solver, float *ms, int *launches, int capacity, int *count);
+/* Kernel launches in one replay of the graph captured by ws_solve_graph. */
+int ws_graph_kernel_count(ws_solver *solver, int *count);
+
 /* Library version / build identification. */
 int ws_version(void);
 const char *ws_error_string(int status);

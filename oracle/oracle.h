@@ -56,6 +56,8 @@ typedef struct orc_problem {
 enum {
     ORC_PREC_FP64 = 0,              /* everything in double: the accuracy oracle */
     ORC_PREC_FP32_REFERENCE = 1,    /* float everywhere, Gauss-Jordan inverse, float dots */
+    ORC_PREC_MIXED = 2,             /* float bulk with double dots, double block accumulation and
+                                       Cholesky, cancellation-free residuals: the device's design */
 };
 
 typedef struct orc_settings {

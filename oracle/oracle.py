@@ -18,6 +18,7 @@ LIB = HERE / "_build" / "liboracle.so"
 
 ORC_PREC_FP64 = 0
 ORC_PREC_FP32_REFERENCE = 1
+ORC_PREC_MIXED = 2
 
 
 def build() -> Path:
@@ -181,10 +182,13 @@ def problem_from_scene(scene, keep):
 
 
 def solve(scene, precision=ORC_PREC_FP64, gn_iters=None, pcg_iters=None, threads=0, debug=False,
-          lambda_reg=None):
+          lambda_reg=None, init_dq=None):
     """Runs the CPU restatement of the full solve (index build + GN loop)."""
     keep = {}
     p = problem_from_scene(scene, keep)
+    if init_dq is not None:
+        keep["init"] = _c(init_dq, np.float32)
+        p.init_dq = _p(keep["init"])
     s = OrcSettings()
     s.gn_iters = scene.gn_iters if gn_iters is None else gn_iters
     s.pcg_iters = scene.pcg_iters if pcg_iters is None else pcg_iters

@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -508,8 +509,12 @@ DenseTerms compact_pixels(int W, int H, const uint32_t *index_map, const float *
     return d;
 }
 
-template <class R>
+// R: bulk arithmetic (terms, assembly, SpMV, vectors); RD: PCG dot products, alpha/beta,
+// diagonal-block accumulation and the block inverse (Cholesky when RD is double,
+// the reference's Gauss-Jordan when RD is float).
+template <class R, class RD = R>
 struct Solver {
+    static constexpr bool kMixed = !std::is_same<R, RD>::value;
     const orc_problem &p;
     const orc_settings &s;
     int threads;
@@ -521,12 +526,37 @@ struct Solver {
     std::vector<DQ<R>> se3;
     // per-iteration term data
     std::vector<R> d_res, d_grad;       // 3, 18 per dense term
-    std::vector<V3<R>> ti_xj, tj_xj;
+    std::vector<V3<R>> ti_xj, tj_xj, reg_res;
     std::vector<uint8_t> valid;
     std::vector<R> cweight;
     std::vector<V3<R>> node_t;
+    std::vector<V3<R>> center;      // twist centre per node (origin unless node-centred)
+
+    // eps * S^T S for the centre c: [[(1 + |c|^2) I - c c^T, -[c]x], [[c]x, I]] * eps, eps = 1e-3.
+    static void centred_regulariser(const V3<R> &cc, RD *out) {
+        const RD eps = RD(1e-3f);
+        const RD c[3] = {RD(cc.x), RD(cc.y), RD(cc.z)};
+        const RD c2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+        const RD X[3][3] = {{0, -c[2], c[1]}, {c[2], 0, -c[0]}, {-c[1], c[0], 0}};   // [c]x
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                out[6 * a + b] = eps * ((a == b ? RD(1) + c2 : RD(0)) - c[a] * c[b]);
+                out[6 * a + 3 + b] = -eps * X[a][b];
+                out[6 * (3 + a) + b] = eps * X[a][b];
+                out[6 * (3 + a) + 3 + b] = (a == b) ? eps : RD(0);
+            }
+    }
+
+    // Rotation part of a Jacobian row for a twist taken about `c` instead of the origin:
+    // rho - c x tau (the translation part tau is unchanged).
+    static void recentre(R *row6, const V3<R> &c) {
+        const V3<R> tau = {row6[3], row6[4], row6[5]};
+        const V3<R> ct = cross(c, tau);
+        row6[0] -= ct.x; row6[1] -= ct.y; row6[2] -= ct.z;
+    }
     // system
     std::vector<R> diag, inv_diag, b, offdiag, x;
+    std::vector<RD> diag_acc;
 
     Solver(const orc_problem &p_, const orc_settings &s_) : p(p_), s(s_) { threads = set_threads(s.threads); }
 
@@ -596,11 +626,17 @@ struct Solver {
             const V3<R> tnw = w2c.rot.tmul(tn);
             R *res = &d_res[3 * t];
             R *g = &d_grad[18 * t];
-            res[0] = dot(tnw, vw - tvw);
+            V3<R> diff = vw - tvw;
+            if (kMixed) {
+                // (R - I) v_ref + t + (v_ref - v_t): the device kernel's cancellation-free form
+                M33<R> Rmi = T.rot;
+                for (int a = 0; a < 3; ++a) Rmi.m[a][a] = T.rot.m[a][a] - R(1);
+                diff = (Rmi.mul(cv) + T.trans) + (cv - tvw);
+            }
+            res[0] = dot(tnw, diff);
             const V3<R> gr = cross(vw, tnw);
             g[0] = gr.x; g[1] = gr.y; g[2] = gr.z; g[3] = tnw.x; g[4] = tnw.y; g[5] = tnw.z;
             // modified optical flow: e = (P R_w2c)(v_w - v_t), P = first two rows
-            const V3<R> diff = vw - tvw;
             const V3<R> row0 = {w2c.rot.m[0][0], w2c.rot.m[0][1], w2c.rot.m[0][2]};
             const V3<R> row1 = {w2c.rot.m[1][0], w2c.rot.m[1][1], w2c.rot.m[1][2]};
             const R ex = dot(row0, diff), ey = dot(row1, diff);
@@ -620,7 +656,7 @@ struct Solver {
 
     // forwardWarpSmootherNodeKernel (examples/mono_star/opt/NodeGraphHandler.cu:7-45).
     void eval_reg() {
-        ti_xj.resize(ne); tj_xj.resize(ne); valid.resize(ne); cweight.resize(ne);
+        ti_xj.resize(ne); tj_xj.resize(ne); reg_res.resize(ne); valid.resize(ne); cweight.resize(ne);
         for (uint32_t e = 0; e < ne; ++e) {
             const uint16_t i = p.edges[3 * e], j = p.edges[3 * e + 1], k = p.edges[3 * e + 2];
             const float *xi = p.node_coords + 4 * i, *xj = p.node_coords + 4 * j;
@@ -628,6 +664,13 @@ struct Solver {
             const V3<R> vj = {R(xj[0]), R(xj[1]), R(xj[2])};
             ti_xj[e] = Ti.rot.mul(vj) + Ti.trans;
             tj_xj[e] = Tj.rot.mul(vj) + Tj.trans;
+            {
+                M33<R> dR;
+                for (int a = 0; a < 3; ++a)
+                    for (int c = 0; c < 3; ++c)
+                        dR.m[a][c] = (Ti.rot.m[a][c] - (a == c ? R(1) : R(0))) - (Tj.rot.m[a][c] - (a == c ? R(1) : R(0)));
+                reg_res[e] = dR.mul(vj) + (Ti.trans - Tj.trans);
+            }
             const float dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
             // squared_norm_xyz(xi - xj) > 64 * r^2, float (CLIP_FARAWAY_NODEGRAPH_PAIR)
             const float d2 = sq3_fused(dx, dy, dz);
@@ -636,7 +679,16 @@ struct Solver {
         }
         // ComputeNodeMotionKernel (NodeMotionHandler.cu:9-19)
         node_t.resize(nn);
-        for (uint32_t n = 0; n < nn; ++n) node_t[n] = dq_se3(se3[n]).trans;
+        center.assign(nn, V3<R>{0, 0, 0});
+        for (uint32_t n = 0; n < nn; ++n) {
+            const SE3<R> T = dq_se3(se3[n]);
+            node_t[n] = T.trans;
+            // node-centred twist coordinates (mixed mode): centre = current warped node position
+            if (kMixed) {
+                const float *x = p.node_coords + 4ull * n;
+                center[n] = T.rot.mul(V3<R>{R(x[0]), R(x[1]), R(x[2])}) + T.trans;
+            }
+        }
     }
 
     // Weight of node `node` in dense term t: the last matching knn slot
@@ -679,12 +731,14 @@ struct Solver {
     // computeJtResidualWithIndexKernel (JtDotResidualIndexed.cu:40-149).
     void assemble_node() {
         diag.assign(36ull * nn, R(0));
+        diag_acc.assign(36ull * nn, RD(0));
         b.assign(6ull * nn, R(0));
         R lam2[3], reg2, node2;
         lambdas(lam2, reg2, node2);
 #pragma omp parallel for num_threads(threads) schedule(dynamic, 16)
         for (long long node = 0; node < (long long)nn; ++node) {
-            R D[36] = {0}, bb[6] = {0};
+            RD D[36] = {0};
+            R bb[6] = {0};
             for (uint32_t it = n2t.offset[node]; it < n2t.offset[node + 1]; ++it) {
                 const uint32_t term = n2t.term_index[it];
                 if (term < off.dense) {
@@ -693,12 +747,15 @@ struct Solver {
                     const R *g = &d_grad[18ull * t];
                     const R *r = &d_res[3ull * t];
                     for (int ch = 0; ch < 3; ++ch) {
+                        R gl[6];
+                        for (int q = 0; q < 6; ++q) gl[q] = g[6 * ch + q];
+                        if (kMixed) recentre(gl, center[node]);
                         R J[6];
-                        for (int q = 0; q < 6; ++q) J[q] = g[6 * ch + q] * w;
-                        for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) D[6 * a + c] += (lam2[ch] * J[a]) * J[c];
+                        for (int q = 0; q < 6; ++q) J[q] = gl[q] * w;
+                        for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) D[6 * a + c] += RD(lam2[ch] * J[a]) * RD(J[c]);
                         // quirk kept: the right-hand side weights the dense term by w^2
                         const R ow = lam2[ch] * (w * w);
-                        for (int q = 0; q < 6; ++q) bb[q] -= ow * r[ch] * g[6 * ch + q];
+                        for (int q = 0; q < 6; ++q) bb[q] -= ow * r[ch] * gl[q];
                     }
                 } else if (term < off.reg) {
                     const uint32_t e = term - off.dense;
@@ -706,20 +763,33 @@ struct Solver {
                     const bool is_i = ((uint32_t)node == p.edges[3 * e]);
                     R J[3][6];
                     reg_jacobian(e, is_i, J);
+                    if (kMixed) for (int ch = 0; ch < 3; ++ch) recentre(J[ch], center[node]);
                     for (int ch = 0; ch < 3; ++ch)
-                        for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) D[6 * a + c] += (reg2 * J[ch][a]) * J[ch][c];
+                        for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) D[6 * a + c] += RD(reg2 * J[ch][a]) * RD(J[ch][c]);
                     // computeRegTermJtResidual (node_graph_reg_jacobian.cuh:193-233)
-                    const V3<R> rr = ti_xj[e] - tj_xj[e];
+                    const V3<R> rr = kMixed ? reg_res[e] : ti_xj[e] - tj_xj[e];
                     const R c2 = cweight[e] * cweight[e];
                     R Ju[3][6];
                     reg_jacobian_unit(e, is_i, Ju);
+                    if (kMixed) for (int ch = 0; ch < 3; ++ch) recentre(Ju[ch], center[node]);
                     const R res3[3] = {rr.x * c2, rr.y * c2, rr.z * c2};
                     for (int q = 0; q < 6; ++q) bb[q] -= reg2 * (res3[0] * Ju[0][q] + res3[1] * Ju[1][q] + res3[2] * Ju[2][q]);
                 } else if (term < off.node) {
                     const uint32_t n = term - off.reg;
                     const float *pred = p.node_motion_pred ? p.node_motion_pred + 4ull * n : nullptr;
                     const R conf = pred ? R(pred[3]) : R(0);
-                    for (int a = 0; a < 3; ++a) D[6 * (3 + a) + 3 + a] += node2 * conf * conf;
+                    if (kMixed && node2 != R(0) && pred) {
+                        for (int ch = 0; ch < 3; ++ch) {
+                            R J[6] = {0, 0, 0, 0, 0, 0};
+                            J[3 + ch] = conf;
+                            recentre(J, center[node]);
+                            for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) D[6 * a + c] += RD(node2 * J[a]) * RD(J[c]);
+                            const R res = (ch == 0 ? node_t[n].x - R(pred[0]) : ch == 1 ? node_t[n].y - R(pred[1]) : node_t[n].z - R(pred[2]));
+                            for (int q = 0; q < 6; ++q) bb[q] -= node2 * res * conf * J[q];
+                        }
+                        continue;
+                    }
+                    for (int a = 0; a < 3; ++a) D[6 * (3 + a) + 3 + a] += RD(node2 * conf * conf);
                     if (pred) {
                         const R c2 = conf * conf;
                         bb[3] -= node2 * (node_t[n].x - R(pred[0])) * c2;
@@ -730,8 +800,16 @@ struct Solver {
                     // feature term: zero Jacobian (PreconditionerRhsBuilder.cu:214-219)
                 }
             }
-            for (int a = 0; a < 6; ++a) D[7 * a] += R(1e-3f);
-            for (int q = 0; q < 36; ++q) diag[36 * node + q] = D[q];
+            if (kMixed) {
+                // the reference's +1e-3 I on the origin twist, seen in node-centred coordinates:
+                // 1e-3 S^T S with S = [[I, 0], [[c]x, I]]
+                RD reg[36];
+                centred_regulariser(center[node], reg);
+                for (int q = 0; q < 36; ++q) D[q] += reg[q];
+            } else {
+                for (int a = 0; a < 6; ++a) D[7 * a] += RD(1e-3f);
+            }
+            for (int q = 0; q < 36; ++q) { diag[36 * node + q] = R(D[q]); diag_acc[36 * node + q] = D[q]; }
             for (int q = 0; q < 6; ++q) b[6 * node + q] = bb[q];
         }
     }
@@ -755,7 +833,10 @@ struct Solver {
                     const R *g = &d_grad[18ull * term];
                     for (int ch = 0; ch < 3; ++ch) {
                         const R f = lam2[ch] * (wr * wc);
-                        for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) A[6 * a + c] += f * g[6 * ch + a] * g[6 * ch + c];
+                        R gr[6], gc[6];
+                        for (int q = 0; q < 6; ++q) gr[q] = gc[q] = g[6 * ch + q];
+                        if (kMixed) { recentre(gr, center[row]); recentre(gc, center[col]); }
+                        for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) A[6 * a + c] += f * gr[a] * gc[c];
                     }
                 } else if (term < off.reg) {
                     const uint32_t e = term - off.dense;
@@ -765,6 +846,7 @@ struct Solver {
                     R Jr[3][6], Jc[3][6];
                     reg_jacobian_unit(e, row == p.edges[3 * e], Jr);
                     reg_jacobian_unit(e, col == p.edges[3 * e], Jc);
+                    if (kMixed) for (int ch = 0; ch < 3; ++ch) { recentre(Jr[ch], center[row]); recentre(Jc[ch], center[col]); }
                     const R ws = reg2 * (cweight[e] * cweight[e]);
                     for (int ch = 0; ch < 3; ++ch)
                         for (int a = 0; a < 6; ++a) for (int c = 0; c < 6; ++c) A[6 * a + c] += (ws * Jr[ch][a]) * Jc[ch][c];
@@ -804,7 +886,8 @@ struct Solver {
     }
 
     // Symmetric 6x6 inverse by Cholesky in double (the FP64 block inversion).
-    static void cholesky_inverse(const R *in, R *out) {
+    template <class T>
+    static void cholesky_inverse(const T *in, R *out) {
         double L[36] = {0};
         for (int i = 0; i < 6; ++i)
             for (int j = 0; j <= i; ++j) {
@@ -834,7 +917,7 @@ struct Solver {
         inv_diag.assign(36ull * nn, R(0));
 #pragma omp parallel for num_threads(threads) schedule(static)
         for (long long n = 0; n < (long long)nn; ++n) {
-            if (s.precision == ORC_PREC_FP64) cholesky_inverse(&diag[36 * n], &inv_diag[36 * n]);
+            if (std::is_same<RD, double>::value) cholesky_inverse(&diag_acc[36 * n], &inv_diag[36 * n]);
             else gauss_jordan_inverse(&diag[36 * n], &inv_diag[36 * n]);
         }
     }
@@ -868,10 +951,10 @@ struct Solver {
         }
     }
 
-    R vdot(const std::vector<R> &a, const std::vector<R> &bv) const {
-        R acc = 0;
+    RD vdot(const std::vector<R> &a, const std::vector<R> &bv) const {
+        RD acc = 0;
 #pragma omp parallel for num_threads(threads) reduction(+ : acc) schedule(static)
-        for (long long i = 0; i < (long long)a.size(); ++i) acc += a[i] * bv[i];
+        for (long long i = 0; i < (long long)a.size(); ++i) acc += RD(a[i]) * RD(bv[i]);
         return acc;
     }
 
@@ -882,16 +965,16 @@ struct Solver {
         x.assign(n6, R(0));
         std::vector<R> r = b, d(n6), q(n6), t(n6), sv(n6);
         precond(r, d);
-        R delta = vdot(r, d);
+        RD delta = vdot(r, d);
         for (int it = 0; it < s.pcg_iters; ++it) {
             spmv(d, q);
-            const R dq = vdot(d, q);
-            const R alpha = (dq != R(0)) ? delta / dq : R(0);
+            const RD dq = vdot(d, q);
+            const R alpha = R((dq != RD(0)) ? delta / dq : RD(0));
             for (size_t i = 0; i < n6; ++i) { x[i] += alpha * d[i]; t[i] = r[i] - alpha * q[i]; }
             precond(t, sv);
-            const R delta_old = delta;
+            const RD delta_old = delta;
             delta = vdot(t, sv);
-            const R beta = (delta_old != R(0)) ? delta / delta_old : R(0);
+            const R beta = R((delta_old != RD(0)) ? delta / delta_old : RD(0));
             for (size_t i = 0; i < n6; ++i) d[i] = sv[i] + beta * d[i];
             r.swap(t);
         }
@@ -900,7 +983,14 @@ struct Solver {
     // ApplyWarpFieldUpdateKernel (SolverIterationData.cu:19-74).
     void update() {
         for (uint32_t n = 0; n < nn; ++n) {
-            const SE3<R> inc = twist_to_se3(&x[6ull * n]);
+            R xo[6];
+            for (int q = 0; q < 6; ++q) xo[q] = x[6ull * n + q];
+            if (kMixed) {
+                // local twist about c -> origin twist: t = t' + c x w
+                const V3<R> cw = cross(center[n], V3<R>{xo[0], xo[1], xo[2]});
+                xo[3] += cw.x; xo[4] += cw.y; xo[5] += cw.z;
+            }
+            const SE3<R> inc = twist_to_se3(xo);
             const SE3<R> prev = dq_to_mat34(se3[n]);
             SE3<R> nw;
             nw.rot = matmul(inc.rot, prev.rot);
@@ -1192,6 +1282,9 @@ int orc_solve(const orc_problem *p, const orc_settings *s, float *out_dq, orc_de
     if (p->num_nodes <= 0) return -2;
     if (s->precision == ORC_PREC_FP64) {
         Solver<double> sv(*p, *s);
+        sv.run(out_dq, dbg);
+    } else if (s->precision == ORC_PREC_MIXED) {
+        Solver<float, double> sv(*p, *s);
         sv.run(out_dq, dbg);
     } else {
         Solver<float> sv(*p, *s);

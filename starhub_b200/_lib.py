@@ -30,7 +30,7 @@ EXPORTED = [
     "ws_solve_graph", "ws_sync_status", "ws_get_solution", "ws_get_counts", "ws_get_dense_terms",
     "ws_get_node2term", "ws_get_node_pairs", "ws_get_system", "ws_get_dense_jacobian", "ws_init_nodes",
     "ws_build_node_graph", "ws_skinning", "ws_forward_warp", "ws_splat_maps", "ws_version",
-    "ws_error_string",
+    "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
 ]
 
 
@@ -106,6 +106,9 @@ def load() -> C.CDLL:
         "ws_splat_maps": (i, [vp, vp, vp, i, i, i, f, f, f, f, i, vp, vp, vp, vp]),
         "ws_version": (i, []),
         "ws_error_string": (C.c_char_p, [i]),
+        "ws_set_profiling": (i, [vp, i]),
+        "ws_get_phase_times": (i, [vp, vp, vp, i, pi]),
+        "ws_graph_kernel_count": (i, [vp, pi]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -36,12 +36,14 @@ void free_all(ws::Workspace &w) {
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
                     w.col_key_alt, w.col_val_alt, w.colidx, w.blocks, w.inv_diag, w.jtr, w.x, w.r, w.s, w.q,
-                    w.d0, w.d1, w.se3, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
+                    w.d0, w.d1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
                     w.error_flag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (w.graph_exec) cudaGraphExecDestroy(w.graph_exec);
     if (w.h_tables) cudaFreeHost(w.h_tables);
+    for (cudaEvent_t e : w.prof_events) cudaEventDestroy(e);
+    if (w.tables_free) cudaEventDestroy(w.tables_free);
 }
 
 // Rigid inverse of a row-major 4x4 camera-to-world transform.  The reference
@@ -185,6 +187,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.inv_diag, (size_t)w.cap_nodes * 36));
     for (float **v : {&w.jtr, &w.x, &w.r, &w.s, &w.q, &w.d0, &w.d1}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
     A(dalloc(&w.se3, (size_t)w.cap_nodes * 8));
+    A(dalloc(&w.centers, w.cap_nodes));
     A(dalloc(&w.chunk_partial, w.cap_chunks));
     A(dalloc(&w.scene_scalars, 8ull * w.cap_scenes));
     A(dalloc(&w.scene_counter, 2ull * w.cap_scenes));
@@ -192,6 +195,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.error_flag, 4));
     w.h_tables_bytes = sizeof(ws::Scene) * w.cap_scenes + 4ull * (w.cap_tiles + w.cap_nodes + w.cap_edges + 2ull * w.cap_chunks);
     A(cudaMallocHost(&w.h_tables, w.h_tables_bytes));
+    A(cudaEventCreateWithFlags(&w.tables_free, cudaEventDisableTiming));
     if (e == cudaSuccess) {
         A(cudaMemset(w.error_flag, 0, 4 * sizeof(int)));
         A(cudaMemset(w.barrier, 0, 4 * sizeof(uint32_t)));
@@ -237,6 +241,12 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
         tiles > w.cap_tiles || chunks > w.cap_chunks)
         return WS_ERR_CAPACITY;
     // host tables, uploaded by the next solve from pinned memory
+    // the previous solve may still be copying these pinned tables to the device
+    if (w.tables_in_flight) {
+        cudaSetDevice(w.device);
+        if (cudaEventSynchronize(w.tables_free) != cudaSuccess) return WS_ERR_CUDA;
+        w.tables_in_flight = false;
+    }
     ws::Scene *hs = reinterpret_cast<ws::Scene *>(w.h_tables);
     uint32_t *tile_scene = reinterpret_cast<uint32_t *>(hs + w.cap_scenes);
     uint32_t *node_scene = tile_scene + w.cap_tiles;
@@ -322,6 +332,12 @@ int ws_set_inputs(ws_solver *h, const ws_inputs *in) { return ws_set_batch(h, in
 
 namespace {
 
+bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (st && cudaStreamIsCapturing(st, &cs) == cudaSuccess) return cs != cudaStreamCaptureStatusNone;
+    return false;
+}
+
 // Uploads the scene tables, initialises the warp, builds the index and runs the GN loop.
 cudaError_t enqueue_solve(ws::Workspace &w, int gn, int pcg, cudaStream_t st) {
     const ws::Scene *hs = reinterpret_cast<const ws::Scene *>(w.h_tables);
@@ -339,13 +355,50 @@ cudaError_t enqueue_solve(ws::Workspace &w, int gn, int pcg, cudaStream_t st) {
     A(cudaMemcpyAsync(w.chunk_scene, chunk_scene, 4ull * w.total_chunks, cudaMemcpyHostToDevice, st));
     A(cudaMemcpyAsync(w.chunk_row, chunk_row, 4ull * w.total_chunks, cudaMemcpyHostToDevice, st));
     if (e != cudaSuccess) return e;
+    if (!capturing(st)) {
+        A(cudaEventRecord(w.tables_free, st));
+        w.tables_in_flight = true;
+    }
+    const bool prof = w.profiling && !capturing(st);
+    size_t ev = 0;
+    auto mark = [&](int phase) {
+        if (!prof) return;
+        if (ev >= w.prof_events.size()) {
+            cudaEvent_t x;
+            cudaEventCreate(&x);
+            w.prof_events.push_back(x);
+        }
+        cudaEventRecord(w.prof_events[ev], st);
+        if (ev >= w.prof_phase.size()) {
+            w.prof_phase.push_back(phase);
+            w.prof_launches.push_back(w.launches);
+        } else {
+            w.prof_phase[ev] = phase;
+            w.prof_launches[ev] = w.launches;
+        }
+        ++ev;
+        w.launches = 0;
+    };
+    w.launches = 0;
+    mark(-1);
     ws::init_warp(w, st);
     for (int s = 0; s < w.num_scenes; ++s)
         if (w.init_ptrs[s])
             A(cudaMemcpyAsync(w.se3 + 8ull * w.h_scenes[s].node_base, w.init_ptrs[s],
                               32ull * w.h_scenes[s].num_nodes, cudaMemcpyDeviceToDevice, st));
     ws::index_build(w, st);
-    for (int it = 0; it < gn && e == cudaSuccess; ++it) A(ws::gn_iteration(w, pcg, st));
+    mark(0);
+    for (int it = 0; it < gn && e == cudaSuccess; ++it) {
+        ws::gn_eval(w, st);
+        mark(1);
+        ws::gn_assemble_node(w, st);
+        mark(2);
+        ws::gn_assemble_pair(w, st);
+        mark(3);
+        A(ws::gn_pcg(w, pcg, st));
+        mark(4);
+    }
+    w.prof_count = prof ? (int)ev : 0;
     A(cudaGetLastError());
     return e;
 }
@@ -397,6 +450,16 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
             cudaGetLastError();
             return WS_ERR_CUDA;
         }
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+        int kernels = 0;
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        w.graph_kernels = kernels;
         const cudaError_t e3 = cudaGraphInstantiate(&w.graph_exec, g, 0);
         cudaGraphDestroy(g);
         if (e3 != cudaSuccess) {
@@ -408,8 +471,47 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
         w.graph_init = w.init_ptrs;
     }
     if (cudaGraphLaunch(w.graph_exec, st) != cudaSuccess) return WS_ERR_CUDA;
+    // the replay's first nodes copy the pinned tables; the tables are free once the replay ends
+    if (cudaEventRecord(w.tables_free, st) != cudaSuccess) return WS_ERR_CUDA;
+    w.tables_in_flight = true;
     w.have_solution = true;
     return WS_OK;
+}
+
+int ws_set_profiling(ws_solver *h, int enable) {
+    if (!h) return WS_ERR_INVALID_ARGUMENT;
+    h->w.profiling = enable != 0;
+    return WS_OK;
+}
+
+int ws_get_phase_times(ws_solver *h, float *ms, int *launches, int cap, int *count) {
+    if (!h || !count) return WS_ERR_INVALID_ARGUMENT;
+    ws::Workspace &w = h->w;
+    *count = ws::Workspace::kPhases;
+    if (w.prof_count < 2) return WS_ERR_NOT_READY;
+    if (cap < ws::Workspace::kPhases) return WS_ERR_CAPACITY;
+    cudaSetDevice(w.device);
+    if (cudaEventSynchronize(w.prof_events[w.prof_count - 1]) != cudaSuccess) return WS_ERR_CUDA;
+    for (int p = 0; p < ws::Workspace::kPhases; ++p) {
+        if (ms) ms[p] = 0.f;
+        if (launches) launches[p] = 0;
+    }
+    for (int i = 1; i < w.prof_count; ++i) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, w.prof_events[i - 1], w.prof_events[i]) != cudaSuccess) return WS_ERR_CUDA;
+        const int p = w.prof_phase[i];
+        if (p >= 0 && p < ws::Workspace::kPhases) {
+            if (ms) ms[p] += t;
+            if (launches) launches[p] += w.prof_launches[i];
+        }
+    }
+    return WS_OK;
+}
+
+int ws_graph_kernel_count(ws_solver *h, int *count) {
+    if (!h || !count) return WS_ERR_INVALID_ARGUMENT;
+    *count = h->w.graph_kernels;
+    return h->w.graph_exec ? WS_OK : WS_ERR_NOT_READY;
 }
 
 int ws_sync_status(ws_solver *h) {

@@ -17,7 +17,7 @@ namespace ws {
 
 constexpr int kVecStride = 8;        // floats per node in PCG vectors
 constexpr int kDenseRecord = 32;     // floats per dense-term record (128 B)
-constexpr int kRegRecord = 12;       // floats per reg-term record (48 B)
+constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------------------
@@ -127,6 +127,36 @@ __device__ __forceinline__ M33 quat_rot(float4 q) {
     r.m[2][1] = 2 * q.y * q.z + 2 * q.x * q.w;
     r.m[2][2] = 1 - 2 * q.x * q.x - 2 * q.y * q.y;
     return r;
+}
+
+// R - I of a unit quaternion, formed without subtracting 1 from near-1 diagonal terms.
+__device__ __forceinline__ M33 quat_rot_minus_identity(float4 q) {
+    M33 r;
+    r.m[0][0] = -2 * q.y * q.y - 2 * q.z * q.z;
+    r.m[0][1] = 2 * q.x * q.y - 2 * q.z * q.w;
+    r.m[0][2] = 2 * q.x * q.z + 2 * q.y * q.w;
+    r.m[1][0] = 2 * q.x * q.y + 2 * q.z * q.w;
+    r.m[1][1] = -2 * q.x * q.x - 2 * q.z * q.z;
+    r.m[1][2] = 2 * q.y * q.z - 2 * q.x * q.w;
+    r.m[2][0] = 2 * q.x * q.z - 2 * q.y * q.w;
+    r.m[2][1] = 2 * q.y * q.z + 2 * q.x * q.w;
+    r.m[2][2] = -2 * q.x * q.x - 2 * q.y * q.y;
+    return r;
+}
+
+// SE(3) with R - I kept beside R, so that differences of warped points of
+// about a metre can be formed from quantities of millimetres.
+struct SE3d { M33 rot, rot_mi; float3 t; };
+
+__device__ __forceinline__ SE3d dq_se3_split(DQf d) {
+    dq_normalize(d);
+    SE3d T;
+    T.rot = quat_rot(d.q0);
+    T.rot_mi = quat_rot_minus_identity(d.q0);
+    const float4 two_q1 = make_float4(2.f * d.q1.x, 2.f * d.q1.y, 2.f * d.q1.z, 2.f * d.q1.w);
+    const float4 tp = qmul(two_q1, qconj(d.q0));
+    T.t = make_float3(tp.x, tp.y, tp.z);
+    return T;
 }
 
 // DualQuaternion::se3_matrix (DualQuaternion.hpp:182-189).

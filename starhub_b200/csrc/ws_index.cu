@@ -395,18 +395,22 @@ void index_build(Workspace &w, cudaStream_t st) {
     // 1. compaction of potential pixels
     k_pixel_count<<<T, kPixTileThreads, 0, st>>>(w.scenes, w.tile_scene, T, w.tile_count);
     exclusive_scan(w.tile_count, w.tile_count, nullptr, (uint32_t)T, w.cap_tiles, w.scan_tmp, st);
+    count_launch(w, 1 + 3);
     k_plan<<<1, 32, 0, st>>>(w.scenes, S, w.tile_count, T, w.plan, w.counts, w.cap_n2t, w.cap_pair_kv, w.error_flag);
     k_pixel_compact<<<T, kPixTileThreads, 0, st>>>(w.scenes, w.tile_scene, T, w.tile_count, w.d_pixels, w.d_knn,
                                                    w.d_sw, w.d_cw, w.d_scene, w.cap_pixels, w.error_flag);
+    count_launch(w, 2);
     // 2. node -> term
     const uint32_t n2t_invalid = (1u << w.node_bits) - 1u;
     k_n2t_kv<<<grid_for(w.cap_n2t, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, S, w.counts, w.d_knn, w.n2t_key,
                                                                     w.n2t_val, n2t_invalid, w.error_flag);
     const bool n2t_alt = radix_sort<uint32_t>(w.n2t_key, w.n2t_val, w.n2t_key_alt, w.n2t_val_alt, w.counts + kCntN2T, 0,
                                               w.cap_n2t, w.node_bits, w.sort_hist, w.sort_digit, st);
+    count_launch(w, 1 + 3 * ((w.node_bits + 7) / 8));
     w.n2t_sorted_key = n2t_alt ? w.n2t_key_alt : w.n2t_key;
     w.n2t_sorted_val = n2t_alt ? w.n2t_val_alt : w.n2t_val;
     k_n2t_offsets<<<grid_for(N + 1, 256, w.num_sms), 256, 0, st>>>(w.n2t_sorted_key, w.counts, N, w.n2t_offset);
+    count_launch(w);
     // 3. node pair -> term
     const int pbits = 2 * w.node_bits;
     const unsigned long long pinvalid = (pbits >= 64) ? ~0ull : ((1ull << pbits) - 1ull);
@@ -416,6 +420,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     const bool pair_alt = radix_sort<unsigned long long>(w.pair_key, w.pair_val, w.pair_key_alt, w.pair_val_alt,
                                                          w.counts + kCntPairKV, 0, w.cap_pair_kv, pbits, w.sort_hist,
                                                          w.sort_digit, st);
+    count_launch(w, 1 + 3 * ((pbits + 7) / 8));
     w.pair_sorted_key = pair_alt ? w.pair_key_alt : w.pair_key;
     w.pair_sorted_val = pair_alt ? w.pair_val_alt : w.pair_val;
     const int pg = grid_for(w.cap_pair_kv, 256, w.num_sms);
@@ -427,6 +432,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     k_half_fill<<<pg, 256, 0, st>>>(w.pair_sorted_key, w.pair_head, w.counts, w.node_bits, w.cap_half,
                                     w.half_row, w.half_col, w.half_begin, w.half_end, w.row_cnt_up, w.row_cnt_lo,
                                     w.error_flag);
+    count_launch(w, 1 + 3 + 1);
     // 4. block CSR
     k_row_first<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_row, w.counts, w.row_first);
     k_row_len<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.row_cnt_up, w.row_cnt_lo, N, w.rowptr);
@@ -434,6 +440,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     k_col_kv<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_col, w.counts, w.col_key, w.col_val);
     const bool col_alt = radix_sort<uint32_t>(w.col_key, w.col_val, w.col_key_alt, w.col_val_alt, w.counts + kCntHalf,
                                               0, w.cap_half, w.node_bits, w.sort_hist, w.sort_digit, st);
+    count_launch(w, 1 + 1 + 3 + 1 + 3 * ((w.node_bits + 7) / 8));
     const uint32_t *scol = col_alt ? w.col_key_alt : w.col_key;
     const uint32_t *sh = col_alt ? w.col_val_alt : w.col_val;
     k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,
@@ -441,6 +448,7 @@ void index_build(Workspace &w, cudaStream_t st) {
                                                                     w.half_slot_up, w.half_slot_lo, w.colidx,
                                                                     w.error_flag);
     k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, N, w.cap_blocks, w.colidx, w.error_flag);
+    count_launch(w, 2);
 }
 
 }  // namespace ws

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const u
             avg.q1 = make_float4(avg.q1.x + w[k] * d.q1.x, avg.q1.y + w[k] * d.q1.y, avg.q1.z + w[k] * d.q1.z,
                                  avg.q1.w + w[k] * d.q1.w);
         }
-        const SE3f T = dq_se3(avg);
+        const SE3d T = dq_se3_split(avg);
         const ushort4 px = pixels[t];
         const size_t spix = (size_t)px.y * sc.pitch + px.x;
         const float4 cv4 = sc.rvert[spix], cn4 = sc.rnorm[spix];
@@ -96,11 +96,14 @@ __global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const u
             if (ok) {
                 const float3 tvw = tmul(W, tv - wt);   // apply_inversed_se3
                 const float3 tnw = tmul(W, tn);        // rot.transpose_dot
-                res[0] = dot3(tnw, vw - tvw);
+                // v_w - v_t = (R - I) v_ref + t + (v_ref - v_t): the same quantity as the
+                // reference's dot(n, v_w - v_t), without cancelling two ~1 m vectors in FP32
+                const float3 cv = f3(cv4.x, cv4.y, cv4.z);
+                const float3 diff = (mul(T.rot_mi, cv) + T.t) + (cv - tvw);
+                res[0] = dot3(tnw, diff);
                 const float3 rr = cross3(vw, tnw);
                 gr[0] = rr.x; gr[1] = rr.y; gr[2] = rr.z;
                 gr[3] = tnw.x; gr[4] = tnw.y; gr[5] = tnw.z;
-                const float3 diff = vw - tvw;
                 const float3 row0 = f3(W.m[0][0], W.m[0][1], W.m[0][2]);
                 const float3 row1 = f3(W.m[1][0], W.m[1][1], W.m[1][2]);
                 const float ex = dot3(row0, diff), ey = dot3(row1, diff);
@@ -133,8 +136,9 @@ __global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const u
 
 // ---------------------------------------------------------------------------
 // ARAP smoothness term (forwardWarpSmootherNodeKernel,
-// examples/mono_star/opt/NodeGraphHandler.cu:7-45).  Record (48 B):
-//   [0,3) Ti xj, [3,6) Tj xj, [6] connect weight, [7] validity, [8] i, [9] j (global ids).
+// examples/mono_star/opt/NodeGraphHandler.cu:7-45).  Record (64 B):
+//   [0,3) Ti xj, [3,6) Tj xj, [6] connect weight, [7] validity, [8] i, [9] j (global ids),
+//   [10,13) Ti xj - Tj xj evaluated without cancellation.
 // ---------------------------------------------------------------------------
 __global__ void k_eval_reg(const Scene *scenes, const uint32_t *edge_scene, uint32_t total_edges, const float *se3,
                            float *record) {
@@ -146,11 +150,18 @@ __global__ void k_eval_reg(const Scene *scenes, const uint32_t *edge_scene, uint
         const uint16_t i = min(sc.edges[3 * el], last), j = min(sc.edges[3 * el + 1], last);
         const uint16_t k = min(sc.edges[3 * el + 2], (uint16_t)(sc.graph_k - 1));
         const float4 xi = sc.node_coords[i], xj = sc.node_coords[j];
-        const SE3f Ti = dq_se3(load_dq(se3 + 8ull * (sc.node_base + i)));
-        const SE3f Tj = dq_se3(load_dq(se3 + 8ull * (sc.node_base + j)));
+        const SE3d Ti = dq_se3_split(load_dq(se3 + 8ull * (sc.node_base + i)));
+        const SE3d Tj = dq_se3_split(load_dq(se3 + 8ull * (sc.node_base + j)));
         const float3 vj = f3(xj.x, xj.y, xj.z);
         const float3 a = mul(Ti.rot, vj) + Ti.t;
         const float3 b = mul(Tj.rot, vj) + Tj.t;
+        // Ti xj - Tj xj = ((Ri - I) - (Rj - I)) xj + (ti - tj), free of cancellation
+        M33 dR;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) dR.m[r][q] = Ti.rot_mi.m[r][q] - Tj.rot_mi.m[r][q];
+        const float3 rij = mul(dR, vj) + (Ti.t - Tj.t);
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
         const float valid = (d2 > 64 * sc.node_r2) ? 0.f : 1.f;   // CLIP_FARAWAY_NODEGRAPH_PAIR
@@ -158,8 +169,33 @@ __global__ void k_eval_reg(const Scene *scenes, const uint32_t *edge_scene, uint
         float4 *out = reinterpret_cast<float4 *>(record + (size_t)kRegRecord * e);
         out[0] = make_float4(a.x, a.y, a.z, b.x);
         out[1] = make_float4(b.y, b.z, c, valid);
-        out[2] = make_float4(__uint_as_float(sc.node_base + i), __uint_as_float(sc.node_base + j), 0.f, 0.f);
+        out[2] = make_float4(__uint_as_float(sc.node_base + i), __uint_as_float(sc.node_base + j), rij.x, rij.y);
+        out[3] = make_float4(rij.z, 0.f, 0.f, 0.f);
     }
+}
+
+// Twist centre of every node for this Gauss-Newton iteration: the node's current warped
+// position.  The mixed-precision path solves for each node's twist about this centre
+// instead of the world origin (block-Jacobi PCG iterates are invariant under this
+// block-diagonal change of variables); the lever arm drops from ~1 m to a few cm,
+// which keeps the 6x6 blocks well conditioned in FP32.
+__global__ void k_node_centers(const Scene *scenes, const uint32_t *node_scene, uint32_t total_nodes,
+                               const float *se3, float4 *centers) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
+        const Scene &sc = scenes[node_scene[g]];
+        const float4 x = sc.node_coords[g - sc.node_base];
+        const SE3f T = dq_se3(load_dq(se3 + 8ull * g));
+        const float3 c = mul(T.rot, f3(x.x, x.y, x.z)) + T.t;
+        centers[g] = make_float4(c.x, c.y, c.z, 0.f);
+    }
+}
+
+// Rotation part of a Jacobian row for a twist about `c`: rho - c x tau.
+__device__ __forceinline__ void recentre(float *row, float3 c) {
+    const float3 ct = cross3(c, f3(row[3], row[4], row[5]));
+    row[0] -= ct.x;
+    row[1] -= ct.y;
+    row[2] -= ct.z;
 }
 
 // Reg Jacobian rows without the connect weight (libs/star/opt/node_graph_reg_jacobian.cuh:85-106).
@@ -211,12 +247,12 @@ __device__ void gauss_jordan6(const float *in, float *out) {
 }
 
 // Symmetric positive definite 6x6 inverse by Cholesky in FP64.
-__device__ void cholesky6_fp64(const float *in, float *out) {
+__device__ void cholesky6_fp64(const double *in, float *out) {
     double L[21];   // packed lower triangle, row i holds i+1 entries
 #define LI(i, j) L[(i) * ((i) + 1) / 2 + (j)]
     for (int i = 0; i < 6; ++i)
         for (int j = 0; j <= i; ++j) {
-            double s = (double)in[6 * i + j];
+            double s = in[6 * i + j];
             for (int k = 0; k < j; ++k) s -= LI(i, k) * LI(j, k);
             if (i == j) LI(i, i) = sqrt(s > 0.0 ? s : 1e-300);
             else LI(i, j) = s / LI(j, j);
@@ -249,12 +285,18 @@ __device__ void cholesky6_fp64(const float *in, float *out) {
 // computeJtResidualWithIndexKernel, JtDotResidualIndexed.cu:40-149).
 // Lane l takes list positions l, l+32, ...; a fixed butterfly combines lanes.
 // ---------------------------------------------------------------------------
+// DAcc is the accumulator type of the diagonal block: float for WS_PREC_FP32 (the reference's
+// FP32 reduction), double for WS_PREC_MIXED, where the block feeds the FP64 Cholesky directly
+// and is rounded to FP32 only for the SpMV.
+template <class DAcc>
 __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, const Plan *plan,
                                                         const uint32_t *node_scene, uint32_t total_nodes,
                                                         const uint32_t *n2t_offset, const uint32_t *n2t_val,
                                                         const float *drec, const float *rrec, const float *se3,
-                                                        const uint32_t *rowptr, uint32_t cap_blocks, float *blocks,
-                                                        float *inv_diag, float *jtr, int precision, int *err) {
+                                                        const float4 *centers, const uint32_t *rowptr,
+                                                        uint32_t cap_blocks, float *blocks, float *inv_diag, float *jtr,
+                                                        int *err) {
+    constexpr bool kFp64 = sizeof(DAcc) == 8;   // mixed precision: also node-centred twists
     const int lane = threadIdx.x & 31;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total_nodes; g += warps) {
@@ -265,11 +307,14 @@ __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, cons
         const float lam2[3] = {sc.lam_depth * sc.lam_depth, sc.lam_of * sc.lam_of, sc.lam_of * sc.lam_of};
         const float reg2 = sc.lam_reg * sc.lam_reg;
         const float node2 = sc.lam_node * sc.lam_node;
-        float D[21], b[6];
+        DAcc D[21];
+        float b[6];
 #pragma unroll
-        for (int i = 0; i < 21; ++i) D[i] = 0.f;
+        for (int i = 0; i < 21; ++i) D[i] = DAcc(0);
 #pragma unroll
         for (int i = 0; i < 6; ++i) b[i] = 0.f;
+        const float4 c4 = centers[g];
+        const float3 cen = f3(c4.x, c4.y, c4.z);
         const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
         for (uint32_t it = beg + lane; it < end; it += 32) {
             const uint32_t term = n2t_val[it];
@@ -289,26 +334,35 @@ __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, cons
                 const float w = wk[slot];
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) {
+                    float gl[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) gl[q] = gv[6 * ch + q];
+                    if (kFp64) recentre(gl, cen);
                     float J[6];
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) J[q] = gv[6 * ch + q] * w;
+                    for (int q = 0; q < 6; ++q) J[q] = gl[q] * w;
 #pragma unroll
                     for (int a = 0; a < 6; ++a)
 #pragma unroll
-                        for (int c = a; c < 6; ++c) D[tri_index(a, c)] += (lam2[ch] * J[a]) * J[c];
+                        for (int c = a; c < 6; ++c) D[tri_index(a, c)] += DAcc(lam2[ch] * J[a]) * DAcc(J[c]);
                     const float ow = lam2[ch] * (w * w);
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) b[q] -= (ow * res[ch]) * gv[6 * ch + q];
+                    for (int q = 0; q < 6; ++q) b[q] -= (ow * res[ch]) * gl[q];
                 }
             } else if (term < nd + ne) {
                 const float4 *rec = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * (sc.edge_base + term - nd));
-                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2];
+                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
                 if (r1.w == 0.f) continue;
                 const float3 a3 = f3(r0.x, r0.y, r0.z), b3 = f3(r0.w, r1.x, r1.y);
+                const float3 rij = f3(r2.z, r2.w, r3.x);
                 const float c = r1.z;
                 const bool is_i = (__float_as_uint(r2.x) == g);
                 float J[3][6];
                 reg_unit_jacobian(a3, b3, is_i, J);
+                if (kFp64) {
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) recentre(J[ch], cen);
+                }
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) {
                     float Jc[6];
@@ -317,11 +371,11 @@ __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, cons
 #pragma unroll
                     for (int a = 0; a < 6; ++a)
 #pragma unroll
-                        for (int cc = a; cc < 6; ++cc) D[tri_index(a, cc)] += (reg2 * Jc[a]) * Jc[cc];
+                        for (int cc = a; cc < 6; ++cc) D[tri_index(a, cc)] += DAcc(reg2 * Jc[a]) * DAcc(Jc[cc]);
                 }
                 // computeRegTermJtResidual (node_graph_reg_jacobian.cuh:193-233)
                 const float c2 = c * c;
-                const float rv[3] = {(a3.x - b3.x) * c2, (a3.y - b3.y) * c2, (a3.z - b3.z) * c2};
+                const float rv[3] = {rij.x * c2, rij.y * c2, rij.z * c2};
 #pragma unroll
                 for (int q = 0; q < 6; ++q) b[q] -= reg2 * (rv[0] * J[0][q] + rv[1] * J[1][q] + rv[2] * J[2][q]);
             } else if (term < nd + ne + nn) {
@@ -331,12 +385,28 @@ __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, cons
                     const float4 pred = sc.node_motion[nl];
                     const SE3f T = dq_se3(load_dq(se3 + 8ull * (sc.node_base + nl)));
                     const float conf = pred.w, c2 = pred.w * pred.w;
-                    D[tri_index(3, 3)] += (node2 * conf) * conf;
-                    D[tri_index(4, 4)] += (node2 * conf) * conf;
-                    D[tri_index(5, 5)] += (node2 * conf) * conf;
-                    b[3] -= node2 * ((T.t.x - pred.x) * c2);
-                    b[4] -= node2 * ((T.t.y - pred.y) * c2);
-                    b[5] -= node2 * ((T.t.z - pred.z) * c2);
+                    if (kFp64) {
+                        const float res3[3] = {T.t.x - pred.x, T.t.y - pred.y, T.t.z - pred.z};
+#pragma unroll
+                        for (int ch = 0; ch < 3; ++ch) {
+                            float J[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                            J[3 + ch] = conf;
+                            recentre(J, cen);
+#pragma unroll
+                            for (int a = 0; a < 6; ++a)
+#pragma unroll
+                                for (int c = a; c < 6; ++c) D[tri_index(a, c)] += DAcc(node2 * J[a]) * DAcc(J[c]);
+#pragma unroll
+                            for (int q = 0; q < 6; ++q) b[q] -= node2 * res3[ch] * conf * J[q];
+                        }
+                    } else {
+                        D[tri_index(3, 3)] += DAcc((node2 * conf) * conf);
+                        D[tri_index(4, 4)] += DAcc((node2 * conf) * conf);
+                        D[tri_index(5, 5)] += DAcc((node2 * conf) * conf);
+                        b[3] -= node2 * ((T.t.x - pred.x) * c2);
+                        b[4] -= node2 * ((T.t.y - pred.y) * c2);
+                        b[5] -= node2 * ((T.t.z - pred.z) * c2);
+                    }
                 }
             }
             // feature terms: zero Jacobian (PreconditionerRhsBuilder.cu:214-219)
@@ -345,14 +415,30 @@ __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, cons
         for (int i = 0; i < 21; ++i) D[i] = warp_sum(D[i]);
 #pragma unroll
         for (int i = 0; i < 6; ++i) b[i] = warp_sum(b[i]);
-        // full block with +1e-3 on the diagonal (PreconditionerRhsBuilder.cu:249-252)
+        // +1e-3 on the diagonal of the origin-twist block (PreconditionerRhsBuilder.cu:249-252);
+        // for node-centred twists the same term is 1e-3 S^T S, S = [[I, 0], [[c]x, I]]
+        if (kFp64) {
+            const DAcc eps = DAcc(1e-3f), cx = cen.x, cy = cen.y, cz = cen.z;
+            const DAcc c2 = cx * cx + cy * cy + cz * cz;
+            const DAcc cv[3] = {cx, cy, cz};
+            const DAcc X[3][3] = {{0, -cz, cy}, {cz, 0, -cx}, {-cy, cx, 0}};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+#pragma unroll
+                for (int c = a; c < 3; ++c) D[tri_index(a, c)] += eps * ((a == c ? DAcc(1) + c2 : DAcc(0)) - cv[a] * cv[c]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) D[tri_index(a, 3 + c)] += -eps * X[a][c];
+                D[tri_index(3 + a, 3 + a)] += eps;
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 6; ++a) D[tri_index(a, a)] += DAcc(1e-3f);
+        }
         float full[36];
 #pragma unroll
         for (int a = 0; a < 6; ++a)
 #pragma unroll
-            for (int c = 0; c < 6; ++c) full[6 * a + c] = (a <= c) ? D[tri_index(a, c)] : D[tri_index(c, a)];
-#pragma unroll
-        for (int a = 0; a < 6; ++a) full[7 * a] += 1e-3f;
+            for (int c = 0; c < 6; ++c) full[6 * a + c] = (float)((a <= c) ? D[tri_index(a, c)] : D[tri_index(c, a)]);
         const uint32_t slot = rowptr[g];
         if (slot < cap_blocks && lane < 9) {
             float4 v = make_float4(full[4 * lane], full[4 * lane + 1], full[4 * lane + 2], full[4 * lane + 3]);
@@ -368,8 +454,16 @@ __global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, cons
             for (int i = 0; i < 6; ++i) bad |= isnan(b[i]);
             if (bad) set_err(err, WS_ERR_NAN);
             float inv[36];
-            if (precision == WS_PREC_FP32) gauss_jordan6(full, inv);
-            else cholesky6_fp64(full, inv);
+            if (kFp64) {
+                double Dd[36];
+#pragma unroll
+                for (int a = 0; a < 6; ++a)
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) Dd[6 * a + c] = (double)((a <= c) ? D[tri_index(a, c)] : D[tri_index(c, a)]);
+                cholesky6_fp64(Dd, inv);
+            } else {
+                gauss_jordan6(full, inv);
+            }
             float4 *o = reinterpret_cast<float4 *>(inv_diag + 36ull * g);
 #pragma unroll
             for (int i = 0; i < 9; ++i) o[i] = make_float4(inv[4 * i], inv[4 * i + 1], inv[4 * i + 2], inv[4 * i + 3]);
@@ -388,7 +482,7 @@ __global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, cons
                                                         const uint32_t *half_begin, const uint32_t *half_end,
                                                         const uint32_t *pair_val, const uint32_t *slot_up,
                                                         const uint32_t *slot_lo, const float *drec, const float *rrec,
-                                                        float *blocks) {
+                                                        const float4 *centers, int centred, float *blocks) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nhalf = counts[kCntHalf];
@@ -403,6 +497,8 @@ __global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, cons
         float A[36];
 #pragma unroll
         for (int i = 0; i < 36; ++i) A[i] = 0.f;
+        const float4 cr4 = centers[row], cc4 = centers[col];
+        const float3 c_row = f3(cr4.x, cr4.y, cr4.z), c_col = f3(cc4.x, cc4.y, cc4.z);
         for (uint32_t it = half_begin[h] + lane; it < half_end[h]; it += 32) {
             const uint32_t term = pair_val[it];
             if (term < nd) {
@@ -424,11 +520,18 @@ __global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, cons
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) {
                     const float f = lam2[ch] * wij;
+                    float gr[6], gc[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) gr[q] = gc[q] = gv[6 * ch + q];
+                    if (centred) {
+                        recentre(gr, c_row);
+                        recentre(gc, c_col);
+                    }
 #pragma unroll
                     for (int a = 0; a < 6; ++a) {
-                        const float fa = f * gv[6 * ch + a];
+                        const float fa = f * gr[a];
 #pragma unroll
-                        for (int c = 0; c < 6; ++c) A[6 * a + c] += fa * gv[6 * ch + c];
+                        for (int c = 0; c < 6; ++c) A[6 * a + c] += fa * gc[c];
                     }
                 }
             } else if (term < nd + ne) {
@@ -442,6 +545,13 @@ __global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, cons
                 float Jr[3][6], Jc[3][6];
                 reg_unit_jacobian(a3, b3, row == ei, Jr);
                 reg_unit_jacobian(a3, b3, col == ei, Jc);
+                if (centred) {
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) {
+                        recentre(Jr[ch], c_row);
+                        recentre(Jc[ch], c_col);
+                    }
+                }
                 const float ws = reg2 * (c * c);
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch)
@@ -503,8 +613,9 @@ struct PcgArgs {
     uint32_t cap_blocks, total_nodes;
     int *err;
     float *se3;
+    const float4 *centers;
     int pcg_iters;
-    int fp64;
+    int fp64;             // FP64 reductions and node-centred twists
 };
 
 __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
@@ -726,6 +837,14 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
         float xv[6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) xv[c] = A.x[8ull * row + c];
+        if (A.fp64) {
+            // node-centred twist -> origin twist: t = t' + c x w
+            const float4 c4 = A.centers[row];
+            const float3 cw = cross3(f3(c4.x, c4.y, c4.z), f3(xv[0], xv[1], xv[2]));
+            xv[3] += cw.x;
+            xv[4] += cw.y;
+            xv[5] += cw.z;
+        }
         const float3 w = f3(xv[0], xv[1], xv[2]);
         SE3f inc;
         if (fabsf(w.x) + fabsf(w.y) + fabsf(w.z) < 1e-4f) {
@@ -773,20 +892,47 @@ static inline int grid_for(uint32_t n, int threads, int num_sms, int per_sm = 8)
 
 void init_warp(Workspace &w, cudaStream_t st) {
     k_init_warp<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.node_scene, w.total_nodes, w.se3);
+    count_launch(w);
 }
 
-cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {
+void gn_eval(Workspace &w, cudaStream_t st) {
+    k_node_centers<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.node_scene, w.total_nodes,
+                                                                           w.se3, w.centers);
+    count_launch(w);
     k_eval_dense<<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
         w.scenes, w.counts, w.d_pixels, w.d_knn, w.d_sw, w.d_cw, w.d_scene, w.se3, w.d_record);
-    if (w.total_edges > 0)
+    count_launch(w);
+    if (w.total_edges > 0) {
         k_eval_reg<<<grid_for(w.total_edges, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.edge_scene, w.total_edges,
                                                                             w.se3, w.r_record);
-    k_assemble_node<<<grid_for(w.total_nodes * 32u, 256, w.num_sms, 16), 256, 0, st>>>(
-        w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
-        w.rowptr, w.cap_blocks, w.blocks, w.inv_diag, w.jtr, w.precision, w.error_flag);
+        count_launch(w);
+    }
+}
+
+void gn_assemble_node(Workspace &w, cudaStream_t st) {
+    const int ng = grid_for(w.total_nodes * 32u, 256, w.num_sms, 16);
+    if (w.precision == WS_PREC_FP32)
+        k_assemble_node<float><<<ng, 256, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
+                                                    w.n2t_sorted_val, w.d_record, w.r_record, w.se3, w.centers,
+                                                    w.rowptr, w.cap_blocks, w.blocks, w.inv_diag, w.jtr,
+                                                    w.error_flag);
+    else
+        k_assemble_node<double><<<ng, 256, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
+                                                     w.n2t_sorted_val, w.d_record, w.r_record, w.se3, w.centers,
+                                                     w.rowptr, w.cap_blocks, w.blocks, w.inv_diag, w.jtr,
+                                                     w.error_flag);
+    count_launch(w);
+}
+
+void gn_assemble_pair(Workspace &w, cudaStream_t st) {
     k_assemble_pair<<<grid_for(w.cap_half * 32u, 256, w.num_sms, 16), 256, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
-        w.half_slot_up, w.half_slot_lo, w.d_record, w.r_record, w.blocks);
+        w.half_slot_up, w.half_slot_lo, w.d_record, w.r_record, w.centers,
+        w.precision == WS_PREC_MIXED ? 1 : 0, w.blocks);
+    count_launch(w);
+}
+
+cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     PcgArgs a;
     a.scenes = w.scenes;
     a.chunk_scene = w.chunk_scene;
@@ -806,6 +952,7 @@ cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {
     a.total_nodes = w.total_nodes;
     a.err = w.error_flag;
     a.se3 = w.se3;
+    a.centers = w.centers;
     a.pcg_iters = pcg_iters;
     a.fp64 = (w.precision == WS_PREC_MIXED) ? 1 : 0;
     const int grid = (int)std::min<uint32_t>(w.total_chunks, (uint32_t)w.pcg_grid);
@@ -813,7 +960,15 @@ cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {
     cudaMemsetAsync(w.barrier, 0, 4 * sizeof(uint32_t), st);
     cudaMemsetAsync(w.scene_counter, 0, 2 * sizeof(uint32_t) * (size_t)w.num_scenes, st);
     void *args[] = {&a};
+    count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, 0, st);
+}
+
+cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {
+    gn_eval(w, st);
+    gn_assemble_node(w, st);
+    gn_assemble_pair(w, st);
+    return gn_pcg(w, pcg_iters, st);
 }
 
 }  // namespace ws

@@ -83,6 +83,7 @@ struct Workspace {
     float *jtr = nullptr, *x = nullptr, *r = nullptr, *s = nullptr, *q = nullptr;
     float *d0 = nullptr, *d1 = nullptr;
     float *se3 = nullptr;               // [cap_nodes * 8] current warp
+    float4 *centers = nullptr;          // [cap_nodes] twist centre per node (current GN iteration)
     double *chunk_partial = nullptr;    // [cap_chunks]
     double *scene_scalars = nullptr;    // [cap_scenes * 8]: delta, alpha, beta, dq ...
     uint32_t *scene_counter = nullptr;  // [cap_scenes * 2]
@@ -93,6 +94,18 @@ struct Workspace {
     void *h_tables = nullptr;
     size_t h_tables_bytes = 0;
     std::vector<const float *> init_ptrs;     // per-scene initial warp (device) or null
+    cudaEvent_t tables_free = nullptr;        // recorded once a solve has consumed the tables
+    bool tables_in_flight = false;
+
+    // per-phase event timing (ws_set_profiling)
+    bool profiling = false;
+    static constexpr int kPhases = 5;
+    std::vector<cudaEvent_t> prof_events;       // recorded in order
+    std::vector<int> prof_phase;                // phase id of the interval ending at each event
+    std::vector<int> prof_launches;             // launches in that interval
+    int launches = 0;                           // launch counter of the current interval
+    int prof_count = 0;                         // events recorded by the last profiled solve
+    int graph_kernels = 0;                      // kernel nodes of the captured graph
 
     // graph capture cache
     cudaGraphExec_t graph_exec = nullptr;
@@ -103,12 +116,20 @@ struct Workspace {
 
 // Index build (ws_index.cu): compaction, node->term, pair->term, block CSR.
 void index_build(Workspace &w, cudaStream_t st);
-// One Gauss-Newton iteration (ws_solve.cu): term evaluation, assembly, PCG, update.
+// One Gauss-Newton iteration (ws_solve.cu): term evaluation, assembly, PCG, update,
+// and its four phases.
 cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st);
+void gn_eval(Workspace &w, cudaStream_t st);
+void gn_assemble_node(Workspace &w, cudaStream_t st);
+void gn_assemble_pair(Workspace &w, cudaStream_t st);
+cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st);
 // Initialise the warp field of every scene (identity or the given initial warp).
 void init_warp(Workspace &w, cudaStream_t st);
 // Occupancy of the persistent PCG kernel.
 int pcg_max_blocks(int device);
+
+// Launch accounting for the measurement hooks.
+inline void count_launch(Workspace &w, int n = 1) { w.launches += n; }
 
 // Counters slot indices.
 enum { kCntDense = 0, kCntN2T = 1, kCntPairKV = 2, kCntHalf = 3, kCntPairValid = 4 };

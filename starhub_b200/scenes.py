@@ -418,13 +418,21 @@ def make_scene(spec: SceneSpec, geometry, seed: int) -> Scene:
                  lambda_of=spec.lambda_of, gn_iters=spec.gn_iters, pcg_iters=spec.pcg_iters)
 
 
-def twist_error(dq_a, dq_b):
-    """Relative error of per-node SE(3) results a against reference b:
-    ||[log R_a - log R_b, t_a - t_b]|| / ||[log R_b, t_b]|| over all nodes."""
-    Ra, ta = dq_to_se3(np.asarray(dq_a))
-    Rb, tb = dq_to_se3(np.asarray(dq_b))
-    va = np.concatenate([rotation_log(Ra), ta], 1)
-    vb = np.concatenate([rotation_log(Rb), tb], 1)
+def node_twists(dq, nodes):
+    """Per-node twist of a solved warp: the rotation vector of the node's rotation and
+    the displacement of the node centre, (N, 6)."""
+    R, t = dq_to_se3(np.asarray(dq))
+    x = np.asarray(nodes)[:, :3].astype(np.float64)
+    disp = np.einsum("nij,nj->ni", R, x) + t - x
+    return np.concatenate([rotation_log(R), disp], 1)
+
+
+def twist_error(dq_a, dq_b, nodes):
+    """Relative twist error of solved warp a against reference b:
+    ||twist_a - twist_b|| / ||twist_b||, stacked over all nodes, with each node's
+    twist taken about the node itself (`node_twists`)."""
+    va = node_twists(dq_a, nodes)
+    vb = node_twists(dq_b, nodes)
     return float(np.linalg.norm(va - vb) / max(np.linalg.norm(vb), 1e-30))
 
 

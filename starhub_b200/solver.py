@@ -208,6 +208,30 @@ class WarpSolver:
         check(self._lib.ws_get_solution(self._h, scene, C.byref(p), C.byref(n)), "ws_get_solution")
         return _wrap_device_floats(p.value, n.value * 8, self.device).view(n.value, 8)
 
+    # -- measurement ---------------------------------------------------------
+    def set_profiling(self, enable: bool) -> None:
+        check(self._lib.ws_set_profiling(self._h, 1 if enable else 0), "ws_set_profiling")
+
+    PHASES = ("index", "eval", "assemble_node", "assemble_pair", "pcg")
+
+    def phase_times(self):
+        """(ms, launches) per phase of the last profiled solve (CUDA events on the solve stream)."""
+        ms = (C.c_float * 5)()
+        ln = (C.c_int * 5)()
+        n = C.c_int()
+        check(self._lib.ws_get_phase_times(self._h, ms, ln, 5, C.byref(n)), "ws_get_phase_times")
+        return dict(zip(self.PHASES, list(ms))), dict(zip(self.PHASES, list(ln)))
+
+    def graph_kernels(self) -> int:
+        n = C.c_int()
+        check(self._lib.ws_graph_kernel_count(self._h, C.byref(n)), "ws_graph_kernel_count")
+        return n.value
+
+    def counts(self, scene=0):
+        nd, nh, nkv = C.c_int(), C.c_int(), C.c_int()
+        check(self._lib.ws_get_counts(self._h, scene, C.byref(nd), C.byref(nh), C.byref(nkv)), "ws_get_counts")
+        return dict(dense_terms=nd.value, half_pairs=nh.value, n2t_kv=nkv.value)
+
     # -- index / system copies for parity tests ------------------------------
     def dense_terms(self, scene=0):
         cap = self._scenes[scene].num_pixels

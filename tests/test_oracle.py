@@ -226,4 +226,25 @@ def test_fp32_reference_mode_close_to_fp64(orc, tiny_scene):
     from starhub_b200.scenes import twist_error
     d64 = orc.solve(tiny_scene, precision=orc.ORC_PREC_FP64)
     d32 = orc.solve(tiny_scene, precision=orc.ORC_PREC_FP32_REFERENCE)
-    assert twist_error(d32, d64) < 5e-3
+    assert twist_error(d32, d64, tiny_scene.nodes) < 5e-3
+
+
+def test_mixed_mode_node_centred_matches_fp64(orc, small_scene):
+    """FP32 bulk with FP64 reductions and node-centred twists: within 1e-4 twist and 1e-5 m
+    of the all-FP64 solve (the device design, restated on the CPU)."""
+    from starhub_b200.scenes import position_error, twist_error
+    d64 = orc.solve(small_scene)
+    dmx = orc.solve(small_scene, precision=orc.ORC_PREC_MIXED)
+    assert twist_error(dmx, d64, small_scene.nodes) < 1e-4
+    assert position_error(small_scene, dmx, d64) < 1e-5
+
+
+def test_node_centred_first_step_is_a_change_of_variables(orc, small_scene):
+    """Block-Jacobi PCG is invariant under per-node changes of twist coordinates: the
+    node-centred step maps back onto the origin-twist step."""
+    _, a = orc.solve(small_scene, gn_iters=1, pcg_iters=5, debug=True)
+    _, b = orc.solve(small_scene, gn_iters=1, pcg_iters=5, debug=True, precision=orc.ORC_PREC_MIXED)
+    c = small_scene.nodes[:, :3].astype(np.float64)
+    xo = b["step"].astype(np.float64).copy()
+    xo[:, 3:] += np.cross(c, xo[:, :3])
+    np.testing.assert_allclose(xo, a["step"], atol=1e-5 * np.abs(a["step"]).max(), rtol=0)
