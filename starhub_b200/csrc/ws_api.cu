@@ -130,7 +130,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     w.cap_edges = (uint32_t)cfg->max_total_edges;
     w.cap_features = (uint32_t)cfg->max_total_features;
     w.cap_tiles = w.cap_pixels / kPixTile + (uint32_t)w.cap_scenes + 1;
-    w.cap_chunks = w.cap_nodes / 8 + (uint32_t)w.cap_scenes + 1;
+    w.cap_chunks = w.cap_nodes / ws::kRowsPerGroup + (uint32_t)w.cap_scenes + 1;
     w.cap_n2t = 4u * w.cap_pixels + 2u * w.cap_edges + w.cap_nodes + 4u * w.cap_features;
     w.cap_pair_kv = 6u * w.cap_pixels + w.cap_edges + 6u * w.cap_features;
     w.cap_half = std::min<uint32_t>(w.cap_pair_kv, 64u * w.cap_nodes);
@@ -235,7 +235,7 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
         feats += (uint64_t)scenes[s].num_features;
         pixels += (uint64_t)scenes[s].width * scenes[s].height;
         tiles += ((uint64_t)scenes[s].width * scenes[s].height + kPixTile - 1) / kPixTile;
-        chunks += ((uint64_t)scenes[s].num_nodes + 7) / 8;
+        chunks += ((uint64_t)scenes[s].num_nodes + ws::kRowsPerGroup - 1) / ws::kRowsPerGroup;
     }
     if (nodes > w.cap_nodes || edges > w.cap_edges || pixels > w.cap_pixels || feats > w.cap_features ||
         tiles > w.cap_tiles || chunks > w.cap_chunks)
@@ -295,7 +295,7 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
         const uint32_t nt = (uint32_t)(((uint64_t)in.width * in.height + kPixTile - 1) / kPixTile);
         sc.tile_base = (int)tb;
         sc.num_tiles = (int)nt;
-        const uint32_t nc = ((uint32_t)in.num_nodes + 7u) / 8u;
+        const uint32_t nc = ((uint32_t)in.num_nodes + ws::kRowsPerGroup - 1) / ws::kRowsPerGroup;
         sc.chunk_base = (int)cb;
         sc.num_chunks = (int)nc;
         for (uint32_t t = 0; t < nt; ++t) tile_scene[tb + t] = (uint32_t)s;
@@ -303,7 +303,7 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
         for (int e = 0; e < in.num_edges; ++e) edge_scene[eb + e] = (uint32_t)s;
         for (uint32_t c = 0; c < nc; ++c) {
             chunk_scene[cb + c] = (uint32_t)s;
-            chunk_row[cb + c] = nb + 8u * c;
+            chunk_row[cb + c] = nb + (uint32_t)ws::kRowsPerGroup * c;
         }
         hs[s] = sc;
         w.init_ptrs[s] = in.init_node_se3;

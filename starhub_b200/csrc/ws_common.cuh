@@ -19,6 +19,7 @@ constexpr int kVecStride = 8;        // floats per node in PCG vectors
 constexpr int kDenseRecord = 32;     // floats per dense-term record (128 B)
 constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
+constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group
 
 // ---------------------------------------------------------------------------
 // Per-scene descriptor, device resident.  Filled on the host from ws_inputs.
@@ -46,7 +47,7 @@ struct Scene {
     const ushort4 *feature_knn;        // may be null
     float lam_depth, lam_of, lam_reg, lam_node, lam_feat;
     int tile_base, num_tiles;          // pixel tiles of this scene
-    int chunk_base, num_chunks;        // PCG row chunks of this scene
+    int chunk_base, num_chunks;        // PCG row groups (kRowsPerGroup nodes) of this scene
 };
 
 // Per-scene counts derived on the device during the index build.

@@ -588,34 +588,36 @@ __global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, cons
 // Persistent block PCG (BlockPCG<6>::SolveNoConvergeCheck,
 // libs/star/pcg_solver/BlockPCG.cuh:67-190, 325-484) for every scene of the batch.
 //
-// Rows (nodes) are grouped in scene-aligned chunks of 8, one warp per row.
-// Per iteration: phase A  d = s + beta d (recomputed for neighbours), q = A d,
-// partial <d, q>;  phase B  alpha, x += alpha d, r -= alpha q, s = M^-1 r,
-// partial <r, s>.  The last chunk of a scene to finish a phase reduces that
-// scene's chunk partials in chunk order and publishes alpha / beta, so every
-// scene's arithmetic is independent of the rest of the batch.  Two bounded
-// grid barriers per iteration; a timed-out wait sets WS_ERR_TIMEOUT and every
-// block leaves.
+// Rows (nodes) are grouped in scene-aligned groups of kRowsPerGroup; every warp
+// owns a fixed set of groups (grid-stride over warps) and walks their rows one at
+// a time, with no block-level synchronisation inside a phase.
+// Per iteration: phase A  d = s + beta d (recomputed for neighbours from s and the
+// previous d), q = A d, <d, q>;  phase B  alpha, x += alpha d, r -= alpha q,
+// s = M^-1 r, <r, s>.  A warp keeps its group's partial in FP64 registers, stores
+// it, and the last group of a scene to finish (a fenced atomic ticket) sums that
+// scene's group partials in group order and publishes alpha or beta; the sums
+// therefore never depend on the rest of the batch.  One bounded grid barrier
+// ends each phase; a timed-out wait sets WS_ERR_TIMEOUT and every block leaves.
 // ---------------------------------------------------------------------------
-constexpr int kPcgThreads = 256;   // 8 warps: one chunk of 8 rows per block round
+constexpr int kPcgThreads = 256;   // 8 warps per block
 
 struct PcgArgs {
     const Scene *scenes;
-    const uint32_t *chunk_scene, *chunk_row;
-    uint32_t total_chunks;
+    const uint32_t *group_scene, *group_row;
+    uint32_t total_groups;
     const uint32_t *rowptr, *colidx;
     const float *blocks, *inv_diag, *jtr;
     float *x, *r, *s, *q, *d0, *d1;
-    double *chunk_partial;
+    double *group_partial;
     double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
-    uint32_t *scene_counter;  // per scene: [0] phase A, [1] phase B
+    uint32_t *scene_counter;  // per scene: [0] phase A, [1] phase B / init
     uint32_t *barrier;        // [0] arrive count, [1] generation
     uint32_t cap_blocks, total_nodes;
     int *err;
     float *se3;
     const float4 *centers;
     int pcg_iters;
-    int fp64;             // FP64 reductions and node-centred twists
+    int fp64;                 // FP64 reductions and node-centred twists
 };
 
 __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
@@ -635,7 +637,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
             unsigned long long spins = 0;
             while (*gen == my_gen) {
                 if (++spins > kSpinLimit) { set_err(err, WS_ERR_TIMEOUT); ok = 0; break; }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
         __threadfence();
@@ -648,195 +650,200 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
 __device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
 
-// CTA-level chunk partial: warps write row partials to smem, thread 0 sums in warp order,
-// publishes the chunk partial, and the last chunk of the scene reduces the scene.
-// Returns nothing; `mode` 0 = phase A (alpha), 1 = phase B (beta), 2 = init (delta only).
-__device__ void publish_partial(const PcgArgs &A, uint32_t chunk, uint32_t scene, double *wpart, int mode) {
-    __shared__ int last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double sum = 0.0;
-        for (int w = 0; w < kPcgThreads / 32; ++w) sum += wpart[w];
-        A.chunk_partial[chunk] = sum;
+// Publishes a group partial; the last group of the scene reduces the scene.
+// mode 0: alpha = delta / sum;  mode 1: beta = sum / delta, delta = sum;  mode 2 (init): delta = sum, beta = 0.
+__device__ __forceinline__ void publish_group(const PcgArgs &A, uint32_t group, uint32_t scene, double part,
+                                              int mode, int lane) {
+    int last = 0;
+    if (lane == 0) {
+        A.group_partial[group] = part;
         __threadfence();
-        const Scene &sc = A.scenes[scene];
         const uint32_t ctr = (mode == 0) ? 0u : 1u;
+        const Scene &sc = A.scenes[scene];
         const uint32_t ticket = atomicAdd(&A.scene_counter[2 * scene + ctr], 1u);
         last = (ticket == (uint32_t)sc.num_chunks - 1u) ? 1 : 0;
-        if (last) atomicExch(&A.scene_counter[2 * scene + ctr], 0u);
-        __threadfence();
-    }
-    __syncthreads();
-    if (last && threadIdx.x < 32) {
-        const Scene &sc = A.scenes[scene];
-        double v = 0.0;
-        for (int c = threadIdx.x; c < sc.num_chunks; c += 32) v += ldcg(A.chunk_partial + sc.chunk_base + c);
-        v = warp_sum(v);
-        if (threadIdx.x == 0) {
-            double *S = A.scalars + 8ull * scene;
-            if (!A.fp64) v = (double)(float)v;
-            if (mode == 0) {
-                const double delta = ldcg(S + 0);
-                double alpha = (v != 0.0) ? delta / v : 0.0;
-                if (!A.fp64) alpha = (double)((float)delta / (float)v);
-                if (v == 0.0) alpha = 0.0;
-                S[1] = alpha;
-            } else {
-                const double delta_old = ldcg(S + 0);
-                double beta = (delta_old != 0.0) ? v / delta_old : 0.0;
-                if (!A.fp64 && delta_old != 0.0) beta = (double)((float)v / (float)delta_old);
-                S[2] = (mode == 2) ? 0.0 : beta;
-                S[0] = v;
-            }
-            S[3] = v;
+        if (last) {
+            atomicExch(&A.scene_counter[2 * scene + ctr], 0u);
             __threadfence();
         }
     }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    const Scene &sc = A.scenes[scene];
+    double v = 0.0;
+    for (int c = lane; c < sc.num_chunks; c += 32) v += ldcg(A.group_partial + sc.chunk_base + c);
+    v = warp_sum(v);
+    if (lane == 0) {
+        double *S = A.scalars + 8ull * scene;
+        if (!A.fp64) v = (double)(float)v;
+        if (mode == 0) {
+            const double delta = ldcg(S + 0);
+            double alpha = (v != 0.0) ? delta / v : 0.0;
+            if (!A.fp64 && v != 0.0) alpha = (double)((float)delta / (float)v);
+            S[1] = alpha;
+        } else {
+            const double delta_old = ldcg(S + 0);
+            double beta = (delta_old != 0.0) ? v / delta_old : 0.0;
+            if (!A.fp64 && delta_old != 0.0) beta = (double)((float)v / (float)delta_old);
+            S[2] = (mode == 2) ? 0.0 : beta;
+            S[0] = v;
+        }
+        S[3] = v;
+        __threadfence();
+    }
 }
 
+// Lane map inside a warp: lanes 2n and 2n+1 own node r0+n of the 16-row group, each
+// three scalar rows (half 0: rows 0-2, half 1: rows 3-5 of the 6x6 block row).
+__device__ __forceinline__ double lane_dot3(const PcgArgs &A, const float *u, const float *v, bool valid) {
+    double p = 0.0;
+    if (valid) {
+        if (A.fp64) p = (double)u[0] * (double)v[0] + (double)u[1] * (double)v[1] + (double)u[2] * (double)v[2];
+        else p = (double)(u[0] * v[0] + u[1] * v[1] + u[2] * v[2]);
+    }
+    if (!A.fp64) {
+        float pf = (float)p;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
+        return (double)pf;
+    }
+    return warp_sum(p);
+}
+
+__device__ __forceinline__ float4 ldcg4(const float *p) { return __ldcg(reinterpret_cast<const float4 *>(p)); }
+
 __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ double wpart[kPcgThreads / 32];
-    const int slot = lane / 6, a = lane % 6;      // SpMV lane mapping: 5 block slots x 6 rows
+    const int lane = threadIdx.x & 31;
+    const int half = lane & 1;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     // ---- init: r = b, s = M^-1 b, x = 0, d = 0, delta = <r, s> ----
-    for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
-        const uint32_t scene = A.chunk_scene[ch];
+    for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
+        const uint32_t scene = A.group_scene[g];
         const Scene &sc = A.scenes[scene];
-        const uint32_t row = A.chunk_row[ch] + warp;
-        const bool active = row < (uint32_t)(sc.node_base + sc.num_nodes);
-        double part = 0.0;
-        if (active && lane < 6) {
-            float bv[6];
+        const uint32_t node = A.group_row[g] + (lane >> 1);
+        const bool valid = node < (uint32_t)(sc.node_base + sc.num_nodes);
+        float bv[6], rl[3] = {0.f, 0.f, 0.f}, sl[3] = {0.f, 0.f, 0.f};
+        if (valid) {
+            const float4 b0 = *reinterpret_cast<const float4 *>(A.jtr + 8ull * node);
+            const float4 b1 = *reinterpret_cast<const float4 *>(A.jtr + 8ull * node + 4);
+            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w; bv[4] = b1.x; bv[5] = b1.y;
+            const float *M = A.inv_diag + 36ull * node + 18 * half;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) bv[c] = A.jtr[8ull * row + c];
-            const float *M = A.inv_diag + 36ull * row + 6 * lane;
-            float sv = 0.f;
+            for (int i = 0; i < 3; ++i) {
+                float acc = 0.f;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) sv += M[c] * bv[c];
-            A.r[8ull * row + lane] = bv[lane];
-            A.s[8ull * row + lane] = sv;
-            A.x[8ull * row + lane] = 0.f;
-            A.d0[8ull * row + lane] = 0.f;
-            A.d1[8ull * row + lane] = 0.f;
-            part = A.fp64 ? (double)bv[lane] * (double)sv : (double)(bv[lane] * sv);
+                for (int c = 0; c < 6; ++c) acc += M[6 * i + c] * bv[c];
+                sl[i] = acc;
+                rl[i] = half ? bv[3 + i] : bv[i];
+                A.r[8ull * node + 3 * half + i] = rl[i];
+                A.s[8ull * node + 3 * half + i] = sl[i];
+                A.x[8ull * node + 3 * half + i] = 0.f;
+                A.d0[8ull * node + 3 * half + i] = 0.f;
+                A.d1[8ull * node + 3 * half + i] = 0.f;
+            }
         }
-        if (!A.fp64) {
-            float pf = (float)part;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
-            part = pf;
-        } else {
-            part = warp_sum(part);
-        }
-        if (lane == 0) wpart[warp] = part;
-        publish_partial(A, ch, scene, wpart, 2);
+        publish_group(A, g, scene, lane_dot3(A, rl, sl, valid), 2, lane);
     }
     if (!grid_barrier(A.barrier, A.err)) return;
 
     for (int it = 0; it < A.pcg_iters; ++it) {
         const float *d_old = (it & 1) ? A.d1 : A.d0;
         float *d_new = (it & 1) ? A.d0 : A.d1;
-        // ---- phase A ----
-        for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
-            const uint32_t scene = A.chunk_scene[ch];
+        // ---- phase A: d = s + beta d, q = A d, <d, q> ----
+        for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
+            const uint32_t scene = A.group_scene[g];
             const Scene &sc = A.scenes[scene];
-            const uint32_t row = A.chunk_row[ch] + warp;
-            const bool active = row < (uint32_t)(sc.node_base + sc.num_nodes);
+            const uint32_t node = A.group_row[g] + (lane >> 1);
+            const bool valid = node < (uint32_t)(sc.node_base + sc.num_nodes);
             const float beta = (float)ldcg(A.scalars + 8ull * scene + 2);
-            double part = 0.0;
-            if (active) {
-                float acc = 0.f;
+            float acc[3] = {0.f, 0.f, 0.f}, dn[3] = {0.f, 0.f, 0.f};
+            if (valid) {
                 // bounds hold by construction; the clamps keep a capacity overflow (already
                 // flagged as WS_ERR_CAPACITY) from reading outside the buffers
-                const uint32_t b1 = min(A.rowptr[row + 1], A.cap_blocks);
-                const uint32_t b0 = min(A.rowptr[row], b1);
-                if (slot < 5) {
-                    for (uint32_t k = b0 + slot; k < b1; k += 5) {
-                        const uint32_t col = min(A.colidx[k], A.total_nodes - 1);
-                        const float2 *blk = reinterpret_cast<const float2 *>(A.blocks + 36ull * k + 6 * a);
-                        const float2 m0 = __ldg(blk), m1 = __ldg(blk + 1), m2 = __ldg(blk + 2);
-                        const float *sp = A.s + 8ull * col, *dp = d_old + 8ull * col;
-                        float dv[6];
+                const uint32_t b1 = min(A.rowptr[node + 1], A.cap_blocks);
+                const uint32_t b0 = min(A.rowptr[node], b1);
+#pragma unroll 2
+                for (uint32_t k = b0; k < b1; ++k) {
+                    const uint32_t col = min(A.colidx[k], A.total_nodes - 1);
+                    const float2 *blk = reinterpret_cast<const float2 *>(A.blocks + 36ull * k + 18 * half);
+                    float m[18];
 #pragma unroll
-                        for (int c = 0; c < 6; ++c) dv[c] = ldcg(sp + c) + beta * ldcg(dp + c);
-                        acc += m0.x * dv[0] + m0.y * dv[1] + m1.x * dv[2] + m1.y * dv[3] + m2.x * dv[4] + m2.y * dv[5];
+                    for (int i = 0; i < 9; ++i) {
+                        const float2 v = __ldg(blk + i);
+                        m[2 * i] = v.x;
+                        m[2 * i + 1] = v.y;
                     }
-                }
-                // combine the 5 slots for matrix row a in fixed order
-                const float t1 = __shfl_sync(0xffffffffu, acc, (a + 6) & 31);
-                const float t2 = __shfl_sync(0xffffffffu, acc, (a + 12) & 31);
-                const float t3 = __shfl_sync(0xffffffffu, acc, (a + 18) & 31);
-                const float t4 = __shfl_sync(0xffffffffu, acc, (a + 24) & 31);
-                if (lane < 6) {
-                    const float qa = (((acc + t1) + t2) + t3) + t4;
-                    const float dn = ldcg(A.s + 8ull * row + lane) + beta * ldcg(d_old + 8ull * row + lane);
-                    d_new[8ull * row + lane] = dn;
-                    A.q[8ull * row + lane] = qa;
-                    part = A.fp64 ? (double)dn * (double)qa : (double)(dn * qa);
-                }
-            }
-            if (!A.fp64) {
-                float pf = (float)part;
+                    const float4 s0 = ldcg4(A.s + 8ull * col), s1 = ldcg4(A.s + 8ull * col + 4);
+                    const float4 e0 = ldcg4(d_old + 8ull * col), e1 = ldcg4(d_old + 8ull * col + 4);
+                    const float dv[6] = {s0.x + beta * e0.x, s0.y + beta * e0.y, s0.z + beta * e0.z,
+                                         s0.w + beta * e0.w, s1.x + beta * e1.x, s1.y + beta * e1.y};
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
-                part = pf;
-            } else {
-                part = warp_sum(part);
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) acc[i] += m[6 * i + c] * dv[c];
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const size_t e = 8ull * node + 3 * half + i;
+                    dn[i] = ldcg(A.s + e) + beta * ldcg(d_old + e);
+                    d_new[e] = dn[i];
+                    A.q[e] = acc[i];
+                }
             }
-            if (lane == 0) wpart[warp] = part;
-            publish_partial(A, ch, scene, wpart, 0);
+            publish_group(A, g, scene, lane_dot3(A, dn, acc, valid), 0, lane);
         }
         if (!grid_barrier(A.barrier, A.err)) return;
-        // ---- phase B ----
-        for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
-            const uint32_t scene = A.chunk_scene[ch];
+        // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
+        for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
+            const uint32_t scene = A.group_scene[g];
             const Scene &sc = A.scenes[scene];
-            const uint32_t row = A.chunk_row[ch] + warp;
-            const bool active = row < (uint32_t)(sc.node_base + sc.num_nodes);
+            const uint32_t node = A.group_row[g] + (lane >> 1);
+            const bool valid = node < (uint32_t)(sc.node_base + sc.num_nodes);
             const float alpha = (float)ldcg(A.scalars + 8ull * scene + 1);
-            double part = 0.0;
-            float rn = 0.f;
-            if (active && lane < 6) {
-                const float dn = ldcg(d_new + 8ull * row + lane);
-                const float qa = ldcg(A.q + 8ull * row + lane);
-                A.x[8ull * row + lane] += alpha * dn;
-                rn = A.r[8ull * row + lane] - alpha * qa;
-                A.r[8ull * row + lane] = rn;
+            float rn[3] = {0.f, 0.f, 0.f}, sv[3] = {0.f, 0.f, 0.f};
+            if (valid) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const size_t e = 8ull * node + 3 * half + i;
+                    A.x[e] += alpha * ldcg(d_new + e);
+                    rn[i] = A.r[e] - alpha * ldcg(A.q + e);
+                    A.r[e] = rn[i];
+                }
             }
+            // the partner lane holds the other three entries of the node's r
             float rv[6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) rv[c] = __shfl_sync(0xffffffffu, rn, c);
-            if (active && lane < 6) {
-                const float *M = A.inv_diag + 36ull * row + 6 * lane;
-                float sv = 0.f;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) sv += M[c] * rv[c];
-                A.s[8ull * row + lane] = sv;
-                part = A.fp64 ? (double)rn * (double)sv : (double)(rn * sv);
+            for (int i = 0; i < 3; ++i) {
+                const float other = __shfl_xor_sync(0xffffffffu, rn[i], 1);
+                rv[i] = half ? other : rn[i];
+                rv[3 + i] = half ? rn[i] : other;
             }
-            if (!A.fp64) {
-                float pf = (float)part;
+            if (valid) {
+                const float *M = A.inv_diag + 36ull * node + 18 * half;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
-                part = pf;
-            } else {
-                part = warp_sum(part);
+                for (int i = 0; i < 3; ++i) {
+                    float acc = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) acc += M[6 * i + c] * rv[c];
+                    sv[i] = acc;
+                    A.s[8ull * node + 3 * half + i] = acc;
+                }
             }
-            if (lane == 0) wpart[warp] = part;
-            publish_partial(A, ch, scene, wpart, 1);
+            publish_group(A, g, scene, lane_dot3(A, rn, sv, valid), 1, lane);
         }
         if (!grid_barrier(A.barrier, A.err)) return;
     }
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
     //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
-    for (uint32_t ch = blockIdx.x; ch < A.total_chunks; ch += gridDim.x) {
-        const uint32_t scene = A.chunk_scene[ch];
+    for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
+        const uint32_t scene = A.group_scene[g];
         const Scene &sc = A.scenes[scene];
-        const uint32_t row = A.chunk_row[ch] + warp;
-        if (row >= (uint32_t)(sc.node_base + sc.num_nodes) || lane != 0) continue;
+        const uint32_t row = A.group_row[g] + lane;
+        if (lane >= kRowsPerGroup || row >= (uint32_t)(sc.node_base + sc.num_nodes)) continue;
         float xv[6];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) xv[c] = A.x[8ull * row + c];
+        for (int c = 0; c < 6; ++c) xv[c] = ldcg(A.x + 8ull * row + c);
         if (A.fp64) {
             // node-centred twist -> origin twist: t = t' + c x w
             const float4 c4 = A.centers[row];
@@ -935,16 +942,16 @@ void gn_assemble_pair(Workspace &w, cudaStream_t st) {
 cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     PcgArgs a;
     a.scenes = w.scenes;
-    a.chunk_scene = w.chunk_scene;
-    a.chunk_row = w.chunk_row;
-    a.total_chunks = w.total_chunks;
+    a.group_scene = w.chunk_scene;
+    a.group_row = w.chunk_row;
+    a.total_groups = w.total_chunks;
     a.rowptr = w.rowptr;
     a.colidx = w.colidx;
     a.blocks = w.blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
     a.x = w.x; a.r = w.r; a.s = w.s; a.q = w.q; a.d0 = w.d0; a.d1 = w.d1;
-    a.chunk_partial = w.chunk_partial;
+    a.group_partial = w.chunk_partial;
     a.scalars = w.scene_scalars;
     a.scene_counter = w.scene_counter;
     a.barrier = w.barrier;
@@ -955,7 +962,9 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     a.centers = w.centers;
     a.pcg_iters = pcg_iters;
     a.fp64 = (w.precision == WS_PREC_MIXED) ? 1 : 0;
-    const int grid = (int)std::min<uint32_t>(w.total_chunks, (uint32_t)w.pcg_grid);
+    // one warp per row group when that fits, else every co-resident block
+    const uint32_t want = (w.total_chunks + (kPcgThreads / 32) - 1) / (kPcgThreads / 32);
+    const int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, (uint32_t)w.pcg_grid));
     // a barrier or counter left half-way by an earlier timed-out launch must not leak into this one
     cudaMemsetAsync(w.barrier, 0, 4 * sizeof(uint32_t), st);
     cudaMemsetAsync(w.scene_counter, 0, 2 * sizeof(uint32_t) * (size_t)w.num_scenes, st);
