@@ -186,6 +186,23 @@ int ws_get_phase_times(ws_solver *solver, float *ms, int *launches, int capacity
 /* Kernel launches in one replay of the graph captured by ws_solve_graph. */
 int ws_graph_kernel_count(ws_solver *solver, int *count);
 
+/* ws_splat_maps without any device allocation.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc or cudaMallocAsync once they are running: a
+ * frame loop or serving process that reserves its whole device budget at start-up and
+ * admits work by footprint, or a host whose own pool owns all device memory.  Such a
+ * caller must not have an allocation fail, or block, in the middle of a frame.
+ * The z-buffer scratch is a file-scope __device__ array of WS_NOALLOC_MAX_PIXELS 64-bit
+ * keys (7.4 MB), which every GPU that loads this library holds until the process exits.
+ * The first call on a device looks up that array's device address (cudaGetSymbolAddress)
+ * with that device current, so make the first call before any stream capture.  Every call
+ * shares the one array and clears it on `stream` before use, so calls that overlap on the
+ * GPU race.  width * height above WS_NOALLOC_MAX_PIXELS returns WS_ERR_CAPACITY. */
+#define WS_NOALLOC_MAX_PIXELS (1280 * 720)
+int ws_splat_maps_noalloc(const float *verts, const float *attr_verts, const float *attr_normals,
+                          int num_verts, int width, int height, float fx, float fy, float cx, float cy,
+                          int footprint, uint32_t *index_map, float *vertex_map, float *normal_map,
+                          void *stream);
+
 /* Library version / build identification. */
 int ws_version(void);
 const char *ws_error_string(int status);

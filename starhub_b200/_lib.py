@@ -24,6 +24,8 @@ WS_ERR_NO_DEVICE = -7
 WS_PREC_MIXED = 0
 WS_PREC_FP32 = 1
 
+WS_NOALLOC_MAX_PIXELS = 1280 * 720
+
 # Every symbol include/warpsolve.h declares.
 EXPORTED = [
     "ws_default_penalties", "ws_create", "ws_destroy", "ws_set_inputs", "ws_set_batch", "ws_solve",
@@ -31,6 +33,7 @@ EXPORTED = [
     "ws_get_node2term", "ws_get_node_pairs", "ws_get_system", "ws_get_dense_jacobian", "ws_init_nodes",
     "ws_build_node_graph", "ws_skinning", "ws_forward_warp", "ws_splat_maps", "ws_version",
     "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
+    "ws_splat_maps_noalloc",
 ]
 
 
@@ -104,6 +107,7 @@ def load() -> C.CDLL:
         "ws_skinning": (i, [vp, i, vp, i, f, vp, vp, vp, vp]),
         "ws_forward_warp": (i, [vp, i, vp, vp, i, vp, vp, vp, vp, vp, vp]),
         "ws_splat_maps": (i, [vp, vp, vp, i, i, i, f, f, f, f, i, vp, vp, vp, vp]),
+        "ws_splat_maps_noalloc": (i, [vp, vp, vp, i, i, i, f, f, f, f, i, vp, vp, vp, vp]),
         "ws_version": (i, []),
         "ws_error_string": (C.c_char_p, [i]),
         "ws_set_profiling": (i, [vp, i]),

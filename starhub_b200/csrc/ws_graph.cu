@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -260,12 +262,43 @@ __global__ void k_splat_resolve(const unsigned long long *zbuf, int npix, const 
     }
 }
 
+// Scratch of ws_splat_maps_noalloc: one depth/id key per pixel of the largest supported
+// image, in the module's static device memory (no allocation at call time).
+static __device__ __align__(256) unsigned long long g_noalloc_zbuf[WS_NOALLOC_MAX_PIXELS];
+
 static int grid_of(long long n, int threads) {
     long long g = (n + threads - 1) / threads;
     return (int)std::max(1LL, std::min(g, 148LL * 32));
 }
 
 }  // namespace ws
+
+namespace {
+
+// Device address of g_noalloc_zbuf per device, looked up once with that device current.
+// Fixed-size table: the lookup path allocates nothing.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned long long *g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_scratch(unsigned long long **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return WS_ERR_CUDA;
+    if (dev < 0 || dev >= kMaxDevices) return WS_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, ws::g_noalloc_zbuf) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return WS_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned long long *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return WS_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -391,6 +424,29 @@ int ws_splat_maps(const float *verts, const float *attr_verts, const float *attr
         zbuf, (int)npix, reinterpret_cast<const float4 *>(attr_verts), reinterpret_cast<const float4 *>(attr_normals),
         index_map, reinterpret_cast<float4 *>(vertex_map), reinterpret_cast<float4 *>(normal_map));
     cudaFreeAsync(zbuf, st);
+    return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
+int ws_splat_maps_noalloc(const float *verts, const float *attr_verts, const float *attr_normals, int n, int W,
+                          int H, float fx, float fy, float cx, float cy, int footprint, uint32_t *index_map,
+                          float *vertex_map, float *normal_map, void *stream) {
+    if (!verts || n < 0 || W <= 0 || H <= 0 || !index_map || footprint < 0 || footprint > 8)
+        return WS_ERR_INVALID_ARGUMENT;
+    if ((vertex_map && !attr_verts) || (normal_map && !attr_normals)) return WS_ERR_INVALID_ARGUMENT;
+    if ((long long)W * H > WS_NOALLOC_MAX_PIXELS) return WS_ERR_CAPACITY;
+    unsigned long long *zbuf = nullptr;
+    const int st_scratch = noalloc_scratch(&zbuf);
+    if (st_scratch != WS_OK) return st_scratch;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t npix = (size_t)W * H;
+    // the array keeps the previous call's keys: clear the part this call uses
+    if (cudaMemsetAsync(zbuf, 0xff, 8 * npix, st) != cudaSuccess) return WS_ERR_CUDA;
+    if (n > 0)
+        ws::k_splat<<<ws::grid_of(n, 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(verts), n, W, H, fx, fy, cx,
+                                                         cy, footprint, zbuf);
+    ws::k_splat_resolve<<<ws::grid_of((long long)npix, 256), 256, 0, st>>>(
+        zbuf, (int)npix, reinterpret_cast<const float4 *>(attr_verts), reinterpret_cast<const float4 *>(attr_normals),
+        index_map, reinterpret_cast<float4 *>(vertex_map), reinterpret_cast<float4 *>(normal_map));
     return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }
 
