@@ -35,7 +35,7 @@ void free_all(ws::Workspace &w) {
                     w.n2t_val_alt, w.n2t_offset, w.pair_key, w.pair_key_alt, w.pair_val, w.pair_val_alt,
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
-                    w.col_key_alt, w.col_val_alt, w.colidx, w.blocks, w.inv_diag, w.jtr, w.x, w.r, w.s, w.q,
+                    w.col_key_alt, w.col_val_alt, w.colidx, w.blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.s, w.q,
                     w.d0, w.d1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
                     w.error_flag};
     for (void *p : ptrs)
@@ -185,6 +185,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.colidx, w.cap_blocks));
     A(dalloc(&w.blocks, (size_t)w.cap_blocks * 36));
     A(dalloc(&w.inv_diag, (size_t)w.cap_nodes * 36));
+    A(dalloc(&w.diag64, (size_t)w.cap_nodes * 21));
     for (float **v : {&w.jtr, &w.x, &w.r, &w.s, &w.q, &w.d0, &w.d1}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
     A(dalloc(&w.se3, (size_t)w.cap_nodes * 8));
     A(dalloc(&w.centers, w.cap_nodes));

@@ -279,307 +279,443 @@ __device__ void cholesky6_fp64(const double *in, float *out) {
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal blocks, preconditioner and right-hand side: one warp per node over
-// its node->term list (computeBlockDiagonalPreconditionerKernel,
-// examples/mono_star/opt/PreconditionerRhsBuilder.cu:110-261, and
-// computeJtResidualWithIndexKernel, JtDotResidualIndexed.cu:40-149).
-// Lane l takes list positions l, l+32, ...; a fixed butterfly combines lanes.
+// Diagonal blocks and right-hand side: one warp per node over its node->term list
+// (computeBlockDiagonalPreconditionerKernel, examples/mono_star/opt/PreconditionerRhsBuilder.cu:110-261,
+// and computeJtResidualWithIndexKernel, JtDotResidualIndexed.cu:40-149).
+//
+// Every term contributes three scaled Jacobian rows u (lambda * J, 6 values) and a scaled
+// residual v, so that D += u u^T and b += v u.  The warp takes 32 list entries at a time,
+// copies their records into shared memory with coalesced loads, and each lane sums its own
+// term's products in registers; at the end of the list the 27 entries are summed over the
+// lanes in lane order through shared memory.  The order is fixed by the list, so results do
+// not depend on what else is in the batch.
+// DAcc is the accumulator type: float for WS_PREC_FP32 (the reference's FP32 sums),
+// double for WS_PREC_MIXED, where D feeds the FP64 Cholesky directly.
 // ---------------------------------------------------------------------------
-// DAcc is the accumulator type of the diagonal block: float for WS_PREC_FP32 (the reference's
-// FP32 reduction), double for WS_PREC_MIXED, where the block feeds the FP64 Cholesky directly
-// and is rounded to FP32 only for the SpMV.
+constexpr int kAssembleThreads = 128;
+
+// Per-warp staging: 32 slots, one per list entry of the current batch.  A slot holds the
+// term's record (dense 128 B, regularisation 64 B) and, after the list, the lane's partial
+// sums.  Slot strides keep 16-byte accesses by consecutive lanes on distinct banks.
+constexpr int kSlotWordsF32 = 36;   // 144 B: a dense record, or 27 (node) / 36 (pair) partial sums
+constexpr int kSlotWordsF64 = 60;   // 240 B: a dense record, or 27 double partial sums
+
+// Copies the records of the warp's 32 terms into their slots.  Lane l names its record by
+// `src` (16-byte units) and `parts` (8 dense, 4 regularisation, 0 none); in pass j the lanes
+// of group l / 8 move record 4 j + l / 8, one 16-byte part each (cp.async, no registers), so
+// every pass reads four whole records on 128-byte lines.  The caller syncs the warp after.
+template <int kSlotWords>
+__device__ __forceinline__ void fetch_records(float *slots, int lane, const float4 *src, int parts) {
+    const int part = lane & 7;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int r = 4 * j + (lane >> 3);
+        const float4 *p = reinterpret_cast<const float4 *>(
+            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), r));
+        const int np = __shfl_sync(0xffffffffu, parts, r);
+        if (part < np) {
+            const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(slots + r * kSlotWords + 4 * part));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(p + part) : "memory");
+        }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Dense record fields (k_eval_dense): gradient rows 0..17 (three channels of 6), residuals
+// 18..20, skinning weights 22..25, node ids 26..29.
+__device__ __forceinline__ void read_weights(const float *slot, float *wk, uint32_t *ids) {
+    const float4 a = *reinterpret_cast<const float4 *>(slot + 20);
+    const float4 b = *reinterpret_cast<const float4 *>(slot + 24);
+    const float2 c = *reinterpret_cast<const float2 *>(slot + 28);
+    wk[0] = a.z;
+    wk[1] = a.w;
+    wk[2] = b.x;
+    wk[3] = b.y;
+    ids[0] = __float_as_uint(b.z);
+    ids[1] = __float_as_uint(b.w);
+    ids[2] = __float_as_uint(c.x);
+    ids[3] = __float_as_uint(c.y);
+}
+__device__ __forceinline__ float read_channel(const float *slot, int ch, float *g) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const float2 v = *reinterpret_cast<const float2 *>(slot + 6 * ch + 2 * q);
+        g[2 * q] = v.x;
+        g[2 * q + 1] = v.y;
+    }
+    return slot[18 + ch];
+}
+
+// Reads one record of `n4` 16-byte parts back from a slot.
+template <int n4>
+__device__ __forceinline__ void read_slot(const float *slot, float *out) {
+#pragma unroll
+    for (int i = 0; i < n4; ++i) {
+        const float4 v = *reinterpret_cast<const float4 *>(slot + 4 * i);
+        out[4 * i] = v.x;
+        out[4 * i + 1] = v.y;
+        out[4 * i + 2] = v.z;
+        out[4 * i + 3] = v.w;
+    }
+}
+
+// Upper-triangle entry e (0..20) of a symmetric 6x6 block -> (a, c), a <= c, row-major order.
+__device__ __forceinline__ void tri_decode(int e, int &a, int &c) {
+    a = 0;
+    c = 0;
+#pragma unroll
+    for (int r = 0, start = 0; r < 6; start += 6 - r, ++r)
+        if (e >= start && e < start + 6 - r) {
+            a = r;
+            c = r + (e - start);
+        }
+}
+
+// Regulariser entry (a, c) of the diagonal block: +1e-3 on the diagonal of the origin-twist
+// block (PreconditionerRhsBuilder.cu:249-252); for node-centred twists the same term is
+// 1e-3 S^T S with S = [[I, 0], [[c]x, I]].
 template <class DAcc>
-__global__ void __launch_bounds__(256) k_assemble_node(const Scene *scenes, const Plan *plan,
-                                                        const uint32_t *node_scene, uint32_t total_nodes,
-                                                        const uint32_t *n2t_offset, const uint32_t *n2t_val,
-                                                        const float *drec, const float *rrec, const float *se3,
-                                                        const float4 *centers, const uint32_t *rowptr,
-                                                        uint32_t cap_blocks, float *blocks, float *inv_diag, float *jtr,
-                                                        int *err) {
-    constexpr bool kFp64 = sizeof(DAcc) == 8;   // mixed precision: also node-centred twists
+__device__ __forceinline__ DAcc regulariser_entry(int a, int c, float3 cen, bool centred) {
+    const DAcc eps = DAcc(1e-3f);
+    if (!centred || a >= 3) return a == c ? eps : DAcc(0);
+    const DAcc x = cen.x, y = cen.y, z = cen.z;
+    const DAcc ca = a == 0 ? x : (a == 1 ? y : z);
+    if (c < 3) {
+        const DAcc cc = c == 0 ? x : (c == 1 ? y : z);
+        return eps * ((a == c ? DAcc(1) + (x * x + y * y + z * z) : DAcc(0)) - ca * cc);
+    }
+    // -eps [c]x with [c]x = [[0, -z, y], [z, 0, -x], [-y, x, 0]]
+    const int k = c - 3;
+    DAcc v = DAcc(0);
+    if (a == 0) v = k == 1 ? -z : (k == 2 ? y : DAcc(0));
+    if (a == 1) v = k == 0 ? z : (k == 2 ? -x : DAcc(0));
+    if (a == 2) v = k == 0 ? -y : (k == 1 ? x : DAcc(0));
+    return -eps * v;
+}
+
+// D += u u^T (upper triangle) and b += v u for one scaled row.
+template <class DAcc>
+__device__ __forceinline__ void accumulate_row(DAcc *D, DAcc *B, const float *row, float scale, float v) {
+    DAcc u[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) u[q] = DAcc(scale * row[q]);
+    const DAcc dv = DAcc(v);
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+#pragma unroll
+        for (int c = a; c < 6; ++c) D[tri_index(a, c)] += u[a] * u[c];
+        B[a] += dv * u[a];
+    }
+}
+
+template <class DAcc>
+__global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_node(const Scene *scenes, const Plan *plan,
+                                                                     const uint32_t *node_scene, uint32_t total_nodes,
+                                                                     const uint32_t *n2t_offset, const uint32_t *n2t_val,
+                                                                     const float *drec, const float *rrec,
+                                                                     const float *se3, const float4 *centers,
+                                                                     const uint32_t *rowptr, uint32_t cap_blocks,
+                                                                     float *blocks, double *diag64, float *jtr, int *err) {
+    constexpr bool kCentred = sizeof(DAcc) == 8;   // mixed precision also uses node-centred twists
+    constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;
+    static_assert(27 * sizeof(DAcc) <= 4 * kSlot, "a slot holds one lane's 27 partial sums");
+    __shared__ __align__(16) float stage[kAssembleThreads / 32][32 * kSlot];
     const int lane = threadIdx.x & 31;
+    float *slots = stage[threadIdx.x >> 5];
+    float *mine = slots + lane * kSlot;
+    int ea = 0, ec = 0;   // lanes 0..20 finish D(ea, ec), lanes 21..26 finish b
+    tri_decode(lane, ea, ec);
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total_nodes; g += warps) {
         const uint32_t s = node_scene[g];
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
-        const float lam2[3] = {sc.lam_depth * sc.lam_depth, sc.lam_of * sc.lam_of, sc.lam_of * sc.lam_of};
-        const float reg2 = sc.lam_reg * sc.lam_reg;
-        const float node2 = sc.lam_node * sc.lam_node;
-        DAcc D[21];
-        float b[6];
-#pragma unroll
-        for (int i = 0; i < 21; ++i) D[i] = DAcc(0);
-#pragma unroll
-        for (int i = 0; i < 6; ++i) b[i] = 0.f;
+        const float lam_d = sc.lam_depth, lam_of = sc.lam_of, lam_r = sc.lam_reg, lam_n = sc.lam_node;
+        const bool motion = lam_n != 0.f && sc.node_motion != nullptr;
+        const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * p.dense_begin);
+        const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
         const float4 c4 = centers[g];
         const float3 cen = f3(c4.x, c4.y, c4.z);
         const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
-        for (uint32_t it = beg + lane; it < end; it += 32) {
-            const uint32_t term = n2t_val[it];
-            if (term < nd) {
-                const float4 *rec = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * (p.dense_begin + term));
-                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4], r5 = rec[5], r6 = rec[6],
-                             r7 = rec[7];
-                const float gv[18] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x,
-                                      r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y};
-                const float res[3] = {r4.z, r4.w, r5.x};
-                const float wk[4] = {r5.z, r5.w, r6.x, r6.y};
-                const uint32_t ids[4] = {__float_as_uint(r6.z), __float_as_uint(r6.w), __float_as_uint(r7.x),
-                                         __float_as_uint(r7.y)};
-                int slot = 0;   // last matching slot (libs/star/opt/dense_image_jacobian.cuh:9-20)
+        DAcc D[21], B[6];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) if (ids[k] == g) slot = k;
-                const float w = wk[slot];
+        for (int i = 0; i < 21; ++i) D[i] = DAcc(0);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) B[i] = DAcc(0);
+        for (uint32_t base = beg; base < end; base += 32) {
+            const uint32_t it = base + lane;
+            const uint32_t term = it < end ? n2t_val[it] : kInvalidIndex;
+            // 1 dense, 2 regularisation edge, 3 node motion; feature terms have a zero Jacobian
+            // (PreconditionerRhsBuilder.cu:214-219)
+            int kind = 0;
+            const float4 *src = nullptr;
+            int parts = 0;
+            if (term < nd) {
+                kind = 1;
+                src = dbase + (size_t)(kDenseRecord / 4) * term;
+                parts = kDenseRecord / 4;
+            } else if (term < nd + ne) {
+                kind = 2;
+                src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
+                parts = kRegRecord / 4;
+            } else if (term < nd + ne + nn && motion) {
+                kind = 3;
+            }
+            fetch_records<kSlot>(slots, lane, src, parts);
+            __syncwarp();
+            if (kind == 1) {
+                // point-to-plane + optical-flow rows (libs/star/opt/dense_image_jacobian.cuh:9-20)
+                float wk[4];
+                uint32_t ids[4];
+                read_weights(mine, wk, ids);
+                float w = wk[0];   // weight of the last slot whose node is g
+#pragma unroll
+                for (int k = 1; k < 4; ++k) if (ids[k] == g) w = wk[k];
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) {
                     float gl[6];
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) gl[q] = gv[6 * ch + q];
-                    if (kFp64) recentre(gl, cen);
-                    float J[6];
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) J[q] = gl[q] * w;
-#pragma unroll
-                    for (int a = 0; a < 6; ++a)
-#pragma unroll
-                        for (int c = a; c < 6; ++c) D[tri_index(a, c)] += DAcc(lam2[ch] * J[a]) * DAcc(J[c]);
-                    const float ow = lam2[ch] * (w * w);
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) b[q] -= (ow * res[ch]) * gl[q];
+                    const float res = read_channel(mine, ch, gl);
+                    if (kCentred) recentre(gl, cen);
+                    const float scale = (ch == 0 ? lam_d : lam_of) * w;
+                    accumulate_row(D, B, gl, scale, -(scale * res));
                 }
-            } else if (term < nd + ne) {
-                const float4 *rec = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * (sc.edge_base + term - nd));
-                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
-                if (r1.w == 0.f) continue;
-                const float3 a3 = f3(r0.x, r0.y, r0.z), b3 = f3(r0.w, r1.x, r1.y);
-                const float3 rij = f3(r2.z, r2.w, r3.x);
-                const float c = r1.z;
-                const bool is_i = (__float_as_uint(r2.x) == g);
-                float J[3][6];
-                reg_unit_jacobian(a3, b3, is_i, J);
-                if (kFp64) {
+            } else if (kind == 2) {
+                // regularisation rows (node_graph_reg_jacobian.cuh:85-106, 193-233)
+                float rec[kRegRecord];
+                read_slot<kRegRecord / 4>(mine, rec);
+                if (rec[7] != 0.f) {
+                    const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
+                    float J[3][6];
+                    reg_unit_jacobian(a3, b3, __float_as_uint(rec[8]) == g, J);
+                    const float scale = lam_r * rec[6];
 #pragma unroll
-                    for (int ch = 0; ch < 3; ++ch) recentre(J[ch], cen);
-                }
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    float Jc[6];
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) Jc[q] = J[ch][q] * c;
-#pragma unroll
-                    for (int a = 0; a < 6; ++a)
-#pragma unroll
-                        for (int cc = a; cc < 6; ++cc) D[tri_index(a, cc)] += DAcc(reg2 * Jc[a]) * DAcc(Jc[cc]);
-                }
-                // computeRegTermJtResidual (node_graph_reg_jacobian.cuh:193-233)
-                const float c2 = c * c;
-                const float rv[3] = {rij.x * c2, rij.y * c2, rij.z * c2};
-#pragma unroll
-                for (int q = 0; q < 6; ++q) b[q] -= reg2 * (rv[0] * J[0][q] + rv[1] * J[1][q] + rv[2] * J[2][q]);
-            } else if (term < nd + ne + nn) {
-                // node-motion term (node_motion_jacobian.cuh:7-36), lambda_node = 0 by default
-                if (node2 != 0.f && sc.node_motion) {
-                    const uint32_t nl = term - nd - ne;
-                    const float4 pred = sc.node_motion[nl];
-                    const SE3f T = dq_se3(load_dq(se3 + 8ull * (sc.node_base + nl)));
-                    const float conf = pred.w, c2 = pred.w * pred.w;
-                    if (kFp64) {
-                        const float res3[3] = {T.t.x - pred.x, T.t.y - pred.y, T.t.z - pred.z};
-#pragma unroll
-                        for (int ch = 0; ch < 3; ++ch) {
-                            float J[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                            J[3 + ch] = conf;
-                            recentre(J, cen);
-#pragma unroll
-                            for (int a = 0; a < 6; ++a)
-#pragma unroll
-                                for (int c = a; c < 6; ++c) D[tri_index(a, c)] += DAcc(node2 * J[a]) * DAcc(J[c]);
-#pragma unroll
-                            for (int q = 0; q < 6; ++q) b[q] -= node2 * res3[ch] * conf * J[q];
-                        }
-                    } else {
-                        D[tri_index(3, 3)] += DAcc((node2 * conf) * conf);
-                        D[tri_index(4, 4)] += DAcc((node2 * conf) * conf);
-                        D[tri_index(5, 5)] += DAcc((node2 * conf) * conf);
-                        b[3] -= node2 * ((T.t.x - pred.x) * c2);
-                        b[4] -= node2 * ((T.t.y - pred.y) * c2);
-                        b[5] -= node2 * ((T.t.z - pred.z) * c2);
+                    for (int ch = 0; ch < 3; ++ch) {
+                        if (kCentred) recentre(J[ch], cen);
+                        accumulate_row(D, B, J[ch], scale, -(scale * rec[10 + ch]));
                     }
                 }
+            } else if (kind == 3) {
+                // node-motion rows (node_motion_jacobian.cuh:7-36), lambda_node = 0 by default
+                const uint32_t nl = term - nd - ne;
+                const float4 pred = sc.node_motion[nl];
+                const SE3f T = dq_se3(load_dq(se3 + 8ull * (sc.node_base + nl)));
+                const float res3[3] = {T.t.x - pred.x, T.t.y - pred.y, T.t.z - pred.z};
+                const float scale = lam_n * pred.w;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    float J[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                    J[3 + ch] = 1.f;
+                    if (kCentred) recentre(J, cen);
+                    accumulate_row(D, B, J, scale, -(scale * res3[ch]));
+                }
             }
-            // feature terms: zero Jacobian (PreconditionerRhsBuilder.cu:214-219)
+            __syncwarp();
         }
+        // lane partial sums -> slots; lane e sums entry e over the lanes in lane order
+        DAcc *part = reinterpret_cast<DAcc *>(mine);
 #pragma unroll
-        for (int i = 0; i < 21; ++i) D[i] = warp_sum(D[i]);
+        for (int i = 0; i < 21; ++i) part[i] = D[i];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) b[i] = warp_sum(b[i]);
-        // +1e-3 on the diagonal of the origin-twist block (PreconditionerRhsBuilder.cu:249-252);
-        // for node-centred twists the same term is 1e-3 S^T S, S = [[I, 0], [[c]x, I]]
-        if (kFp64) {
-            const DAcc eps = DAcc(1e-3f), cx = cen.x, cy = cen.y, cz = cen.z;
-            const DAcc c2 = cx * cx + cy * cy + cz * cz;
-            const DAcc cv[3] = {cx, cy, cz};
-            const DAcc X[3][3] = {{0, -cz, cy}, {cz, 0, -cx}, {-cy, cx, 0}};
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-#pragma unroll
-                for (int c = a; c < 3; ++c) D[tri_index(a, c)] += eps * ((a == c ? DAcc(1) + c2 : DAcc(0)) - cv[a] * cv[c]);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) D[tri_index(a, 3 + c)] += -eps * X[a][c];
-                D[tri_index(3 + a, 3 + a)] += eps;
+        for (int i = 0; i < 6; ++i) part[21 + i] = B[i];
+        __syncwarp();
+        DAcc acc = DAcc(0);
+        if (lane < 27) {
+#pragma unroll 8
+            for (int l = 0; l < 32; ++l) acc += reinterpret_cast<const DAcc *>(slots + l * kSlot)[lane];
+        }
+        __syncwarp();
+        if (lane < 21) {
+            acc += regulariser_entry<DAcc>(ea, ec, cen, kCentred);
+            const uint32_t slot = rowptr[g];
+            if (slot < cap_blocks) {
+                float *blk = blocks + 36ull * slot;
+                blk[6 * ea + ec] = (float)acc;
+                blk[6 * ec + ea] = (float)acc;
             }
-        } else {
-#pragma unroll
-            for (int a = 0; a < 6; ++a) D[tri_index(a, a)] += DAcc(1e-3f);
-        }
-        float full[36];
-#pragma unroll
-        for (int a = 0; a < 6; ++a)
-#pragma unroll
-            for (int c = 0; c < 6; ++c) full[6 * a + c] = (float)((a <= c) ? D[tri_index(a, c)] : D[tri_index(c, a)]);
-        const uint32_t slot = rowptr[g];
-        if (slot < cap_blocks && lane < 9) {
-            float4 v = make_float4(full[4 * lane], full[4 * lane + 1], full[4 * lane + 2], full[4 * lane + 3]);
-            reinterpret_cast<float4 *>(blocks + 36ull * slot)[lane] = v;
-        }
-        if (lane < 2) {
-            reinterpret_cast<float4 *>(jtr + 8ull * g)[lane] =
-                lane == 0 ? make_float4(b[0], b[1], b[2], b[3]) : make_float4(b[4], b[5], 0.f, 0.f);
-        }
-        if (lane == 0) {
-            bool bad = false;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) bad |= isnan(b[i]);
-            if (bad) set_err(err, WS_ERR_NAN);
-            float inv[36];
-            if (kFp64) {
-                double Dd[36];
-#pragma unroll
-                for (int a = 0; a < 6; ++a)
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) Dd[6 * a + c] = (double)((a <= c) ? D[tri_index(a, c)] : D[tri_index(c, a)]);
-                cholesky6_fp64(Dd, inv);
-            } else {
-                gauss_jordan6(full, inv);
-            }
-            float4 *o = reinterpret_cast<float4 *>(inv_diag + 36ull * g);
-#pragma unroll
-            for (int i = 0; i < 9; ++i) o[i] = make_float4(inv[4 * i], inv[4 * i + 1], inv[4 * i + 2], inv[4 * i + 3]);
+            if (kCentred) diag64[21ull * g + lane] = (double)acc;
+        } else if (lane < 29) {
+            const float bq = lane < 27 ? (float)acc : 0.f;
+            jtr[8ull * g + (lane - 21)] = bq;
+            if (isnan(bq)) set_err(err, WS_ERR_NAN);
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Off-diagonal blocks, once per unordered node pair (computeJtJNonDiagonalBlockKernel,
-// examples/mono_star/opt/JtJMaterializer.cu:66-174): A_ij goes to the (i, j) slot and
-// its transpose to the (j, i) slot.  A[6*i+a][6*j+c] = sum lambda^2 (J_i^T J_j)[a][c].
+// Block-diagonal preconditioner, one thread per node: FP64 Cholesky of the FP64
+// accumulated block (mixed precision) or the reference's FP32 Gauss-Jordan with
+// partial pivoting of the stored block (BlockDiagonalPreconditionerInverse.cuh:14-73).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_assemble_pair(const Scene *scenes, const Plan *plan,
-                                                        const uint32_t *node_scene, const uint32_t *counts,
-                                                        const uint32_t *half_row, const uint32_t *half_col,
-                                                        const uint32_t *half_begin, const uint32_t *half_end,
-                                                        const uint32_t *pair_val, const uint32_t *slot_up,
-                                                        const uint32_t *slot_lo, const float *drec, const float *rrec,
-                                                        const float4 *centers, int centred, float *blocks) {
+__global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, const float *blocks,
+                                                       const uint32_t *rowptr, uint32_t total_nodes,
+                                                       uint32_t cap_blocks, int fp64, float *inv_diag) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
+        float inv[36];
+        if (fp64) {
+            double Dd[36];
+            const double *src = diag64 + 21ull * g;
+#pragma unroll
+            for (int a = 0; a < 6; ++a)
+#pragma unroll
+                for (int c = a; c < 6; ++c) {
+                    const double v = src[tri_index(a, c)];
+                    Dd[6 * a + c] = v;
+                    Dd[6 * c + a] = v;
+                }
+            cholesky6_fp64(Dd, inv);
+        } else {
+            const uint32_t slot = rowptr[g];
+            float full[36];
+            if (slot < cap_blocks) {
+#pragma unroll
+                for (int i = 0; i < 36; ++i) full[i] = blocks[36ull * slot + i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 36; ++i) full[i] = (i % 7 == 0) ? 1.f : 0.f;
+            }
+            gauss_jordan6(full, inv);
+        }
+        float4 *o = reinterpret_cast<float4 *>(inv_diag + 36ull * g);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) o[i] = make_float4(inv[4 * i], inv[4 * i + 1], inv[4 * i + 2], inv[4 * i + 3]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Off-diagonal blocks, once per unordered node pair (i < j) over the pair's term list
+// (computeDenseImageJtJBlockJacobian, dense_image_jacobian.cuh:82-126; computeRegJtJLocalBlock,
+// node_graph_reg_jacobian.cuh:273-358), written to the upper slot and transposed to the lower.
+// Each term gives three row pairs (u_i, u_j), the scaled Jacobian rows of the two nodes, and
+// A = sum u_i u_j^T.  Lanes take terms, sum their products in registers, and the 36 entries
+// are then summed over the lanes in lane order through shared memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, const float *uc, float si, float sj) {
+    float a[6], c[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        a[q] = si * ur[q];
+        c[q] = sj * uc[q];
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) A[6 * i + j] += a[i] * c[j];
+}
+
+__global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_pair(
+    const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
+    const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
+    const uint32_t *pair_val, const uint32_t *slot_up, const uint32_t *slot_lo, const float *drec,
+    const float *rrec, const float4 *centers, int centred, float *blocks) {
+    constexpr int kSlot = kSlotWordsF32;
+    static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
+    __shared__ __align__(16) float stage[kAssembleThreads / 32][32 * kSlot];
     const int lane = threadIdx.x & 31;
+    float *slots = stage[threadIdx.x >> 5];
+    float *mine = slots + lane * kSlot;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nhalf = counts[kCntHalf];
     for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < nhalf; h += warps) {
+        const uint32_t su = slot_up[h], sl = slot_lo[h];
+        if (su == kInvalidIndex) continue;
         const uint32_t row = half_row[h], col = half_col[h];
         const uint32_t s = node_scene[row];
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges;
-        const float lam2[3] = {sc.lam_depth * sc.lam_depth, sc.lam_of * sc.lam_of, sc.lam_of * sc.lam_of};
-        const float reg2 = sc.lam_reg * sc.lam_reg;
+        const float lam_d = sc.lam_depth, lam_of = sc.lam_of, lam_r = sc.lam_reg;
+        const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * p.dense_begin);
+        const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
+        const float4 cr4 = centers[row], cc4 = centers[col];
+        const float3 c_row = f3(cr4.x, cr4.y, cr4.z), c_col = f3(cc4.x, cc4.y, cc4.z);
+        const uint32_t end = half_end[h];
         float A[36];
 #pragma unroll
         for (int i = 0; i < 36; ++i) A[i] = 0.f;
-        const float4 cr4 = centers[row], cc4 = centers[col];
-        const float3 c_row = f3(cr4.x, cr4.y, cr4.z), c_col = f3(cc4.x, cc4.y, cc4.z);
-        for (uint32_t it = half_begin[h] + lane; it < half_end[h]; it += 32) {
-            const uint32_t term = pair_val[it];
+        for (uint32_t base = half_begin[h]; base < end; base += 32) {
+            const uint32_t it = base + lane;
+            const uint32_t term = it < end ? pair_val[it] : kInvalidIndex;
+            int kind = 0;   // 1 dense, 2 regularisation edge; node-motion terms own no pairs
+            const float4 *src = nullptr;
+            int parts = 0;
             if (term < nd) {
-                const float4 *rec = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * (p.dense_begin + term));
-                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4], r5 = rec[5], r6 = rec[6],
-                             r7 = rec[7];
-                const float gv[18] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x,
-                                      r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y};
-                const float wk[4] = {r5.z, r5.w, r6.x, r6.y};
-                const uint32_t ids[4] = {__float_as_uint(r6.z), __float_as_uint(r6.w), __float_as_uint(r7.x),
-                                         __float_as_uint(r7.y)};
-                int si = 0, sj = 0;   // computeDenseImageJtJBlockJacobian (dense_image_jacobian.cuh:82-126)
+                kind = 1;
+                src = dbase + (size_t)(kDenseRecord / 4) * term;
+                parts = kDenseRecord / 4;
+            } else if (term < nd + ne) {
+                kind = 2;
+                src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
+                parts = kRegRecord / 4;
+            }
+            fetch_records<kSlot>(slots, lane, src, parts);
+            __syncwarp();
+            if (kind == 1) {
+                float wk[4];
+                uint32_t ids[4];
+                read_weights(mine, wk, ids);
+                float wi = wk[0], wj = wk[0];   // last matching slots
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (ids[k] == row) si = k;
-                    if (ids[k] == col) sj = k;
+                for (int k = 1; k < 4; ++k) {
+                    if (ids[k] == row) wi = wk[k];
+                    if (ids[k] == col) wj = wk[k];
                 }
-                const float wij = wk[si] * wk[sj];
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) {
-                    const float f = lam2[ch] * wij;
                     float gr[6], gc[6];
+                    read_channel(mine, ch, gr);
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) gr[q] = gc[q] = gv[6 * ch + q];
+                    for (int q = 0; q < 6; ++q) gc[q] = gr[q];
                     if (centred) {
                         recentre(gr, c_row);
                         recentre(gc, c_col);
                     }
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) {
-                        const float fa = f * gr[a];
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) A[6 * a + c] += fa * gc[c];
-                    }
+                    const float lam = ch == 0 ? lam_d : lam_of;
+                    accumulate_pair_row(A, gr, gc, lam * wi, lam * wj);
                 }
-            } else if (term < nd + ne) {
-                // computeRegJtJLocalBlock (libs/star/opt/node_graph_reg_jacobian.cuh:273-358)
-                const float4 *rec = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * (sc.edge_base + term - nd));
-                const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2];
-                if (r1.w == 0.f) continue;
-                const float3 a3 = f3(r0.x, r0.y, r0.z), b3 = f3(r0.w, r1.x, r1.y);
-                const float c = r1.z;
-                const uint32_t ei = __float_as_uint(r2.x);
-                float Jr[3][6], Jc[3][6];
-                reg_unit_jacobian(a3, b3, row == ei, Jr);
-                reg_unit_jacobian(a3, b3, col == ei, Jc);
-                if (centred) {
+            } else if (kind == 2) {
+                float rec[kRegRecord];
+                read_slot<kRegRecord / 4>(mine, rec);
+                if (rec[7] != 0.f) {
+                    const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
+                    const uint32_t ei = __float_as_uint(rec[8]);
+                    float Jr[3][6], Jc[3][6];
+                    reg_unit_jacobian(a3, b3, row == ei, Jr);
+                    reg_unit_jacobian(a3, b3, col == ei, Jc);
+                    const float scale = lam_r * rec[6];
 #pragma unroll
                     for (int ch = 0; ch < 3; ++ch) {
-                        recentre(Jr[ch], c_row);
-                        recentre(Jc[ch], c_col);
+                        if (centred) {
+                            recentre(Jr[ch], c_row);
+                            recentre(Jc[ch], c_col);
+                        }
+                        accumulate_pair_row(A, Jr[ch], Jc[ch], scale, scale);
                     }
                 }
-                const float ws = reg2 * (c * c);
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch)
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) {
-                        const float fa = ws * Jr[ch][a];
-#pragma unroll
-                        for (int cc = 0; cc < 6; ++cc) A[6 * a + cc] += fa * Jc[ch][cc];
-                    }
             }
-            // node-motion terms own no pairs; feature terms have zero Jacobian
+            __syncwarp();
         }
 #pragma unroll
-        for (int i = 0; i < 36; ++i) A[i] = warp_sum(A[i]);
-        const uint32_t su = slot_up[h], sl = slot_lo[h];
-        if (su == kInvalidIndex) continue;
-        if (lane < 9) {
-            reinterpret_cast<float4 *>(blocks + 36ull * su)[lane] =
-                make_float4(A[4 * lane], A[4 * lane + 1], A[4 * lane + 2], A[4 * lane + 3]);
-        } else if (lane < 18) {
-            const int q = lane - 9;
-            float v[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int idx = 4 * q + e, a = idx / 6, c = idx % 6;
-                v[e] = A[6 * c + a];
-            }
-            reinterpret_cast<float4 *>(blocks + 36ull * sl)[q] = make_float4(v[0], v[1], v[2], v[3]);
+        for (int i = 0; i < 9; ++i)
+            *reinterpret_cast<float4 *>(mine + 4 * i) = make_float4(A[4 * i], A[4 * i + 1], A[4 * i + 2], A[4 * i + 3]);
+        __syncwarp();
+        float acc0 = 0.f, acc1 = 0.f;   // entries lane and 32 + lane (lanes 0..3)
+#pragma unroll 8
+        for (int l = 0; l < 32; ++l) {
+            acc0 += slots[l * kSlot + lane];
+            if (lane < 4) acc1 += slots[l * kSlot + 32 + lane];
+        }
+        __syncwarp();
+        float *up = blocks + 36ull * su, *lo = blocks + 36ull * sl;
+        {
+            const int a = lane / 6, c = lane % 6;
+            up[lane] = acc0;
+            lo[6 * c + a] = acc0;
+        }
+        if (lane < 4) {
+            const int e = 32 + lane, a = e / 6, c = e % 6;
+            up[e] = acc1;
+            lo[6 * c + a] = acc1;
         }
     }
 }
@@ -917,22 +1053,25 @@ void gn_eval(Workspace &w, cudaStream_t st) {
 }
 
 void gn_assemble_node(Workspace &w, cudaStream_t st) {
-    const int ng = grid_for(w.total_nodes * 32u, 256, w.num_sms, 16);
+    const int ng = grid_for(w.total_nodes * 32u, kAssembleThreads, w.num_sms, 32);
     if (w.precision == WS_PREC_FP32)
-        k_assemble_node<float><<<ng, 256, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
+        k_assemble_node<float><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
                                                     w.n2t_sorted_val, w.d_record, w.r_record, w.se3, w.centers,
-                                                    w.rowptr, w.cap_blocks, w.blocks, w.inv_diag, w.jtr,
+                                                    w.rowptr, w.cap_blocks, w.blocks, w.diag64, w.jtr,
                                                     w.error_flag);
     else
-        k_assemble_node<double><<<ng, 256, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
+        k_assemble_node<double><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
                                                      w.n2t_sorted_val, w.d_record, w.r_record, w.se3, w.centers,
-                                                     w.rowptr, w.cap_blocks, w.blocks, w.inv_diag, w.jtr,
+                                                     w.rowptr, w.cap_blocks, w.blocks, w.diag64, w.jtr,
                                                      w.error_flag);
+    count_launch(w);
+    k_block_inverse<<<grid_for(w.total_nodes, 128, w.num_sms, 16), 128, 0, st>>>(
+        w.diag64, w.blocks, w.rowptr, w.total_nodes, w.cap_blocks, w.precision == WS_PREC_MIXED ? 1 : 0, w.inv_diag);
     count_launch(w);
 }
 
 void gn_assemble_pair(Workspace &w, cudaStream_t st) {
-    k_assemble_pair<<<grid_for(w.cap_half * 32u, 256, w.num_sms, 16), 256, 0, st>>>(
+    k_assemble_pair<<<grid_for(w.cap_half * 32u, kAssembleThreads, w.num_sms, 32), kAssembleThreads, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
         w.half_slot_up, w.half_slot_lo, w.d_record, w.r_record, w.centers,
         w.precision == WS_PREC_MIXED ? 1 : 0, w.blocks);

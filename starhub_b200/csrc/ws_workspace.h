@@ -80,6 +80,7 @@ struct Workspace {
 
     // per-node system and PCG state (stride kVecStride)
     float *inv_diag = nullptr;          // [cap_nodes * 36]
+    double *diag64 = nullptr;           // [cap_nodes * 21] FP64 diagonal blocks (upper triangle)
     float *jtr = nullptr, *x = nullptr, *r = nullptr, *s = nullptr, *q = nullptr;
     float *d0 = nullptr, *d1 = nullptr;
     float *se3 = nullptr;               // [cap_nodes * 8] current warp
