@@ -35,7 +35,7 @@ void free_all(ws::Workspace &w) {
                     w.n2t_val_alt, w.n2t_offset, w.pair_key, w.pair_key_alt, w.pair_val, w.pair_val_alt,
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
-                    w.col_key_alt, w.col_val_alt, w.colidx, w.blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.s, w.q,
+                    w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.s, w.q,
                     w.d0, w.d1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
                     w.error_flag};
     for (void *p : ptrs)
@@ -134,6 +134,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     w.cap_n2t = 4u * w.cap_pixels + 2u * w.cap_edges + w.cap_nodes + 4u * w.cap_features;
     w.cap_pair_kv = 6u * w.cap_pixels + w.cap_edges + 6u * w.cap_features;
     w.cap_half = std::min<uint32_t>(w.cap_pair_kv, 64u * w.cap_nodes);
+    w.cap_half = std::min<uint32_t>(w.cap_half, ws::kRefTransposed - 1u);
     w.cap_blocks = w.cap_nodes + 2u * w.cap_half;
     const uint32_t sort_cap = std::max(std::max(w.cap_n2t, w.cap_pair_kv), w.cap_half);
     const uint32_t scan_cap = std::max(std::max(w.cap_pair_kv, w.cap_nodes), w.cap_tiles) + 1;
@@ -183,7 +184,10 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.col_key_alt, w.cap_half));
     A(dalloc(&w.col_val_alt, w.cap_half));
     A(dalloc(&w.colidx, w.cap_blocks));
-    A(dalloc(&w.blocks, (size_t)w.cap_blocks * 36));
+    A(dalloc(&w.entry_ref, w.cap_blocks));
+    A(dalloc(&w.entry_info, w.cap_blocks));
+    A(dalloc(&w.diag_blocks, (size_t)w.cap_nodes * 36));
+    A(dalloc(&w.pair_blocks, (size_t)std::max<uint32_t>(1u, w.cap_half) * 36));
     A(dalloc(&w.inv_diag, (size_t)w.cap_nodes * 36));
     A(dalloc(&w.diag64, (size_t)w.cap_nodes * 21));
     for (float **v : {&w.jtr, &w.x, &w.r, &w.s, &w.q, &w.d0, &w.d1}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
@@ -203,13 +207,16 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
         A(cudaMemset(w.scene_counter, 0, 2ull * w.cap_scenes * sizeof(uint32_t)));
         A(cudaMemset(w.se3, 0, (size_t)w.cap_nodes * 8 * sizeof(float)));
     }
+    if (e == cudaSuccess) {
+        w.pcg_grid = ws::pcg_max_blocks(w.device);
+        A(dalloc(&w.pcg_warp_groups, (size_t)w.pcg_grid * ws::pcg_warps_per_block() + 1));
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         free_all(w);
         delete h;
         return e == cudaErrorMemoryAllocation ? WS_ERR_CAPACITY : WS_ERR_CUDA;
     }
-    w.pcg_grid = ws::pcg_max_blocks(w.device);
     *out = h;
     return WS_OK;
 }
@@ -696,7 +703,33 @@ int ws_get_system(ws_solver *h, int scene, uint32_t *rowptr, uint32_t *cols, flo
         const auto ci = download(w.colidx + b, e - b);
         for (uint32_t i = 0; i < e - b; ++i) cols[i] = ci[i] - (uint32_t)sc.node_base;
     }
-    if (blocks) cudaMemcpy(blocks, w.blocks + 36ull * b, 144ull * (e - b), cudaMemcpyDeviceToHost);
+    if (blocks) {
+        // expand the symmetric store (diagonal per node, one block per pair) into full block-CSR rows
+        const auto ref = download(w.entry_ref + b, e - b);
+        const auto diag = download(w.diag_blocks + 36ull * sc.node_base, 36ull * sc.num_nodes);
+        uint32_t hmin = 0xFFFFFFFFu, hmax = 0;
+        for (uint32_t r : ref)
+            if (r != ws::kInvalidIndex) {
+                hmin = std::min(hmin, r & ~ws::kRefTransposed);
+                hmax = std::max(hmax, r & ~ws::kRefTransposed);
+            }
+        std::vector<float> pb;
+        if (hmin <= hmax) pb = download(w.pair_blocks + 36ull * hmin, 36ull * (hmax - hmin + 1));
+        for (int i = 0; i < sc.num_nodes; ++i)
+            for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+                float *out = blocks + 36ull * (k - b);
+                if (k == rp[i]) {
+                    std::copy(diag.begin() + 36ull * i, diag.begin() + 36ull * (i + 1), out);
+                    continue;
+                }
+                const uint32_t r = ref[k - b];
+                if (r == ws::kInvalidIndex) return WS_ERR_CAPACITY;
+                const float *src = pb.data() + 36ull * ((r & ~ws::kRefTransposed) - hmin);
+                const bool tr = (r & ws::kRefTransposed) != 0;
+                for (int a = 0; a < 6; ++a)
+                    for (int c = 0; c < 6; ++c) out[6 * a + c] = tr ? src[6 * c + a] : src[6 * a + c];
+            }
+    }
     if (inv_diag) cudaMemcpy(inv_diag, w.inv_diag + 36ull * sc.node_base, 144ull * sc.num_nodes, cudaMemcpyDeviceToHost);
     auto vec6 = [&](const float *src, float *dst) {
         const auto v = download(src + 8ull * sc.node_base, 8ull * sc.num_nodes);

@@ -347,7 +347,7 @@ __global__ void k_col_kv(const uint32_t *half_col, const uint32_t *counts, uint3
 __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, const uint32_t *counts,
                         const uint32_t *half_row, const uint32_t *half_col, const uint32_t *row_first,
                         const uint32_t *row_cnt_lo, const uint32_t *rowptr, uint32_t cap_blocks,
-                        uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx, int *err) {
+                        uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx, uint32_t *entry_ref, int *err) {
     const uint32_t n = counts[kCntHalf];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t col = sorted_col[k];
@@ -370,15 +370,46 @@ __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, co
         slot_up[h] = s_up;
         colidx[s_lo] = row;
         colidx[s_up] = half_col[h];
+        entry_ref[s_up] = h;
+        entry_ref[s_lo] = h | kRefTransposed;
     }
 }
 
-__global__ void k_diag_cols(const uint32_t *rowptr, uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx,
-                            int *err) {
+// Diagonal slot of every row, plus the packed (col, ref, row, scene) record of each slot of
+// the row that the PCG streams.
+__global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *node_scene, uint32_t total_nodes,
+                            uint32_t cap_blocks, uint32_t *colidx, uint32_t *entry_ref, uint4 *entry_info, int *err) {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         const uint32_t s = rowptr[g];
-        if (s < cap_blocks) colidx[s] = g;
+        const uint32_t e = min(rowptr[g + 1], cap_blocks);
+        const uint32_t scene = node_scene[g];
+        if (s < cap_blocks) {
+            colidx[s] = g;
+            entry_ref[s] = kInvalidIndex;   // the diagonal block lives in diag_blocks[g]
+        }
+        for (uint32_t k = s; k < e; ++k) entry_info[k] = make_uint4(colidx[k], entry_ref[k], g, scene);
         if (g + 1 == total_nodes && rowptr[total_nodes] > cap_blocks) set_error(err, WS_ERR_CAPACITY);
+    }
+}
+
+// First row group of every PCG warp, chosen so that the warps' slot ranges are about equal:
+// warp w starts at the first group whose first slot is at or past w / warps of all slots.
+__global__ void k_pcg_ranges(const uint32_t *rowptr, const uint32_t *group_row, uint32_t groups,
+                             uint32_t total_nodes, uint32_t cap_blocks, uint32_t warps, uint32_t *warp_groups) {
+    const uint32_t total = min(rowptr[total_nodes], cap_blocks);
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w <= warps; w += gridDim.x * blockDim.x) {
+        if (w == warps) {
+            warp_groups[w] = groups;
+            continue;
+        }
+        const uint32_t target = (uint32_t)(((unsigned long long)total * w) / warps);
+        uint32_t lo = 0, hi = groups;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (rowptr[min(group_row[mid], total_nodes)] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        warp_groups[w] = lo;
     }
 }
 
@@ -445,10 +476,14 @@ void index_build(Workspace &w, cudaStream_t st) {
     const uint32_t *sh = col_alt ? w.col_val_alt : w.col_val;
     k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,
                                                                     w.row_first, w.row_cnt_lo, w.rowptr, w.cap_blocks,
-                                                                    w.half_slot_up, w.half_slot_lo, w.colidx,
+                                                                    w.half_slot_up, w.half_slot_lo, w.colidx, w.entry_ref,
                                                                     w.error_flag);
-    k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, N, w.cap_blocks, w.colidx, w.error_flag);
-    count_launch(w, 2);
+    k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.node_scene, N, w.cap_blocks, w.colidx,
+                                                             w.entry_ref, w.entry_info, w.error_flag);
+    const uint32_t warps = (uint32_t)(pcg_launch_blocks(w) * pcg_warps_per_block());
+    k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.chunk_row, w.total_chunks, N,
+                                                                      w.cap_blocks, warps, w.pcg_warp_groups);
+    count_launch(w, 3);
 }
 
 }  // namespace ws

@@ -414,8 +414,8 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_node(const Sce
                                                                      const uint32_t *n2t_offset, const uint32_t *n2t_val,
                                                                      const float *drec, const float *rrec,
                                                                      const float *se3, const float4 *centers,
-                                                                     const uint32_t *rowptr, uint32_t cap_blocks,
-                                                                     float *blocks, double *diag64, float *jtr, int *err) {
+                                                                     float *diag_blocks, double *diag64, float *jtr,
+                                                                     int *err) {
     constexpr bool kCentred = sizeof(DAcc) == 8;   // mixed precision also uses node-centred twists
     constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;
     static_assert(27 * sizeof(DAcc) <= 4 * kSlot, "a slot holds one lane's 27 partial sums");
@@ -527,12 +527,9 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_node(const Sce
         __syncwarp();
         if (lane < 21) {
             acc += regulariser_entry<DAcc>(ea, ec, cen, kCentred);
-            const uint32_t slot = rowptr[g];
-            if (slot < cap_blocks) {
-                float *blk = blocks + 36ull * slot;
-                blk[6 * ea + ec] = (float)acc;
-                blk[6 * ec + ea] = (float)acc;
-            }
+            float *blk = diag_blocks + 36ull * g;
+            blk[6 * ea + ec] = (float)acc;
+            blk[6 * ec + ea] = (float)acc;
             if (kCentred) diag64[21ull * g + lane] = (double)acc;
         } else if (lane < 29) {
             const float bq = lane < 27 ? (float)acc : 0.f;
@@ -547,9 +544,8 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_node(const Sce
 // accumulated block (mixed precision) or the reference's FP32 Gauss-Jordan with
 // partial pivoting of the stored block (BlockDiagonalPreconditionerInverse.cuh:14-73).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, const float *blocks,
-                                                       const uint32_t *rowptr, uint32_t total_nodes,
-                                                       uint32_t cap_blocks, int fp64, float *inv_diag) {
+__global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, const float *diag_blocks,
+                                                       uint32_t total_nodes, int fp64, float *inv_diag) {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         float inv[36];
         if (fp64) {
@@ -565,15 +561,9 @@ __global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, con
                 }
             cholesky6_fp64(Dd, inv);
         } else {
-            const uint32_t slot = rowptr[g];
             float full[36];
-            if (slot < cap_blocks) {
 #pragma unroll
-                for (int i = 0; i < 36; ++i) full[i] = blocks[36ull * slot + i];
-            } else {
-#pragma unroll
-                for (int i = 0; i < 36; ++i) full[i] = (i % 7 == 0) ? 1.f : 0.f;
-            }
+            for (int i = 0; i < 36; ++i) full[i] = diag_blocks[36ull * g + i];
             gauss_jordan6(full, inv);
         }
         float4 *o = reinterpret_cast<float4 *>(inv_diag + 36ull * g);
@@ -585,7 +575,8 @@ __global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, con
 // ---------------------------------------------------------------------------
 // Off-diagonal blocks, once per unordered node pair (i < j) over the pair's term list
 // (computeDenseImageJtJBlockJacobian, dense_image_jacobian.cuh:82-126; computeRegJtJLocalBlock,
-// node_graph_reg_jacobian.cuh:273-358), written to the upper slot and transposed to the lower.
+// node_graph_reg_jacobian.cuh:273-358), stored once per pair; the lower-triangle CSR entry reads
+// it transposed.
 // Each term gives three row pairs (u_i, u_j), the scaled Jacobian rows of the two nodes, and
 // A = sum u_i u_j^T.  Lanes take terms, sum their products in registers, and the 36 entries
 // are then summed over the lanes in lane order through shared memory.
@@ -606,8 +597,8 @@ __device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, c
 __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
-    const uint32_t *pair_val, const uint32_t *slot_up, const uint32_t *slot_lo, const float *drec,
-    const float *rrec, const float4 *centers, int centred, float *blocks) {
+    const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
+    const float4 *centers, int centred, float *pair_blocks) {
     constexpr int kSlot = kSlotWordsF32;
     static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
     __shared__ __align__(16) float stage[kAssembleThreads / 32][32 * kSlot];
@@ -617,8 +608,7 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_pair(
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nhalf = counts[kCntHalf];
     for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < nhalf; h += warps) {
-        const uint32_t su = slot_up[h], sl = slot_lo[h];
-        if (su == kInvalidIndex) continue;
+        if (slot_up[h] == kInvalidIndex) continue;   // capacity overflow, already flagged
         const uint32_t row = half_row[h], col = half_col[h];
         const uint32_t s = node_scene[row];
         const Scene &sc = scenes[s];
@@ -706,17 +696,9 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_pair(
             if (lane < 4) acc1 += slots[l * kSlot + 32 + lane];
         }
         __syncwarp();
-        float *up = blocks + 36ull * su, *lo = blocks + 36ull * sl;
-        {
-            const int a = lane / 6, c = lane % 6;
-            up[lane] = acc0;
-            lo[6 * c + a] = acc0;
-        }
-        if (lane < 4) {
-            const int e = 32 + lane, a = e / 6, c = e % 6;
-            up[e] = acc1;
-            lo[6 * c + a] = acc1;
-        }
+        float *blk = pair_blocks + 36ull * h;   // row-major, rows of node `row`, columns of node `col`
+        blk[lane] = acc0;
+        if (lane < 4) blk[32 + lane] = acc1;
     }
 }
 
@@ -735,26 +717,29 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_pair(
 // therefore never depend on the rest of the batch.  One bounded grid barrier
 // ends each phase; a timed-out wait sets WS_ERR_TIMEOUT and every block leaves.
 // ---------------------------------------------------------------------------
-constexpr int kPcgThreads = 256;   // 8 warps per block
 
 struct PcgArgs {
     const Scene *scenes;
     const uint32_t *group_scene, *group_row;
     uint32_t total_groups;
-    const uint32_t *rowptr, *colidx;
-    const float *blocks, *inv_diag, *jtr;
+    const uint32_t *rowptr, *colidx, *entry_ref;
+    const uint4 *entry_info;
+    const uint32_t *warp_groups;   // [warps + 1] first row group of each warp
+    const float *diag_blocks, *pair_blocks, *inv_diag, *jtr;
     float *x, *r, *s, *q, *d0, *d1;
     double *group_partial;
     double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
     uint32_t *scene_counter;  // per scene: [0] phase A, [1] phase B / init
     uint32_t *barrier;        // [0] arrive count, [1] generation
-    uint32_t cap_blocks, total_nodes;
+    uint32_t cap_blocks, cap_half, total_nodes, num_scenes;
     int *err;
     float *se3;
     const float4 *centers;
     int pcg_iters;
     int fp64;                 // FP64 reductions and node-centred twists
 };
+
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // requested sleep, about two seconds
 
 __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
     __syncthreads();
@@ -770,10 +755,15 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
-            unsigned long long spins = 0;
+            // exponential backoff keeps the polling of early arrivals from loading the L2 slice
+            // that holds the barrier word while other blocks are still working
+            unsigned long long waited_ns = 0;
+            unsigned sleep_ns = 64;
             while (*gen == my_gen) {
-                if (++spins > kSpinLimit) { set_err(err, WS_ERR_TIMEOUT); ok = 0; break; }
-                __nanosleep(32);
+                if (waited_ns > kBarrierTimeoutNs) { set_err(err, WS_ERR_TIMEOUT); ok = 0; break; }
+                __nanosleep(sleep_ns);
+                waited_ns += sleep_ns;
+                sleep_ns = min(sleep_ns * 2u, 256u);
             }
         }
         __threadfence();
@@ -786,39 +776,29 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
 __device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
 
-// Publishes a group partial; the last group of the scene reduces the scene.
+// ---------------------------------------------------------------------------
+// Scene reductions.  Every row group writes its partial to group_partial[g]; a warp then
+// publishes all groups of its range at once: one fence, and per scene one atomicAdd of the
+// number of its groups in that scene.  The arrival that completes the scene's count sums
+// the scene's partials in group order (so the value does not depend on who arrives last)
+// and updates the scene scalars.
 // mode 0: alpha = delta / sum;  mode 1: beta = sum / delta, delta = sum;  mode 2 (init): delta = sum, beta = 0.
-__device__ __forceinline__ void publish_group(const PcgArgs &A, uint32_t group, uint32_t scene, double part,
-                                              int mode, int lane) {
-    int last = 0;
-    if (lane == 0) {
-        A.group_partial[group] = part;
-        __threadfence();
-        const uint32_t ctr = (mode == 0) ? 0u : 1u;
-        const Scene &sc = A.scenes[scene];
-        const uint32_t ticket = atomicAdd(&A.scene_counter[2 * scene + ctr], 1u);
-        last = (ticket == (uint32_t)sc.num_chunks - 1u) ? 1 : 0;
-        if (last) {
-            atomicExch(&A.scene_counter[2 * scene + ctr], 0u);
-            __threadfence();
-        }
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (!last) return;
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reduce_scene(const PcgArgs &A, uint32_t scene, int mode, int lane) {
     const Scene &sc = A.scenes[scene];
     double v = 0.0;
-    for (int c = lane; c < sc.num_chunks; c += 32) v += ldcg(A.group_partial + sc.chunk_base + c);
+    for (int c = lane; c < sc.num_chunks; c += 32) v += __ldcg(A.group_partial + sc.chunk_base + c);
     v = warp_sum(v);
     if (lane == 0) {
         double *S = A.scalars + 8ull * scene;
         if (!A.fp64) v = (double)(float)v;
         if (mode == 0) {
-            const double delta = ldcg(S + 0);
+            const double delta = __ldcg(S + 0);
             double alpha = (v != 0.0) ? delta / v : 0.0;
             if (!A.fp64 && v != 0.0) alpha = (double)((float)delta / (float)v);
             S[1] = alpha;
         } else {
-            const double delta_old = ldcg(S + 0);
+            const double delta_old = __ldcg(S + 0);
             double beta = (delta_old != 0.0) ? v / delta_old : 0.0;
             if (!A.fp64 && delta_old != 0.0) beta = (double)((float)v / (float)delta_old);
             S[2] = (mode == 2) ? 0.0 : beta;
@@ -829,154 +809,393 @@ __device__ __forceinline__ void publish_group(const PcgArgs &A, uint32_t group, 
     }
 }
 
-// Lane map inside a warp: lanes 2n and 2n+1 own node r0+n of the 16-row group, each
-// three scalar rows (half 0: rows 0-2, half 1: rows 3-5 of the 6x6 block row).
-__device__ __forceinline__ double lane_dot3(const PcgArgs &A, const float *u, const float *v, bool valid) {
-    double p = 0.0;
-    if (valid) {
-        if (A.fp64) p = (double)u[0] * (double)v[0] + (double)u[1] * (double)v[1] + (double)u[2] * (double)v[2];
-        else p = (double)(u[0] * v[0] + u[1] * v[1] + u[2] * v[2]);
+__device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, int mode, int lane) {
+    if (g_begin >= g_end) return;
+    if (lane == 0) __threadfence();   // this warp's group partials (written by lanes 0 and 16) first
+    __syncwarp();
+    const uint32_t ctr = (mode == 0) ? 0u : 1u;
+    for (uint32_t base = g_begin; base < g_end; base += 32) {
+        const uint32_t g = base + lane;
+        const uint32_t sc = g < g_end ? A.group_scene[g] : kInvalidIndex;
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, sc, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, g < g_end && (lane == 0 || prev != sc));
+        const unsigned inside = __ballot_sync(0xffffffffu, g < g_end);
+        for (unsigned m = starts; m; m &= m - 1) {
+            const int s0 = __ffs(m) - 1;
+            const unsigned later = m & (m - 1);
+            const int s1 = later ? __ffs(later) - 1 : 32 - __clz(inside);
+            const uint32_t scene = __shfl_sync(0xffffffffu, sc, s0);
+            int last = 0;
+            if (lane == 0) {
+                const uint32_t n = (uint32_t)(s1 - s0);
+                const uint32_t ticket = atomicAdd(&A.scene_counter[2 * scene + ctr], n);
+                last = (ticket + n == (uint32_t)A.scenes[scene].num_chunks) ? 1 : 0;
+                if (last) {
+                    atomicExch(&A.scene_counter[2 * scene + ctr], 0u);
+                    __threadfence();
+                }
+            }
+            if (__shfl_sync(0xffffffffu, last, 0)) reduce_scene(A, scene, mode, lane);
+        }
     }
-    if (!A.fp64) {
-        float pf = (float)p;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) pf += __shfl_xor_sync(0xffffffffu, pf, o);
-        return (double)pf;
-    }
-    return warp_sum(p);
 }
 
-__device__ __forceinline__ float4 ldcg4(const float *p) { return __ldcg(reinterpret_cast<const float4 *>(p)); }
+// Sum over the 16 lanes of a half warp (fixed butterfly inside the half).
+__device__ __forceinline__ double half_sum(double v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float half_sum(float v) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
-    const int lane = threadIdx.x & 31;
-    const int half = lane & 1;
-    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    // ---- init: r = b, s = M^-1 b, x = 0, d = 0, delta = <r, s> ----
-    for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
-        const uint32_t scene = A.group_scene[g];
-        const Scene &sc = A.scenes[scene];
-        const uint32_t node = A.group_row[g] + (lane >> 1);
-        const bool valid = node < (uint32_t)(sc.node_base + sc.num_nodes);
-        float bv[6], rl[3] = {0.f, 0.f, 0.f}, sl[3] = {0.f, 0.f, 0.f};
+// <u, v> over 6 entries in the precision of the mode, summed over the half warp's nodes.
+__device__ __forceinline__ double node_dot_half(const PcgArgs &A, const float *u, const float *v, bool valid) {
+    if (A.fp64) {
+        double p = 0.0;
+        if (valid)
+#pragma unroll
+            for (int i = 0; i < 6; ++i) p += (double)u[i] * (double)v[i];
+        return half_sum(p);
+    }
+    float p = 0.f;
+    if (valid)
+#pragma unroll
+        for (int i = 0; i < 6; ++i) p += u[i] * v[i];
+    return (double)half_sum(p);
+}
+
+__device__ __forceinline__ void load6(const float *p, float *v) {
+    const float4 a = __ldcg(reinterpret_cast<const float4 *>(p));
+    const float2 b = __ldcg(reinterpret_cast<const float2 *>(p + 4));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
+}
+__device__ __forceinline__ void store6(float *p, const float *v) {
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<float2 *>(p + 4)[0] = make_float2(v[4], v[5]);
+}
+// y = M x for one node's 6x6 block (row-major).
+__device__ __forceinline__ void matvec6(const float *M, const float *x, float *y) {
+    float m[36];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(M) + i);
+        m[4 * i] = v.x; m[4 * i + 1] = v.y; m[4 * i + 2] = v.z; m[4 * i + 3] = v.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        float a = 0.f;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) a += m[6 * i + c] * x[c];
+        y[i] = a;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase A of a PCG iteration over one warp's rows: d = s + beta d_old, q = A d and the
+// per-row <d, q>.  The warp streams its contiguous slot range 32 slots at a time:
+//   * the packed slot records of chunk j + 2 are loaded while chunk j is computed;
+//   * the 6x6 blocks of chunk j + 1 are copied into shared memory with cp.async and its
+//     s / d_old vectors and beta are loaded into registers, also while chunk j is computed;
+//   * lane l multiplies slot l's block (transposed for a lower-triangle slot) with d of the
+//     slot's column, and the lane that ends a row sums the row's products in slot order,
+//     continuing a row that began in an earlier chunk from a carried partial sum.
+// Each row's sum therefore runs over its slots in a fixed order whatever the chunk
+// alignment, so results do not depend on which warp handled the row or on the batch.
+// ---------------------------------------------------------------------------
+constexpr int kPcgThreads = 256;                              // 8 warps per block
+constexpr int kPcgChunkFloats = 32 * 36;                      // one staged block per lane
+constexpr int kPcgRing = 64;                                  // rows kept in the per-warp rings
+constexpr int kPcgWarpFloats = 2 * kPcgChunkFloats + 32 * 8 + kPcgRing * 8 + 2 * kPcgRing;
+constexpr size_t kPcgSmemBytes = sizeof(float) * kPcgWarpFloats * (kPcgThreads / 32);
+
+// Packed slot record (col, ref, row, scene); row = kInvalidIndex past the end of the range.
+// Loaded raw and only read one chunk later, so the load never stalls the warp.
+__device__ __forceinline__ uint4 load_slot(const uint4 *info, uint32_t k, uint32_t end) {
+    uint4 v = make_uint4(0u, kInvalidIndex, kInvalidIndex, 0u);
+    if (k < end) v = __ldg(info + k);
+    return v;
+}
+
+__device__ __forceinline__ void cp_async16(float *dst, const float *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Operands of one chunk held in registers: the slot record, s and d_old of its column, beta.
+struct PcgOperands {
+    uint4 slot;
+    float4 s0, d0;
+    float2 s1, d1;
+    double beta;
+};
+
+__device__ __forceinline__ const float *slot_block(const PcgArgs &A, uint32_t col, uint32_t ref) {
+    return ref == kInvalidIndex ? A.diag_blocks + 36ull * col
+                                : A.pair_blocks + 36ull * min(ref & ~kRefTransposed, A.cap_half - 1);
+}
+
+// Starts a chunk: block copies into `stage` and register loads of s, d_old and beta.  The
+// 32 x 9 16-byte parts of the chunk's blocks are spread flat over the lanes (part 32 p + l is
+// piece (32 p + l) % 9 of block (32 p + l) / 9), so each copy instruction reads about four
+// whole blocks instead of one piece of 32 blocks.
+__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *d_old, uint4 x, float *stage, int lane,
+                                           PcgOperands &op) {
+    op.slot = x;
+    const float *src = nullptr;
+    if (x.z != kInvalidIndex) {
+        const uint32_t col = min(x.x, A.total_nodes - 1);
+        src = slot_block(A, col, x.y);
+        op.s0 = __ldcg(reinterpret_cast<const float4 *>(A.s + 8ull * col));
+        op.s1 = __ldcg(reinterpret_cast<const float2 *>(A.s + 8ull * col + 4));
+        op.d0 = __ldcg(reinterpret_cast<const float4 *>(d_old + 8ull * col));
+        op.d1 = __ldcg(reinterpret_cast<const float2 *>(d_old + 8ull * col + 4));
+        op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
+    }
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const int part = 32 * p + lane, e = part / 9, piece = part - 9 * e;
+        const float *b = reinterpret_cast<const float *>(
+            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), e));
+        if (b) cp_async16(stage + 36 * e + 4 * piece, b + 4 * piece);
+    }
+    cp_async_commit();
+}
+
+__device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *d_old,
+                            float *d_new, float *wsm, int lane) {
+    if (g0 >= g1) return;
+    float *stage[2] = {wsm, wsm + kPcgChunkFloats};
+    float *prod = wsm + 2 * kPcgChunkFloats;                  // [32][8] per-slot products
+    float *dring = prod + 32 * 8;                             // [kPcgRing][8] d of the row, by row
+    double *gring = reinterpret_cast<double *>(dring + kPcgRing * 8);   // [kPcgRing] <d, q> by row
+    const uint32_t e0 = A.rowptr[r0], e1 = min(A.rowptr[r1], A.cap_blocks);
+    const uint32_t nchunks = e1 > e0 ? (e1 - e0 + 31) / 32 : 0;
+    uint4 nxt = load_slot(A.entry_info, e0 + 32 + lane, e1);
+    PcgOperands cur;
+    issue_chunk(A, d_old, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
+    float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    uint32_t carry_row = kInvalidIndex;
+    uint32_t group = g0, group_end = (g0 + 1 < A.total_groups) ? A.group_row[g0 + 1] : A.total_nodes;
+    for (uint32_t j = 0; j < nchunks; ++j) {
+        // chunk j + 1 in flight, chunk j + 2 records requested
+        PcgOperands next;
+        issue_chunk(A, d_old, nxt, stage[(j + 1) & 1], lane, next);
+        const uint4 after = load_slot(A.entry_info, e0 + 32 * (j + 2) + lane, e1);
+        cp_async_wait_prior();
+        __syncwarp();
+        const bool valid = cur.slot.z != kInvalidIndex;
+        const uint32_t xrow = valid ? min(cur.slot.z, A.total_nodes - 1) : kInvalidIndex;
+        const uint32_t xref = cur.slot.y;
+        float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
-            const float4 b0 = *reinterpret_cast<const float4 *>(A.jtr + 8ull * node);
-            const float4 b1 = *reinterpret_cast<const float4 *>(A.jtr + 8ull * node + 4);
-            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w; bv[4] = b1.x; bv[5] = b1.y;
-            const float *M = A.inv_diag + 36ull * node + 18 * half;
+            const float beta = (float)cur.beta;
+            const float dv[6] = {cur.s0.x + beta * cur.d0.x, cur.s0.y + beta * cur.d0.y,
+                                 cur.s0.z + beta * cur.d0.z, cur.s0.w + beta * cur.d0.w,
+                                 cur.s1.x + beta * cur.d1.x, cur.s1.y + beta * cur.d1.y};
+            float m[36];
+            const float4 *blk = reinterpret_cast<const float4 *>(stage[j & 1] + 36 * lane);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                float acc = 0.f;
+            for (int i = 0; i < 9; ++i) {
+                const float4 v = blk[i];
+                m[4 * i] = v.x;
+                m[4 * i + 1] = v.y;
+                m[4 * i + 2] = v.z;
+                m[4 * i + 3] = v.w;
+            }
+            const bool tr = xref != kInvalidIndex && (xref & kRefTransposed) != 0;
 #pragma unroll
-                for (int c = 0; c < 6; ++c) acc += M[6 * i + c] * bv[c];
-                sl[i] = acc;
-                rl[i] = half ? bv[3 + i] : bv[i];
-                A.r[8ull * node + 3 * half + i] = rl[i];
-                A.s[8ull * node + 3 * half + i] = sl[i];
-                A.x[8ull * node + 3 * half + i] = 0.f;
-                A.d0[8ull * node + 3 * half + i] = 0.f;
-                A.d1[8ull * node + 3 * half + i] = 0.f;
+            for (int i = 0; i < 6; ++i) {
+                float a = 0.f, t = 0.f;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    a += m[6 * i + c] * dv[c];
+                    t += m[6 * c + i] * dv[c];
+                }
+                p[i] = tr ? t : a;
+            }
+            float4 *pp = reinterpret_cast<float4 *>(prod + 8 * lane);
+            pp[0] = make_float4(p[0], p[1], p[2], p[3]);
+            pp[1] = make_float4(p[4], p[5], 0.f, 0.f);
+            if (xref == kInvalidIndex) {   // diagonal slot: d of the row itself
+                float4 *dd = reinterpret_cast<float4 *>(dring + 8 * (xrow & (kPcgRing - 1)));
+                dd[0] = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                dd[1] = make_float4(dv[4], dv[5], 0.f, 0.f);
             }
         }
-        publish_group(A, g, scene, lane_dot3(A, rl, sl, valid), 2, lane);
+        __syncwarp();
+        // row segments of this chunk
+        const uint32_t next_first = __shfl_sync(0xffffffffu, next.slot.z, 0);
+        const uint32_t row_up = __shfl_up_sync(0xffffffffu, xrow, 1);
+        const uint32_t row_dn = __shfl_down_sync(0xffffffffu, xrow, 1);
+        const uint32_t following = (lane == 31) ? next_first : row_dn;
+        const bool starts = valid && (lane == 0 || row_up != xrow);
+        const unsigned start_mask = __ballot_sync(0xffffffffu, starts);
+        const unsigned valid_mask = __ballot_sync(0xffffffffu, valid);
+        const int last = 31 - __clz(valid_mask);
+        const bool ends_row = valid && following != xrow;
+        const bool owner = valid && (ends_row || lane == last);
+        float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (owner) {
+            const int first = 31 - __clz(start_mask & (0xffffffffu >> (31 - lane)));
+            if (first == 0 && xrow == carry_row) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) sum[i] = carry[i];
+            }
+            for (int l = first; l <= lane; ++l) {
+                const float4 a = reinterpret_cast<const float4 *>(prod + 8 * l)[0];
+                const float2 b = reinterpret_cast<const float2 *>(prod + 8 * l + 4)[0];
+                sum[0] += a.x;
+                sum[1] += a.y;
+                sum[2] += a.z;
+                sum[3] += a.w;
+                sum[4] += b.x;
+                sum[5] += b.y;
+            }
+            if (ends_row) {
+                const float *dn = dring + 8 * (xrow & (kPcgRing - 1));
+                double dot = 0.0;
+                float dotf = 0.f;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    dot += (double)dn[i] * (double)sum[i];
+                    dotf += dn[i] * sum[i];
+                }
+                float4 *qo = reinterpret_cast<float4 *>(A.q + 8ull * xrow);
+                float4 *dno = reinterpret_cast<float4 *>(d_new + 8ull * xrow);
+                qo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
+                qo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
+                dno[0] = make_float4(dn[0], dn[1], dn[2], dn[3]);
+                dno[1] = make_float4(dn[4], dn[5], 0.f, 0.f);
+                gring[xrow & (kPcgRing - 1)] = A.fp64 ? dot : (double)dotf;
+            }
+        }
+        // partial sum of a row that continues into the next chunk
+        const bool cont = __shfl_sync(0xffffffffu, owner && !ends_row ? 1 : 0, last) != 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) carry[i] = __shfl_sync(0xffffffffu, sum[i], last);
+        const uint32_t last_row = __shfl_sync(0xffffffffu, xrow, last);
+        carry_row = cont ? last_row : kInvalidIndex;
+        __syncwarp();
+        // groups whose rows are all done: their <d, q> partial, summed in row order
+        const uint32_t done_below = cont ? last_row : last_row + 1;
+        while (group < g1 && group_end <= done_below) {
+            const uint32_t grow = A.group_row[group];
+            double v = 0.0;
+            if (grow + lane < group_end) v = gring[(grow + lane) & (kPcgRing - 1)];
+            double part;
+            if (A.fp64) {
+                part = warp_sum(v);
+            } else {
+                float f = (float)v;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) f += __shfl_xor_sync(0xffffffffu, f, o);
+                part = (double)f;
+            }
+            if (lane == 0) A.group_partial[group] = part;
+            ++group;
+            group_end = (group + 1 < A.total_groups) ? A.group_row[group + 1] : A.total_nodes;
+        }
+        cur = next;
+        nxt = after;
     }
+    // drain the last (empty) copy group before the stage buffers are reused
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncwarp();
+}
+
+// One step of the per-node phases: lanes 0-15 take the rows of group g, lanes 16-31 those
+// of group g + 1 (fewer in a scene's last group).
+struct NodeStep {
+    uint32_t gg, node, scene;
+    bool group_ok, valid;
+};
+__device__ __forceinline__ NodeStep node_step(const PcgArgs &A, uint32_t g, uint32_t g_end, int lane) {
+    NodeStep n;
+    n.gg = g + (uint32_t)(lane >> 4);
+    n.group_ok = n.gg < g_end;
+    const uint32_t first = n.group_ok ? A.group_row[n.gg] : 0u;
+    const uint32_t stop = !n.group_ok ? 0u : (n.gg + 1 < A.total_groups ? A.group_row[n.gg + 1] : A.total_nodes);
+    n.scene = n.group_ok ? min(A.group_scene[n.gg], A.num_scenes - 1) : 0u;
+    n.node = first + (uint32_t)(lane & 15);
+    n.valid = n.group_ok && n.node < stop;
+    return n;
+}
+
+__global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
+    extern __shared__ __align__(16) float pcg_smem[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
+    // this warp's contiguous range of row groups (balanced by slot count) and their rows
+    const uint32_t g_begin = min(A.warp_groups[gwarp], A.total_groups);
+    const uint32_t g_end = max(g_begin, min(A.warp_groups[gwarp + 1], A.total_groups));
+    const uint32_t r_begin = g_begin < A.total_groups ? A.group_row[g_begin] : A.total_nodes;
+    const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
+
+    // ---- init: r = b, s = M^-1 b, x = 0, d = 0, delta = <r, s> ----
+    for (uint32_t g = g_begin; g < g_end; g += 2) {
+        const NodeStep n = node_step(A, g, g_end, lane);
+        float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (n.valid) {
+            const float zero[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            load6(A.jtr + 8ull * n.node, rv);
+            matvec6(A.inv_diag + 36ull * n.node, rv, sv);
+            store6(A.r + 8ull * n.node, rv);
+            store6(A.s + 8ull * n.node, sv);
+            store6(A.x + 8ull * n.node, zero);
+            store6(A.d0 + 8ull * n.node, zero);
+            store6(A.d1 + 8ull * n.node, zero);
+        }
+        const double part = node_dot_half(A, rv, sv, n.valid);
+        if ((lane & 15) == 0 && n.group_ok) A.group_partial[n.gg] = part;
+    }
+    publish_range(A, g_begin, g_end, 2, lane);
     if (!grid_barrier(A.barrier, A.err)) return;
 
     for (int it = 0; it < A.pcg_iters; ++it) {
         const float *d_old = (it & 1) ? A.d1 : A.d0;
         float *d_new = (it & 1) ? A.d0 : A.d1;
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
-        for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
-            const uint32_t scene = A.group_scene[g];
-            const Scene &sc = A.scenes[scene];
-            const uint32_t node = A.group_row[g] + (lane >> 1);
-            const bool valid = node < (uint32_t)(sc.node_base + sc.num_nodes);
-            const float beta = (float)ldcg(A.scalars + 8ull * scene + 2);
-            float acc[3] = {0.f, 0.f, 0.f}, dn[3] = {0.f, 0.f, 0.f};
-            if (valid) {
-                // bounds hold by construction; the clamps keep a capacity overflow (already
-                // flagged as WS_ERR_CAPACITY) from reading outside the buffers
-                const uint32_t b1 = min(A.rowptr[node + 1], A.cap_blocks);
-                const uint32_t b0 = min(A.rowptr[node], b1);
-#pragma unroll 2
-                for (uint32_t k = b0; k < b1; ++k) {
-                    const uint32_t col = min(A.colidx[k], A.total_nodes - 1);
-                    const float2 *blk = reinterpret_cast<const float2 *>(A.blocks + 36ull * k + 18 * half);
-                    float m[18];
-#pragma unroll
-                    for (int i = 0; i < 9; ++i) {
-                        const float2 v = __ldg(blk + i);
-                        m[2 * i] = v.x;
-                        m[2 * i + 1] = v.y;
-                    }
-                    const float4 s0 = ldcg4(A.s + 8ull * col), s1 = ldcg4(A.s + 8ull * col + 4);
-                    const float4 e0 = ldcg4(d_old + 8ull * col), e1 = ldcg4(d_old + 8ull * col + 4);
-                    const float dv[6] = {s0.x + beta * e0.x, s0.y + beta * e0.y, s0.z + beta * e0.z,
-                                         s0.w + beta * e0.w, s1.x + beta * e1.x, s1.y + beta * e1.y};
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) acc[i] += m[6 * i + c] * dv[c];
-                }
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const size_t e = 8ull * node + 3 * half + i;
-                    dn[i] = ldcg(A.s + e) + beta * ldcg(d_old + e);
-                    d_new[e] = dn[i];
-                    A.q[e] = acc[i];
-                }
-            }
-            publish_group(A, g, scene, lane_dot3(A, dn, acc, valid), 0, lane);
-        }
+        pcg_phase_a(A, g_begin, g_end, r_begin, r_end, d_old, d_new, wsm, lane);
+        publish_range(A, g_begin, g_end, 0, lane);
         if (!grid_barrier(A.barrier, A.err)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
-        for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
-            const uint32_t scene = A.group_scene[g];
-            const Scene &sc = A.scenes[scene];
-            const uint32_t node = A.group_row[g] + (lane >> 1);
-            const bool valid = node < (uint32_t)(sc.node_base + sc.num_nodes);
-            const float alpha = (float)ldcg(A.scalars + 8ull * scene + 1);
-            float rn[3] = {0.f, 0.f, 0.f}, sv[3] = {0.f, 0.f, 0.f};
-            if (valid) {
+        for (uint32_t g = g_begin; g < g_end; g += 2) {
+            const NodeStep n = node_step(A, g, g_end, lane);
+            float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (n.valid) {
+                const float alpha = (float)__ldcg(A.scalars + 8ull * n.scene + 1);
+                float xv[6], dv[6], qv[6];
+                load6(A.x + 8ull * n.node, xv);
+                load6(d_new + 8ull * n.node, dv);
+                load6(A.r + 8ull * n.node, rv);
+                load6(A.q + 8ull * n.node, qv);
 #pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const size_t e = 8ull * node + 3 * half + i;
-                    A.x[e] += alpha * ldcg(d_new + e);
-                    rn[i] = A.r[e] - alpha * ldcg(A.q + e);
-                    A.r[e] = rn[i];
+                for (int i = 0; i < 6; ++i) {
+                    xv[i] += alpha * dv[i];
+                    rv[i] -= alpha * qv[i];
                 }
+                matvec6(A.inv_diag + 36ull * n.node, rv, sv);
+                store6(A.x + 8ull * n.node, xv);
+                store6(A.r + 8ull * n.node, rv);
+                store6(A.s + 8ull * n.node, sv);
             }
-            // the partner lane holds the other three entries of the node's r
-            float rv[6];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const float other = __shfl_xor_sync(0xffffffffu, rn[i], 1);
-                rv[i] = half ? other : rn[i];
-                rv[3 + i] = half ? rn[i] : other;
-            }
-            if (valid) {
-                const float *M = A.inv_diag + 36ull * node + 18 * half;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    float acc = 0.f;
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) acc += M[6 * i + c] * rv[c];
-                    sv[i] = acc;
-                    A.s[8ull * node + 3 * half + i] = acc;
-                }
-            }
-            publish_group(A, g, scene, lane_dot3(A, rn, sv, valid), 1, lane);
+            const double part = node_dot_half(A, rv, sv, n.valid);
+            if ((lane & 15) == 0 && n.group_ok) A.group_partial[n.gg] = part;
         }
+        publish_range(A, g_begin, g_end, 1, lane);
         if (!grid_barrier(A.barrier, A.err)) return;
     }
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
     //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
-    for (uint32_t g = gwarp; g < A.total_groups; g += nwarps) {
-        const uint32_t scene = A.group_scene[g];
-        const Scene &sc = A.scenes[scene];
-        const uint32_t row = A.group_row[g] + lane;
-        if (lane >= kRowsPerGroup || row >= (uint32_t)(sc.node_base + sc.num_nodes)) continue;
+    for (uint32_t row = r_begin + lane; row < r_end; row += 32) {
         float xv[6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) xv[c] = ldcg(A.x + 8ull * row + c);
@@ -1020,9 +1239,17 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
     }
 }
 
+// One warp per row group when that fits, else every co-resident block.
+int pcg_launch_blocks(const Workspace &w) {
+    const uint32_t want = (w.total_chunks + (kPcgThreads / 32) - 1) / (kPcgThreads / 32);
+    return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, (uint32_t)w.pcg_grid));
+}
+int pcg_warps_per_block() { return kPcgThreads / 32; }
+
 int pcg_max_blocks(int device) {
     int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, 0);
+    cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, kPcgSmemBytes);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per_sm) * std::max(1, sms);
 }
@@ -1055,26 +1282,24 @@ void gn_eval(Workspace &w, cudaStream_t st) {
 void gn_assemble_node(Workspace &w, cudaStream_t st) {
     const int ng = grid_for(w.total_nodes * 32u, kAssembleThreads, w.num_sms, 32);
     if (w.precision == WS_PREC_FP32)
-        k_assemble_node<float><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
-                                                    w.n2t_sorted_val, w.d_record, w.r_record, w.se3, w.centers,
-                                                    w.rowptr, w.cap_blocks, w.blocks, w.diag64, w.jtr,
-                                                    w.error_flag);
+        k_assemble_node<float><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes,
+                                                                 w.n2t_offset, w.n2t_sorted_val, w.d_record,
+                                                                 w.r_record, w.se3, w.centers, w.diag_blocks,
+                                                                 w.diag64, w.jtr, w.error_flag);
     else
-        k_assemble_node<double><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset,
-                                                     w.n2t_sorted_val, w.d_record, w.r_record, w.se3, w.centers,
-                                                     w.rowptr, w.cap_blocks, w.blocks, w.diag64, w.jtr,
-                                                     w.error_flag);
+        k_assemble_node<double><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes,
+                                                                  w.n2t_offset, w.n2t_sorted_val, w.d_record,
+                                                                  w.r_record, w.se3, w.centers, w.diag_blocks,
+                                                                  w.diag64, w.jtr, w.error_flag);
     count_launch(w);
     k_block_inverse<<<grid_for(w.total_nodes, 128, w.num_sms, 16), 128, 0, st>>>(
-        w.diag64, w.blocks, w.rowptr, w.total_nodes, w.cap_blocks, w.precision == WS_PREC_MIXED ? 1 : 0, w.inv_diag);
+        w.diag64, w.diag_blocks, w.total_nodes, w.precision == WS_PREC_MIXED ? 1 : 0, w.inv_diag);
     count_launch(w);
 }
-
 void gn_assemble_pair(Workspace &w, cudaStream_t st) {
     k_assemble_pair<<<grid_for(w.cap_half * 32u, kAssembleThreads, w.num_sms, 32), kAssembleThreads, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
-        w.half_slot_up, w.half_slot_lo, w.d_record, w.r_record, w.centers,
-        w.precision == WS_PREC_MIXED ? 1 : 0, w.blocks);
+        w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.pair_blocks);
     count_launch(w);
 }
 
@@ -1086,7 +1311,11 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     a.total_groups = w.total_chunks;
     a.rowptr = w.rowptr;
     a.colidx = w.colidx;
-    a.blocks = w.blocks;
+    a.entry_ref = w.entry_ref;
+    a.entry_info = w.entry_info;
+    a.warp_groups = w.pcg_warp_groups;
+    a.diag_blocks = w.diag_blocks;
+    a.pair_blocks = w.pair_blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
     a.x = w.x; a.r = w.r; a.s = w.s; a.q = w.q; a.d0 = w.d0; a.d1 = w.d1;
@@ -1095,21 +1324,21 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     a.scene_counter = w.scene_counter;
     a.barrier = w.barrier;
     a.cap_blocks = w.cap_blocks;
+    a.cap_half = std::max<uint32_t>(1u, w.cap_half);
+    a.num_scenes = (uint32_t)std::max(1, w.num_scenes);
     a.total_nodes = w.total_nodes;
     a.err = w.error_flag;
     a.se3 = w.se3;
     a.centers = w.centers;
     a.pcg_iters = pcg_iters;
     a.fp64 = (w.precision == WS_PREC_MIXED) ? 1 : 0;
-    // one warp per row group when that fits, else every co-resident block
-    const uint32_t want = (w.total_chunks + (kPcgThreads / 32) - 1) / (kPcgThreads / 32);
-    const int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, (uint32_t)w.pcg_grid));
+    const int grid = pcg_launch_blocks(w);
     // a barrier or counter left half-way by an earlier timed-out launch must not leak into this one
     cudaMemsetAsync(w.barrier, 0, 4 * sizeof(uint32_t), st);
     cudaMemsetAsync(w.scene_counter, 0, 2 * sizeof(uint32_t) * (size_t)w.num_scenes, st);
     void *args[] = {&a};
     count_launch(w);
-    return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, 0, st);
+    return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);
 }
 
 cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {

@@ -76,7 +76,14 @@ struct Workspace {
     uint32_t *rowptr = nullptr;                              // [cap_nodes + 1]
     uint32_t *col_key = nullptr, *col_val = nullptr, *col_key_alt = nullptr, *col_val_alt = nullptr; // [cap_half]
     uint32_t *colidx = nullptr;                              // [cap_blocks]
-    float *blocks = nullptr;                                 // [cap_blocks * 36]
+    // Symmetric block storage: one 6x6 block per node (diagonal) and one per unordered pair
+    // (row < col orientation); entry_ref maps an off-diagonal CSR slot to its pair block,
+    // with kRefTransposed set for the lower-triangle entry.
+    uint32_t *entry_ref = nullptr;                           // [cap_blocks]
+    uint4 *entry_info = nullptr;                             // [cap_blocks] (col, ref, row, scene) for the PCG
+    uint32_t *pcg_warp_groups = nullptr;                     // [pcg_grid * warps per block + 1]
+    float *diag_blocks = nullptr;                            // [cap_nodes * 36]
+    float *pair_blocks = nullptr;                            // [cap_half * 36]
 
     // per-node system and PCG state (stride kVecStride)
     float *inv_diag = nullptr;          // [cap_nodes * 36]
@@ -128,6 +135,8 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st);
 void init_warp(Workspace &w, cudaStream_t st);
 // Occupancy of the persistent PCG kernel.
 int pcg_max_blocks(int device);
+int pcg_launch_blocks(const Workspace &w);
+int pcg_warps_per_block();
 
 // Launch accounting for the measurement hooks.
 inline void count_launch(Workspace &w, int n = 1) { w.launches += n; }
