@@ -35,8 +35,8 @@ void free_all(ws::Workspace &w) {
                     w.n2t_val_alt, w.n2t_offset, w.pair_key, w.pair_key_alt, w.pair_val, w.pair_val_alt,
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
-                    w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.s, w.q,
-                    w.d0, w.d1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
+                    w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
+                    w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
                     w.error_flag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -190,7 +190,8 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.pair_blocks, (size_t)std::max<uint32_t>(1u, w.cap_half) * 36));
     A(dalloc(&w.inv_diag, (size_t)w.cap_nodes * 36));
     A(dalloc(&w.diag64, (size_t)w.cap_nodes * 21));
-    for (float **v : {&w.jtr, &w.x, &w.r, &w.s, &w.q, &w.d0, &w.d1}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
+    for (float **v : {&w.jtr, &w.x, &w.r, &w.q}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
+    for (float **v : {&w.sd0, &w.sd1}) A(dalloc(v, (size_t)w.cap_nodes * 2 * ws::kVecStride));
     A(dalloc(&w.se3, (size_t)w.cap_nodes * 8));
     A(dalloc(&w.centers, w.cap_nodes));
     A(dalloc(&w.chunk_partial, w.cap_chunks));

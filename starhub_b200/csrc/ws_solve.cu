@@ -726,7 +726,8 @@ struct PcgArgs {
     const uint4 *entry_info;
     const uint32_t *warp_groups;   // [warps + 1] first row group of each warp
     const float *diag_blocks, *pair_blocks, *inv_diag, *jtr;
-    float *x, *r, *s, *q, *d0, *d1;
+    float *x, *r, *q;
+    float *sd0, *sd1;         // [node][16]: s (6, padded to 8) then d (6, padded); swapped every iteration
     double *group_partial;
     double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
     uint32_t *scene_counter;  // per scene: [0] phase A, [1] phase B / init
@@ -906,10 +907,11 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 // Each row's sum therefore runs over its slots in a fixed order whatever the chunk
 // alignment, so results do not depend on which warp handled the row or on the batch.
 // ---------------------------------------------------------------------------
-constexpr int kPcgThreads = 256;                              // 8 warps per block
-constexpr int kPcgChunkFloats = 32 * 36;                      // one staged block per lane
+constexpr int kPcgThreads = 128;                              // 4 warps per block
+constexpr int kPcgSlot = 52;                                  // block (36) + s/d record (16) per slot
+constexpr int kPcgChunkFloats = 32 * kPcgSlot;
 constexpr int kPcgRing = 64;                                  // rows kept in the per-warp rings
-constexpr int kPcgWarpFloats = 2 * kPcgChunkFloats + 32 * 8 + kPcgRing * 8 + 2 * kPcgRing;
+constexpr int kPcgWarpFloats = 2 * kPcgChunkFloats + kPcgRing * 8 + 2 * kPcgRing;
 constexpr size_t kPcgSmemBytes = sizeof(float) * kPcgWarpFloats * (kPcgThreads / 32);
 
 // Packed slot record (col, ref, row, scene); row = kInvalidIndex past the end of the range.
@@ -930,8 +932,6 @@ __device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.w
 // Operands of one chunk held in registers: the slot record, s and d_old of its column, beta.
 struct PcgOperands {
     uint4 slot;
-    float4 s0, d0;
-    float2 s1, d1;
     double beta;
 };
 
@@ -940,52 +940,55 @@ __device__ __forceinline__ const float *slot_block(const PcgArgs &A, uint32_t co
                                 : A.pair_blocks + 36ull * min(ref & ~kRefTransposed, A.cap_half - 1);
 }
 
-// Starts a chunk: block copies into `stage` and register loads of s, d_old and beta.  The
-// 32 x 9 16-byte parts of the chunk's blocks are spread flat over the lanes (part 32 p + l is
-// piece (32 p + l) % 9 of block (32 p + l) / 9), so each copy instruction reads about four
-// whole blocks instead of one piece of 32 blocks.
-__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *d_old, uint4 x, float *stage, int lane,
+// Starts a chunk: copies of each slot's block and of its column's s/d record into `stage`,
+// and a register load of beta.  The chunk's 16-byte parts (9 per block, 4 per record) are
+// spread flat over the lanes, so each copy instruction reads a few whole blocks or records
+// instead of one piece of 32 of them.
+__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *sd_old, uint4 x, float *stage, int lane,
                                            PcgOperands &op) {
     op.slot = x;
-    const float *src = nullptr;
+    const float *blk = nullptr, *vec = nullptr;
     if (x.z != kInvalidIndex) {
         const uint32_t col = min(x.x, A.total_nodes - 1);
-        src = slot_block(A, col, x.y);
-        op.s0 = __ldcg(reinterpret_cast<const float4 *>(A.s + 8ull * col));
-        op.s1 = __ldcg(reinterpret_cast<const float2 *>(A.s + 8ull * col + 4));
-        op.d0 = __ldcg(reinterpret_cast<const float4 *>(d_old + 8ull * col));
-        op.d1 = __ldcg(reinterpret_cast<const float2 *>(d_old + 8ull * col + 4));
+        blk = slot_block(A, col, x.y);
+        vec = sd_old + 16ull * col;
         op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
     }
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
         const int part = 32 * p + lane, e = part / 9, piece = part - 9 * e;
         const float *b = reinterpret_cast<const float *>(
-            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), e));
-        if (b) cp_async16(stage + 36 * e + 4 * piece, b + 4 * piece);
+            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(blk), e));
+        if (b) cp_async16(stage + kPcgSlot * e + 4 * piece, b + 4 * piece);
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int part = 32 * p + lane, e = part >> 2, piece = part & 3;
+        const float *v = reinterpret_cast<const float *>(
+            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vec), e));
+        if (v) cp_async16(stage + kPcgSlot * e + 36 + 4 * piece, v + 4 * piece);
     }
     cp_async_commit();
 }
 
-__device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *d_old,
-                            float *d_new, float *wsm, int lane) {
+__device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *sd_old,
+                            float *sd_new, float *wsm, int lane) {
     if (g0 >= g1) return;
     float *stage[2] = {wsm, wsm + kPcgChunkFloats};
-    float *prod = wsm + 2 * kPcgChunkFloats;                  // [32][8] per-slot products
-    float *dring = prod + 32 * 8;                             // [kPcgRing][8] d of the row, by row
+    float *dring = wsm + 2 * kPcgChunkFloats;                 // [kPcgRing][8] d of the row, by row
     double *gring = reinterpret_cast<double *>(dring + kPcgRing * 8);   // [kPcgRing] <d, q> by row
     const uint32_t e0 = A.rowptr[r0], e1 = min(A.rowptr[r1], A.cap_blocks);
     const uint32_t nchunks = e1 > e0 ? (e1 - e0 + 31) / 32 : 0;
     uint4 nxt = load_slot(A.entry_info, e0 + 32 + lane, e1);
     PcgOperands cur;
-    issue_chunk(A, d_old, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
+    issue_chunk(A, sd_old, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
     uint32_t group = g0, group_end = (g0 + 1 < A.total_groups) ? A.group_row[g0 + 1] : A.total_nodes;
     for (uint32_t j = 0; j < nchunks; ++j) {
         // chunk j + 1 in flight, chunk j + 2 records requested
         PcgOperands next;
-        issue_chunk(A, d_old, nxt, stage[(j + 1) & 1], lane, next);
+        issue_chunk(A, sd_old, nxt, stage[(j + 1) & 1], lane, next);
         const uint4 after = load_slot(A.entry_info, e0 + 32 * (j + 2) + lane, e1);
         cp_async_wait_prior();
         __syncwarp();
@@ -993,13 +996,17 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
         const uint32_t xrow = valid ? min(cur.slot.z, A.total_nodes - 1) : kInvalidIndex;
         const uint32_t xref = cur.slot.y;
         float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float *mine = stage[j & 1] + kPcgSlot * lane;
         if (valid) {
             const float beta = (float)cur.beta;
-            const float dv[6] = {cur.s0.x + beta * cur.d0.x, cur.s0.y + beta * cur.d0.y,
-                                 cur.s0.z + beta * cur.d0.z, cur.s0.w + beta * cur.d0.w,
-                                 cur.s1.x + beta * cur.d1.x, cur.s1.y + beta * cur.d1.y};
+            const float4 s0 = reinterpret_cast<const float4 *>(mine + 36)[0];
+            const float2 s1 = reinterpret_cast<const float2 *>(mine + 40)[0];
+            const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
+            const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
+            const float dv[6] = {s0.x + beta * d0.x, s0.y + beta * d0.y, s0.z + beta * d0.z,
+                                 s0.w + beta * d0.w, s1.x + beta * d1.x, s1.y + beta * d1.y};
             float m[36];
-            const float4 *blk = reinterpret_cast<const float4 *>(stage[j & 1] + 36 * lane);
+            const float4 *blk = reinterpret_cast<const float4 *>(mine);
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 const float4 v = blk[i];
@@ -1019,7 +1026,7 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
                 }
                 p[i] = tr ? t : a;
             }
-            float4 *pp = reinterpret_cast<float4 *>(prod + 8 * lane);
+            float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
             pp[0] = make_float4(p[0], p[1], p[2], p[3]);
             pp[1] = make_float4(p[4], p[5], 0.f, 0.f);
             if (xref == kInvalidIndex) {   // diagonal slot: d of the row itself
@@ -1047,9 +1054,10 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
 #pragma unroll
                 for (int i = 0; i < 6; ++i) sum[i] = carry[i];
             }
+            const float *chunk = stage[j & 1];
             for (int l = first; l <= lane; ++l) {
-                const float4 a = reinterpret_cast<const float4 *>(prod + 8 * l)[0];
-                const float2 b = reinterpret_cast<const float2 *>(prod + 8 * l + 4)[0];
+                const float4 a = reinterpret_cast<const float4 *>(chunk + kPcgSlot * l)[0];
+                const float2 b = reinterpret_cast<const float2 *>(chunk + kPcgSlot * l + 4)[0];
                 sum[0] += a.x;
                 sum[1] += a.y;
                 sum[2] += a.z;
@@ -1067,7 +1075,7 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
                     dotf += dn[i] * sum[i];
                 }
                 float4 *qo = reinterpret_cast<float4 *>(A.q + 8ull * xrow);
-                float4 *dno = reinterpret_cast<float4 *>(d_new + 8ull * xrow);
+                float4 *dno = reinterpret_cast<float4 *>(sd_new + 16ull * xrow + 8);
                 qo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
                 qo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
                 dno[0] = make_float4(dn[0], dn[1], dn[2], dn[3]);
@@ -1127,7 +1135,7 @@ __device__ __forceinline__ NodeStep node_step(const PcgArgs &A, uint32_t g, uint
     return n;
 }
 
-__global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
+__global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     extern __shared__ __align__(16) float pcg_smem[];
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1148,10 +1156,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
             load6(A.jtr + 8ull * n.node, rv);
             matvec6(A.inv_diag + 36ull * n.node, rv, sv);
             store6(A.r + 8ull * n.node, rv);
-            store6(A.s + 8ull * n.node, sv);
+            store6(A.sd0 + 16ull * n.node, sv);
+            store6(A.sd0 + 16ull * n.node + 8, zero);
             store6(A.x + 8ull * n.node, zero);
-            store6(A.d0 + 8ull * n.node, zero);
-            store6(A.d1 + 8ull * n.node, zero);
         }
         const double part = node_dot_half(A, rv, sv, n.valid);
         if ((lane & 15) == 0 && n.group_ok) A.group_partial[n.gg] = part;
@@ -1160,10 +1167,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
     if (!grid_barrier(A.barrier, A.err)) return;
 
     for (int it = 0; it < A.pcg_iters; ++it) {
-        const float *d_old = (it & 1) ? A.d1 : A.d0;
-        float *d_new = (it & 1) ? A.d0 : A.d1;
+        const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
+        float *sd_new = (it & 1) ? A.sd0 : A.sd1;
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
-        pcg_phase_a(A, g_begin, g_end, r_begin, r_end, d_old, d_new, wsm, lane);
+        pcg_phase_a(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
         publish_range(A, g_begin, g_end, 0, lane);
         if (!grid_barrier(A.barrier, A.err)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
@@ -1174,7 +1181,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
                 const float alpha = (float)__ldcg(A.scalars + 8ull * n.scene + 1);
                 float xv[6], dv[6], qv[6];
                 load6(A.x + 8ull * n.node, xv);
-                load6(d_new + 8ull * n.node, dv);
+                load6(sd_new + 16ull * n.node + 8, dv);
                 load6(A.r + 8ull * n.node, rv);
                 load6(A.q + 8ull * n.node, qv);
 #pragma unroll
@@ -1185,7 +1192,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
                 matvec6(A.inv_diag + 36ull * n.node, rv, sv);
                 store6(A.x + 8ull * n.node, xv);
                 store6(A.r + 8ull * n.node, rv);
-                store6(A.s + 8ull * n.node, sv);
+                store6(sd_new + 16ull * n.node, sv);
             }
             const double part = node_dot_half(A, rv, sv, n.valid);
             if ((lane & 15) == 0 && n.group_ok) A.group_partial[n.gg] = part;
@@ -1318,7 +1325,7 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     a.pair_blocks = w.pair_blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
-    a.x = w.x; a.r = w.r; a.s = w.s; a.q = w.q; a.d0 = w.d0; a.d1 = w.d1;
+    a.x = w.x; a.r = w.r; a.q = w.q; a.sd0 = w.sd0; a.sd1 = w.sd1;
     a.group_partial = w.chunk_partial;
     a.scalars = w.scene_scalars;
     a.scene_counter = w.scene_counter;

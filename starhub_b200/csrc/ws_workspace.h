@@ -88,8 +88,10 @@ struct Workspace {
     // per-node system and PCG state (stride kVecStride)
     float *inv_diag = nullptr;          // [cap_nodes * 36]
     double *diag64 = nullptr;           // [cap_nodes * 21] FP64 diagonal blocks (upper triangle)
-    float *jtr = nullptr, *x = nullptr, *r = nullptr, *s = nullptr, *q = nullptr;
-    float *d0 = nullptr, *d1 = nullptr;
+    float *jtr = nullptr, *x = nullptr, *r = nullptr, *q = nullptr;
+    // PCG search vectors: per node s (6, padded to 8) then d (6, padded to 8), two copies
+    // that swap roles every iteration (the SpMV reads one while the other is written)
+    float *sd0 = nullptr, *sd1 = nullptr;
     float *se3 = nullptr;               // [cap_nodes * 8] current warp
     float4 *centers = nullptr;          // [cap_nodes] twist centre per node (current GN iteration)
     double *chunk_partial = nullptr;    // [cap_chunks]
