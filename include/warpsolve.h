@@ -203,6 +203,92 @@ int ws_splat_maps_noalloc(const float *verts, const float *attr_verts, const flo
                           int footprint, uint32_t *index_map, float *vertex_map, float *normal_map,
                           void *stream);
 
+/* ---- Serving: a persistent request loop with continuous batching -----------------------
+ * No reference counterpart: the reference solves one frame of one stream per call
+ * (OptimizationProcessorWarpSolver::ProcessFrame).  A server keeps the node graph, surfel
+ * skinning and warp of every registered stream resident on its device, takes one frame
+ * per request, and solves the requests that are waiting as batches on `executors` streams,
+ * so that batches overlap on the device.  A new batch starts as soon as an executor is free,
+ * from the oldest waiting frames that fit its capacities, at most one frame per stream
+ * (a stream's frames are solved in submission order, each starting from the warp its
+ * previous frame produced).  A request's result is bit-identical whatever it was batched with.
+ * Memory admission: executors are sized at creation and scenes are admitted by the bytes they
+ * keep resident; the sum never exceeds memory_budget. */
+typedef struct ws_server ws_server;
+
+typedef struct ws_server_config {
+    int device;
+    unsigned long long memory_budget; /* bytes of device memory for executors + resident scenes */
+    int executors;              /* batches in flight at once (one stream and solver each) */
+    int max_batch_scenes;       /* capacities of one batch (one executor) */
+    int max_batch_nodes;
+    int max_batch_pixels;
+    int max_batch_edges;
+    int gn_iters, pcg_iters;    /* per solve */
+    int precision;              /* WS_PREC_MIXED or WS_PREC_FP32 */
+} ws_server_config;
+
+/* One frame of a stream: non-owning device views, valid until the request is done. */
+typedef struct ws_frame {
+    const void *measure_vertex_confid;
+    const void *measure_normal_radius;
+    const void *reference_vertex;
+    const void *reference_normal;
+    const uint32_t *index_map;
+    const void *opticalflow;          /* NULL = zero flow */
+    int pitch;                        /* texels, 0 = width */
+    float cam2world[16];
+    const float *node_motion_pred;    /* NULL = none */
+    float *solution_out;              /* optional device buffer (8 floats per node) that receives
+                                         this frame's solution; NULL = only the resident warp */
+} ws_frame;
+
+typedef struct ws_request_info {
+    int status;                 /* WS_OK when solved, WS_ERR_NOT_READY while waiting or running */
+    int scene;                  /* stream (scene) id */
+    int num_nodes;
+    int batch_scenes;           /* frames in the batch that solved it */
+    double queue_ms;            /* submit -> batch launch (host clock) */
+    double solve_ms;            /* batch launch -> batch done */
+    double latency_ms;          /* submit -> done */
+} ws_request_info;
+
+typedef struct ws_server_stats {
+    unsigned long long submitted, completed, failed, batches;
+    double mean_batch_scenes;
+    double p50_latency_ms, p99_latency_ms, mean_latency_ms;   /* over completed requests */
+    unsigned long long executor_bytes, resident_bytes, memory_budget;
+    int scenes;
+} ws_server_stats;
+
+/* Creates the executors (WS_ERR_CAPACITY if they alone exceed memory_budget) and starts the
+ * scheduler and completion threads. */
+int ws_server_create(const ws_server_config *cfg, ws_server **out);
+/* Finishes the batches in flight, drops waiting requests, frees everything. */
+int ws_server_destroy(ws_server *s);
+/* Copies a stream's static state (surfel knn and weights, node coordinates, graph, connect
+ * weights, camera, penalties) and its initial warp into resident device memory.  Map fields
+ * of `scene` are ignored.  WS_ERR_CAPACITY if the resident bytes would exceed the budget. */
+int ws_server_add_scene(ws_server *s, const ws_inputs *scene, int *scene_id);
+/* WS_ERR_NOT_READY while the scene has frames waiting or in flight. */
+int ws_server_remove_scene(ws_server *s, int scene_id);
+/* Queues one frame of a stream.  WS_ERR_CAPACITY if the scene alone exceeds a batch. */
+int ws_submit(ws_server *s, int scene_id, const ws_frame *frame, unsigned long long *request_id);
+/* Non-blocking status; a finished request stays queryable until ws_server_forget. */
+int ws_poll(ws_server *s, unsigned long long request_id, ws_request_info *info);
+/* Blocks until the request is done (or the server stops). */
+int ws_wait(ws_server *s, unsigned long long request_id, ws_request_info *info);
+int ws_server_forget(ws_server *s, unsigned long long request_id);
+/* The stream's resident warp (its latest solution), device pointer to 8 floats per node. */
+int ws_server_get_warp(ws_server *s, int scene_id, const float **dev_dq, int *num_nodes);
+/* Copies the stream's resident warp into `dev_out` (device, 8 floats per node) and waits for
+ * the copy; WS_ERR_NOT_READY while the stream has frames waiting or in flight. */
+int ws_server_copy_warp(ws_server *s, int scene_id, float *dev_out);
+/* Overwrites the stream's resident warp from device memory (8 floats per node);
+ * WS_ERR_NOT_READY while the stream has frames waiting or in flight. */
+int ws_server_set_warp(ws_server *s, int scene_id, const float *dev_dq);
+int ws_server_get_stats(ws_server *s, ws_server_stats *stats);
+
 /* Library version / build identification. */
 int ws_version(void);
 const char *ws_error_string(int status);

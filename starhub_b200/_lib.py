@@ -33,7 +33,9 @@ EXPORTED = [
     "ws_get_node2term", "ws_get_node_pairs", "ws_get_system", "ws_get_dense_jacobian", "ws_init_nodes",
     "ws_build_node_graph", "ws_skinning", "ws_forward_warp", "ws_splat_maps", "ws_version",
     "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
-    "ws_splat_maps_noalloc",
+    "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
+    "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
+    "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats",
 ]
 
 
@@ -63,6 +65,39 @@ class WsInputs(C.Structure):
         ("lambda_depth", C.c_float), ("lambda_optical_flow", C.c_float), ("lambda_reg", C.c_float),
         ("lambda_node_translation", C.c_float), ("lambda_feature", C.c_float),
         ("init_node_se3", C.c_void_p),
+    ]
+
+
+class WsServerConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int), ("memory_budget", C.c_ulonglong), ("executors", C.c_int),
+        ("max_batch_scenes", C.c_int), ("max_batch_nodes", C.c_int), ("max_batch_pixels", C.c_int),
+        ("max_batch_edges", C.c_int), ("gn_iters", C.c_int), ("pcg_iters", C.c_int), ("precision", C.c_int),
+    ]
+
+
+class WsFrame(C.Structure):
+    _fields_ = [
+        ("measure_vertex_confid", C.c_void_p), ("measure_normal_radius", C.c_void_p),
+        ("reference_vertex", C.c_void_p), ("reference_normal", C.c_void_p), ("index_map", C.c_void_p),
+        ("opticalflow", C.c_void_p), ("pitch", C.c_int), ("cam2world", C.c_float * 16),
+        ("node_motion_pred", C.c_void_p), ("solution_out", C.c_void_p),
+    ]
+
+
+class WsRequestInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("scene", C.c_int), ("num_nodes", C.c_int), ("batch_scenes", C.c_int),
+        ("queue_ms", C.c_double), ("solve_ms", C.c_double), ("latency_ms", C.c_double),
+    ]
+
+
+class WsServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_ulonglong), ("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
+        ("batches", C.c_ulonglong), ("mean_batch_scenes", C.c_double), ("p50_latency_ms", C.c_double),
+        ("p99_latency_ms", C.c_double), ("mean_latency_ms", C.c_double), ("executor_bytes", C.c_ulonglong),
+        ("resident_bytes", C.c_ulonglong), ("memory_budget", C.c_ulonglong), ("scenes", C.c_int),
     ]
 
 
@@ -113,6 +148,18 @@ def load() -> C.CDLL:
         "ws_set_profiling": (i, [vp, i]),
         "ws_get_phase_times": (i, [vp, vp, vp, i, pi]),
         "ws_graph_kernel_count": (i, [vp, pi]),
+        "ws_server_create": (i, [C.POINTER(WsServerConfig), C.POINTER(vp)]),
+        "ws_server_destroy": (i, [vp]),
+        "ws_server_add_scene": (i, [vp, C.POINTER(WsInputs), pi]),
+        "ws_server_remove_scene": (i, [vp, i]),
+        "ws_submit": (i, [vp, i, C.POINTER(WsFrame), C.POINTER(C.c_ulonglong)]),
+        "ws_poll": (i, [vp, C.c_ulonglong, C.POINTER(WsRequestInfo)]),
+        "ws_wait": (i, [vp, C.c_ulonglong, C.POINTER(WsRequestInfo)]),
+        "ws_server_forget": (i, [vp, C.c_ulonglong]),
+        "ws_server_get_warp": (i, [vp, i, C.POINTER(vp), pi]),
+        "ws_server_copy_warp": (i, [vp, i, vp]),
+        "ws_server_set_warp": (i, [vp, i, vp]),
+        "ws_server_get_stats": (i, [vp, C.POINTER(WsServerStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

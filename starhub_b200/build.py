@@ -18,9 +18,9 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libwarpsolve.so"
-SOURCES = ["ws_api.cu", "ws_index.cu", "ws_solve.cu", "ws_graph.cu"]
+SOURCES = ["ws_api.cu", "ws_index.cu", "ws_solve.cu", "ws_graph.cu", "ws_server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-pthread",
          "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
 
 
@@ -58,7 +58,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     objs = [str(BUILD / (s + ".o")) for s in SOURCES]
     if force or jobs or not LIB.exists():
         tmp = LIB.with_suffix(".so.tmp")
-        run([cc, *ARCH, "-shared", "--cudart", "static", "-o", str(tmp), *objs])
+        run([cc, *ARCH, "-shared", "--cudart", "static", "-Xcompiler", "-pthread", "-o", str(tmp), *objs])
         os.replace(tmp, LIB)
     return LIB
 
