@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--cpu-sample", type=int, default=8, help="scenes in the bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--serving-requests", type=int, default=2000,
+                   help="requests of the serving run (32 frame streams, 1k-16k nodes); 0 skips it")
     return p.parse_args()
 
 
@@ -375,6 +377,27 @@ def main():
                "sample": f"{len(sample)} of the {len(ds)} scenes (evenly spaced), FP32 restatement, index build + "
                          f"5 GN x 20 PCG each, {dt:.1f} s"}
 
+    # ---- serving: 32 frame streams against the continuous-batching server ----
+    serving_out = None
+    if args.serving_requests > 0:
+        from starhub_b200 import serving
+        srng = np.random.default_rng(args.seed + 4)
+        counts = np.exp(srng.uniform(np.log(1000), np.log(16000), 32)).astype(int)
+        streams = serving.build_streams(counts, frames=8, seed=args.seed + 4 + 1000 * rank)
+        budget = 40e9
+        with serving.Server(memory_budget=int(budget), executors=2, max_batch_scenes=32,
+                            max_batch_nodes=int(counts.sum()) + 1024, max_batch_pixels=32 * 640 * 480,
+                            max_batch_edges=int(sum(x.ds.num_edges for x in streams)) + 1024,
+                            gn_iters=GN_ITERS, pcg_iters=PCG_ITERS, device=local) as srv:
+            r = serving.run_streams(srv, streams, args.serving_requests, seed=args.seed)
+        serving_out = {"streams": 32, "node_counts": "log-uniform [1000, 16000]",
+                       "arrivals": "every 33 ms + Exp(5 ms) per stream", "requests": r["requests"],
+                       "solved": r["solved"], "solves_per_s": r["solves_per_s"], "p50_ms": r["p50_ms"],
+                       "p99_ms": r["p99_ms"], "mean_batch_scenes": r["mean_batch_scenes"], "executors": 2,
+                       "budget_gb": budget / 1e9, "executor_gb": r["executor_bytes"] / 1e9,
+                       "resident_gb": r["resident_bytes"] / 1e9}
+        del streams
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -396,6 +419,7 @@ def main():
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_, "ms_per_launch": ms_},
             "cpu_baseline": cpu,
+            "serving": serving_out,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": sampler.summary(),

@@ -1,0 +1,100 @@
+"""Large union scene with the optical-flow term (torus + sphere + bumpy plane at 0.8-1.5 m,
+1.2 M surfels, about 8k nodes, 1280x720, flow on a 4-px grid with 0.5 px noise and 10%
+uniform outliers, lambda_of = 0.1, 10 Gauss-Newton x 30 PCG iterations).
+
+The compaction with flow targets (round-to-nearest of x + flow, y + flow) must be
+bit-exact, the first iteration's terms and step must match the FP64 oracle, and the
+mixed-precision solve must be within 1e-4 relative twist error and 1e-5 m warped-position
+error of the FP64 oracle where the Gauss-Newton trajectory is stable (see the 10 x 30 case).  The reference hard-codes lambda_of = 0, so this
+is oracle-only parity (the scene also exceeds the reference's node and surfel caps).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def union_scene(ws):
+    from starhub_b200 import scenes
+    from starhub_b200.solver import GpuGeometry
+    return scenes.make_scene(scenes.config_spec(1), GpuGeometry(), seed=1_000_003 * 1)
+
+
+def test_flow_compaction_bit_exact(union_scene, orc):
+    import torch
+    from starhub_b200.solver import DeviceScene, WarpSolver
+    sc = union_scene
+    assert sc.flow is not None and np.abs(sc.flow).max() > 0
+    ds = DeviceScene.from_scene(sc)
+    s = WarpSolver(max_nodes=ds.num_nodes, max_pixels=ds.num_pixels, max_edges=ds.num_edges)
+    s.SetSolverInputs(ds)
+    s.SolveStreamed(1, 1, stream=torch.cuda.Stream())
+    s.Sync()
+    pix, knn, sw, cw = s.dense_terms()
+    opix, oknn, osw, ocw = orc.compact_pixels(sc)
+    np.testing.assert_array_equal(pix, opix)
+    np.testing.assert_array_equal(knn, oknn)
+    np.testing.assert_array_equal(sw, osw)
+    np.testing.assert_array_equal(cw, ocw)
+
+
+def _solve(sc, gn, pcg):
+    import torch
+    from starhub_b200.solver import DeviceScene, WarpSolver
+    ds = DeviceScene.from_scene(sc)
+    assert ds.lambda_of > 0
+    s = WarpSolver(max_nodes=ds.num_nodes, max_pixels=ds.num_pixels, max_edges=ds.num_edges)
+    s.SetSolverInputs(ds)
+    s.SolveStreamed(gn, pcg, stream=torch.cuda.Stream())
+    s.Sync()
+    return s.SolvedNodeSE3(0).cpu().numpy().copy()
+
+
+@pytest.mark.parametrize("gn,pcg", [(5, 30), (10, 100)])
+def test_flow_solve_matches_fp64_oracle(union_scene, orc, gn, pcg):
+    from starhub_b200.scenes import position_error, twist_error
+    sc = union_scene
+    dq = _solve(sc, gn, pcg)
+    ref = orc.solve(sc, gn_iters=gn, pcg_iters=pcg)
+    assert twist_error(dq, ref, sc.nodes) <= 1e-4
+    assert position_error(sc, dq, ref) <= 1e-5
+
+
+def test_flow_solve_at_10x30_tracks_the_oracle_mixed_mode(union_scene, orc):
+    """At 10 Gauss-Newton x 30 PCG the trajectory of this scene is sensitive: the validity
+    tests of the dense terms (normal angle, depth gap) switch terms on or off depending on
+    precision-level differences of the unconverged steps, and the CPU oracle's own mixed-
+    precision restatement departs from its FP64 mode by a few 1e-3 as well.  The device
+    result must be as close to FP64 as that restatement (and within 1e-4 when it is)."""
+    from starhub_b200.scenes import twist_error
+    sc = union_scene
+    dq = _solve(sc, 10, 30)
+    ref = orc.solve(sc, gn_iters=10, pcg_iters=30)
+    mixed = orc.solve(sc, gn_iters=10, pcg_iters=30, precision=orc.ORC_PREC_MIXED)
+    bound = max(1e-4, 1.5 * twist_error(mixed, ref, sc.nodes))
+    assert twist_error(dq, ref, sc.nodes) <= bound
+
+
+def test_flow_first_iteration_terms_and_step(union_scene, orc):
+    """First Gauss-Newton iteration with the flow channels active: residuals and gradients
+    of all three channels against the FP64 oracle, and the first step."""
+    import torch
+    from starhub_b200.solver import DeviceScene, WarpSolver
+    sc = union_scene
+    ds = DeviceScene.from_scene(sc)
+    s = WarpSolver(max_nodes=ds.num_nodes, max_pixels=ds.num_pixels, max_edges=ds.num_edges)
+    s.SetSolverInputs(ds)
+    s.SolveStreamed(1, sc.pcg_iters, stream=torch.cuda.Stream())
+    s.Sync()
+    _, info64 = orc.solve(sc, gn_iters=1, pcg_iters=sc.pcg_iters, debug=True)
+    res, grad = s.dense_jacobian()
+    assert np.abs(info64["residual"][:, 1:]).max() > 0          # flow channels are active
+    np.testing.assert_allclose(res, info64["residual"], atol=2e-6 * max(1.0, np.abs(info64["residual"]).max()),
+                               rtol=0)
+    np.testing.assert_allclose(grad, info64["gradient"], atol=2e-5 * np.abs(info64["gradient"]).max(), rtol=0)
+    sysm = s.system()
+    c = sc.nodes[:, :3].astype(np.float64)
+    ref = info64["step"].astype(np.float64).copy()
+    ref[:, 3:] -= np.cross(c, ref[:, :3])
+    np.testing.assert_allclose(sysm["step"], ref, atol=1e-4 * np.abs(ref).max(), rtol=0)
