@@ -57,10 +57,31 @@ def scene_node_targets(n, seed):
     return np.exp(rng.uniform(np.log(500), np.log(8000), n)).astype(int)
 
 
+def rank_seed(seed, rank):
+    """Scene seed of a replica: every rank solves its own, different scenes (weak scaling)."""
+    return seed + 7919 * rank
+
+
+def max_over_ranks(ms, world, device):
+    """Device time of the slowest rank (all ranks take the same collective step)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, scenes_per_rank, steps, max_ms):
+    """Whole-job solves/s: all ranks' scenes over the slowest rank's time."""
+    return world * scenes_per_rank * steps / (max_ms / 1e3)
+
+
 def build_scenes(n, seed, geometry, rank=0):
     from starhub_b200 import scenes
     out = []
-    for i, target in enumerate(scene_node_targets(n, seed + 7919 * rank)):
+    for i, target in enumerate(scene_node_targets(n, rank_seed(seed, rank))):
         spec = scenes.spec_for_nodes(int(target), scenes.config_spec(2))
         out.append(scenes.make_scene(spec, geometry, seed=1_000_003 * 2 + 1000 * rank + i))
     return out
@@ -250,12 +271,8 @@ def main():
         torch.cuda.synchronize(dev)
     status = batch._lib.ws_sync_status(batch._h)
     step_ms = np.array([a.elapsed_time(b_) for a, b_ in ev])
-    total_ms = t_all0.elapsed_time(t_all1)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * len(ds) * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(t_all0.elapsed_time(t_all1), world, dev)
+    value = job_throughput(world, len(ds), args.steps, total_ms)
 
     # ---- accuracy of the timed configuration: a sample of scenes vs the FP64 oracle (rank 0) ----
     # (checked in the test suite; the bench records the twist error of one scene per run)
@@ -336,12 +353,8 @@ def main():
         e2e_step()
     q1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = q0.elapsed_time(q1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * len(ds) * e2e_steps / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1), world, dev)
+    e2e_value = job_throughput(world, len(ds), e2e_steps, e2e_ms)
 
     # ---- roofline of the dominant kernel ----
     peak, peak_kind = measured_peak_hbm()
