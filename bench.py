@@ -386,9 +386,14 @@ def main():
         sample = [host_scenes[i] for i in idx]
         threads = os.cpu_count() or 1
         rate, dt = cpu_solve_rate(sample, threads, precision=1)
+        rate64, dt64 = cpu_solve_rate(sample, threads, precision=0)
+        rate1, dt1 = cpu_solve_rate(sample[:2], 1, precision=1)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{len(sample)} of the {len(ds)} scenes (evenly spaced), FP32 restatement, index build + "
-                         f"5 GN x 20 PCG each, {dt:.1f} s"}
+                         f"5 GN x 20 PCG each, {dt:.1f} s",
+               "fp64_all_cores": rate64, "fp32_single_thread": rate1,
+               "other_samples": f"FP64 restatement on the same scenes ({dt64:.1f} s); FP32 single-threaded on the "
+                                f"first 2 of them ({dt1:.1f} s)"}
 
     # ---- serving: 32 frame streams against the continuous-batching server ----
     serving_out = None
