@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--seed", type=int, default=2)
     p.add_argument("--cpu-sample", type=int, default=8, help="scenes in the bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--spmv-replicas", type=int, default=6,
+                   help="replicate the scene batch this many times for the >1 GB SpMV measurement; 1 skips it")
     p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the serving run (32 frame streams, 1k-16k nodes); 0 skips it")
     return p.parse_args()
@@ -150,6 +152,30 @@ def load_traffic():
         except Exception:
             return {}
     return {}
+
+
+def measure_spmv(solver, n_nodes, nnzb, stream, dev, launches=20, warmup=3):
+    """Times ws_spmv on the solver's assembled matrix; algorithmic bytes per launch:
+    nnzb * (144 + 4) + N * (24 + 24) + 4 * (N + 1)."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.randn((n_nodes, 8), device=dev, generator=g)
+    y = torch.empty_like(x)
+    for _ in range(warmup):
+        solver.spmv(x, y, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(launches):
+        solver.spmv(x, y, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / launches
+    bytes_ = nnzb * (144 + 4) + n_nodes * (24 + 24) + 4 * (n_nodes + 1)
+    peak, kind = measured_peak_hbm()
+    gbs = bytes_ / (ms / 1e3) / 1e9
+    return {"nodes": n_nodes, "block_nnz": int(nnzb), "algorithmic_bytes": int(bytes_), "ms_per_launch": ms,
+            "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak, "peak_kind": kind}
 
 
 def cpu_solve_rate(sample, threads, precision):
@@ -356,6 +382,21 @@ def main():
     e2e_ms = max_over_ranks(q0.elapsed_time(q1), world, dev)
     e2e_value = job_throughput(world, len(ds), e2e_steps, e2e_ms)
 
+    # ---- standalone block-SpMV (ws_spmv) on the assembled matrices: the 64 scenes, and the
+    #      same scenes replicated 6x in one batch so that the matrix exceeds 1 GB ----
+    nnzb64 = sum(ds[i].num_nodes + 2 * counts[i]["half_pairs"] for i in range(len(ds)))
+    spmv_out = {"batch": measure_spmv(batch, tot_nodes, nnzb64, stream, dev)}
+    if args.spmv_replicas > 1:
+        rep = args.spmv_replicas
+        big = WarpSolver(max_nodes=rep * tot_nodes, max_pixels=rep * tot_pix, max_edges=rep * tot_edges,
+                         max_scenes=rep * len(ds), device=local)
+        big.SetBatchInputs(ds * rep)
+        big.SolveStreamed(1, 1, stream=stream)
+        big.Sync()
+        spmv_out[f"batch_x{rep}"] = measure_spmv(big, rep * tot_nodes, rep * nnzb64, stream, dev)
+        del big
+        torch.cuda.empty_cache()
+
     # ---- roofline of the dominant kernel ----
     peak, peak_kind = measured_peak_hbm()
     n_tot = tot_nodes
@@ -438,6 +479,7 @@ def main():
                          "algorithmic_bytes_per_launch": bytes_, "ms_per_launch": ms_},
             "cpu_baseline": cpu,
             "serving": serving_out,
+            "spmv": spmv_out,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": sampler.summary(),

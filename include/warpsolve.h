@@ -118,6 +118,15 @@ int ws_sync_status(ws_solver *solver);
  * 8 floats per node of `scene`, valid until the next ws_set_* on this solver. */
 int ws_get_solution(ws_solver *solver, int scene, const float **dev_node_se3, int *num_nodes);
 
+/* ApplySpMVBinBlockCSR::ApplySpMV / BinBlockCSR<6>::SparseMV
+ * (libs/star/pcg_solver/ApplySpMVBinBlockCSR.cuh:12-27,92-111, BinBlockCSR.cuh:6-34):
+ * y = A x with the block matrix assembled in the last Gauss-Newton iteration of the last
+ * solve, for every scene of the batch at once.  x and y are device arrays of 8 floats per
+ * node (6 used) in batch order: scene i's nodes follow those of scenes 0..i-1.  In
+ * WS_PREC_MIXED the unknowns are node-centred twists (t' = t - c x w), as in the solve.
+ * Asynchronous on `stream`; WS_ERR_NOT_READY before the first solve. */
+int ws_spmv(ws_solver *solver, const float *x, float *y, void *stream);
+
 /* Counts of the last index build (host copies; synchronises). */
 int ws_get_counts(ws_solver *solver, int scene, int *num_dense_terms, int *num_half_pairs, int *num_n2t_kv);
 

@@ -537,6 +537,14 @@ int ws_sync_status(ws_solver *h) {
     return flag;
 }
 
+int ws_spmv(ws_solver *h, const float *x, float *y, void *stream) {
+    if (!h || !x || !y) return WS_ERR_INVALID_ARGUMENT;
+    ws::Workspace &w = h->w;
+    if (!w.have_solution) return WS_ERR_NOT_READY;
+    cudaSetDevice(w.device);
+    return ws::gn_spmv(w, x, y, (cudaStream_t)stream) == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
 int ws_get_solution(ws_solver *h, int scene, const float **dev, int *num_nodes) {
     if (!h || !dev || !num_nodes) return WS_ERR_INVALID_ARGUMENT;
     ws::Workspace &w = h->w;

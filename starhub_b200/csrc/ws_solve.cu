@@ -940,19 +940,22 @@ __device__ __forceinline__ const float *slot_block(const PcgArgs &A, uint32_t co
                                 : A.pair_blocks + 36ull * min(ref & ~kRefTransposed, A.cap_half - 1);
 }
 
-// Starts a chunk: copies of each slot's block and of its column's s/d record into `stage`,
-// and a register load of beta.  The chunk's 16-byte parts (9 per block, 4 per record) are
-// spread flat over the lanes, so each copy instruction reads a few whole blocks or records
-// instead of one piece of 32 of them.
-__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *sd_old, uint4 x, float *stage, int lane,
+// Starts a chunk: copies of each slot's block and of its column's vector record into
+// `stage`, and (PCG) a register load of beta.  The PCG's vector record is the column's s/d
+// pair (64 B); a plain SpMV's is x of the column (32 B).  The chunk's 16-byte parts (9 per
+// block, 4 or 2 per vector record) are spread flat over the lanes, so each copy
+// instruction reads a few whole blocks or records instead of one piece of 32 of them.
+template <bool kPcg>
+__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_in, uint4 x, float *stage, int lane,
                                            PcgOperands &op) {
+    constexpr int kVecParts = kPcg ? 4 : 2;
     op.slot = x;
     const float *blk = nullptr, *vec = nullptr;
     if (x.z != kInvalidIndex) {
         const uint32_t col = min(x.x, A.total_nodes - 1);
         blk = slot_block(A, col, x.y);
-        vec = sd_old + 16ull * col;
-        op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
+        vec = vec_in + (kPcg ? 16ull : 8ull) * col;
+        if (kPcg) op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
     }
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
@@ -962,8 +965,8 @@ __device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *sd_ol
         if (b) cp_async16(stage + kPcgSlot * e + 4 * piece, b + 4 * piece);
     }
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int part = 32 * p + lane, e = part >> 2, piece = part & 3;
+    for (int p = 0; p < kVecParts; ++p) {
+        const int part = 32 * p + lane, e = part / kVecParts, piece = part - kVecParts * e;
         const float *v = reinterpret_cast<const float *>(
             __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vec), e));
         if (v) cp_async16(stage + kPcgSlot * e + 36 + 4 * piece, v + 4 * piece);
@@ -971,8 +974,12 @@ __device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *sd_ol
     cp_async_commit();
 }
 
-__device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *sd_old,
-                            float *sd_new, float *wsm, int lane) {
+// kPcg: phase A of a PCG iteration (vec_in = s/d records of the previous iteration, out =
+// the s/d records whose d this iteration writes, plus q and the group partials of <d, q>).
+// Otherwise a plain y = A x over the warp's rows (vec_in = x, out = y, 8 floats per node).
+template <bool kPcg>
+__device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
+                            float *out, float *wsm, int lane) {
     if (g0 >= g1) return;
     float *stage[2] = {wsm, wsm + kPcgChunkFloats};
     float *dring = wsm + 2 * kPcgChunkFloats;                 // [kPcgRing][8] d of the row, by row
@@ -981,14 +988,14 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
     const uint32_t nchunks = e1 > e0 ? (e1 - e0 + 31) / 32 : 0;
     uint4 nxt = load_slot(A.entry_info, e0 + 32 + lane, e1);
     PcgOperands cur;
-    issue_chunk(A, sd_old, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
+    issue_chunk<kPcg>(A, vec_in, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
     uint32_t group = g0, group_end = (g0 + 1 < A.total_groups) ? A.group_row[g0 + 1] : A.total_nodes;
     for (uint32_t j = 0; j < nchunks; ++j) {
         // chunk j + 1 in flight, chunk j + 2 records requested
         PcgOperands next;
-        issue_chunk(A, sd_old, nxt, stage[(j + 1) & 1], lane, next);
+        issue_chunk<kPcg>(A, vec_in, nxt, stage[(j + 1) & 1], lane, next);
         const uint4 after = load_slot(A.entry_info, e0 + 32 * (j + 2) + lane, e1);
         cp_async_wait_prior();
         __syncwarp();
@@ -998,13 +1005,18 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
         float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         float *mine = stage[j & 1] + kPcgSlot * lane;
         if (valid) {
-            const float beta = (float)cur.beta;
+            float dv[6];
             const float4 s0 = reinterpret_cast<const float4 *>(mine + 36)[0];
             const float2 s1 = reinterpret_cast<const float2 *>(mine + 40)[0];
-            const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
-            const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
-            const float dv[6] = {s0.x + beta * d0.x, s0.y + beta * d0.y, s0.z + beta * d0.z,
-                                 s0.w + beta * d0.w, s1.x + beta * d1.x, s1.y + beta * d1.y};
+            if (kPcg) {
+                const float beta = (float)cur.beta;
+                const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
+                const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
+                dv[0] = s0.x + beta * d0.x; dv[1] = s0.y + beta * d0.y; dv[2] = s0.z + beta * d0.z;
+                dv[3] = s0.w + beta * d0.w; dv[4] = s1.x + beta * d1.x; dv[5] = s1.y + beta * d1.y;
+            } else {
+                dv[0] = s0.x; dv[1] = s0.y; dv[2] = s0.z; dv[3] = s0.w; dv[4] = s1.x; dv[5] = s1.y;
+            }
             float m[36];
             const float4 *blk = reinterpret_cast<const float4 *>(mine);
 #pragma unroll
@@ -1029,7 +1041,7 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
             float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
             pp[0] = make_float4(p[0], p[1], p[2], p[3]);
             pp[1] = make_float4(p[4], p[5], 0.f, 0.f);
-            if (xref == kInvalidIndex) {   // diagonal slot: d of the row itself
+            if (kPcg && xref == kInvalidIndex) {   // diagonal slot: d of the row itself
                 float4 *dd = reinterpret_cast<float4 *>(dring + 8 * (xrow & (kPcgRing - 1)));
                 dd[0] = make_float4(dv[0], dv[1], dv[2], dv[3]);
                 dd[1] = make_float4(dv[4], dv[5], 0.f, 0.f);
@@ -1065,7 +1077,11 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
                 sum[4] += b.x;
                 sum[5] += b.y;
             }
-            if (ends_row) {
+            if (ends_row && !kPcg) {
+                float4 *yo = reinterpret_cast<float4 *>(out + 8ull * xrow);
+                yo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
+                yo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
+            } else if (ends_row) {
                 const float *dn = dring + 8 * (xrow & (kPcgRing - 1));
                 double dot = 0.0;
                 float dotf = 0.f;
@@ -1075,7 +1091,7 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
                     dotf += dn[i] * sum[i];
                 }
                 float4 *qo = reinterpret_cast<float4 *>(A.q + 8ull * xrow);
-                float4 *dno = reinterpret_cast<float4 *>(sd_new + 16ull * xrow + 8);
+                float4 *dno = reinterpret_cast<float4 *>(out + 16ull * xrow + 8);
                 qo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
                 qo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
                 dno[0] = make_float4(dn[0], dn[1], dn[2], dn[3]);
@@ -1092,7 +1108,7 @@ __device__ void pcg_phase_a(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
         __syncwarp();
         // groups whose rows are all done: their <d, q> partial, summed in row order
         const uint32_t done_below = cont ? last_row : last_row + 1;
-        while (group < g1 && group_end <= done_below) {
+        while (kPcg && group < g1 && group_end <= done_below) {
             const uint32_t grow = A.group_row[group];
             double v = 0.0;
             if (grow + lane < group_end) v = gring[(grow + lane) & (kPcgRing - 1)];
@@ -1170,7 +1186,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
         float *sd_new = (it & 1) ? A.sd0 : A.sd1;
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
-        pcg_phase_a(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
+        stream_rows<true>(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
         publish_range(A, g_begin, g_end, 0, lane);
         if (!grid_barrier(A.barrier, A.err)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
@@ -1246,6 +1262,20 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     }
 }
 
+// Standalone y = A x over the assembled symmetric store of the last Gauss-Newton iteration
+// (x, y: 8 floats per node), with the PCG's slot-balanced warp ranges and streaming.
+__global__ void __launch_bounds__(kPcgThreads, 3) k_spmv(PcgArgs A, const float *x, float *y) {
+    extern __shared__ __align__(16) float pcg_smem[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
+    const uint32_t g_begin = min(A.warp_groups[gwarp], A.total_groups);
+    const uint32_t g_end = max(g_begin, min(A.warp_groups[gwarp + 1], A.total_groups));
+    const uint32_t r_begin = g_begin < A.total_groups ? A.group_row[g_begin] : A.total_nodes;
+    const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
+    stream_rows<false>(A, g_begin, g_end, r_begin, r_end, x, y, wsm, lane);
+}
+
 // One warp per row group when that fits, else every co-resident block.
 int pcg_launch_blocks(const Workspace &w) {
     const uint32_t want = (w.total_chunks + (kPcgThreads / 32) - 1) / (kPcgThreads / 32);
@@ -1256,6 +1286,7 @@ int pcg_warps_per_block() { return kPcgThreads / 32; }
 int pcg_max_blocks(int device) {
     int per_sm = 0, sms = 0;
     cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmemBytes);
+    cudaFuncSetAttribute(k_spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmemBytes);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, kPcgSmemBytes);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per_sm) * std::max(1, sms);
@@ -1310,7 +1341,7 @@ void gn_assemble_pair(Workspace &w, cudaStream_t st) {
     count_launch(w);
 }
 
-cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
+static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     PcgArgs a;
     a.scenes = w.scenes;
     a.group_scene = w.chunk_scene;
@@ -1339,6 +1370,11 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     a.centers = w.centers;
     a.pcg_iters = pcg_iters;
     a.fp64 = (w.precision == WS_PREC_MIXED) ? 1 : 0;
+    return a;
+}
+
+cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
+    PcgArgs a = pcg_args(w, pcg_iters);
     const int grid = pcg_launch_blocks(w);
     // a barrier or counter left half-way by an earlier timed-out launch must not leak into this one
     cudaMemsetAsync(w.barrier, 0, 4 * sizeof(uint32_t), st);
@@ -1346,6 +1382,12 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     void *args[] = {&a};
     count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);
+}
+
+cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st) {
+    const PcgArgs a = pcg_args(w, 0);
+    k_spmv<<<pcg_launch_blocks(w), kPcgThreads, kPcgSmemBytes, st>>>(a, x, y);
+    return cudaGetLastError();
 }
 
 cudaError_t gn_iteration(Workspace &w, int pcg_iters, cudaStream_t st) {

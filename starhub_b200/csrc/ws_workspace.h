@@ -138,6 +138,7 @@ void init_warp(Workspace &w, cudaStream_t st);
 // Occupancy of the persistent PCG kernel.
 int pcg_max_blocks(int device);
 int pcg_launch_blocks(const Workspace &w);
+cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st);
 int pcg_warps_per_block();
 
 // Launch accounting for the measurement hooks.

@@ -208,6 +208,11 @@ class WarpSolver:
         check(self._lib.ws_get_solution(self._h, scene, C.byref(p), C.byref(n)), "ws_get_solution")
         return _wrap_device_floats(p.value, n.value * 8, self.device).view(n.value, 8)
 
+    def spmv(self, x: torch.Tensor, y: torch.Tensor, stream=None) -> None:
+        """y = A x with the last assembled block matrix (x, y: (total_nodes, 8) float32 CUDA)."""
+        check(self._lib.ws_spmv(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), _stream_ptr(stream)),
+              "ws_spmv")
+
     # -- measurement ---------------------------------------------------------
     def set_profiling(self, enable: bool) -> None:
         check(self._lib.ws_set_profiling(self._h, 1 if enable else 0), "ws_set_profiling")
