@@ -1067,6 +1067,8 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
                 for (int i = 0; i < 6; ++i) sum[i] = carry[i];
             }
             const float *chunk = stage[j & 1];
+            // sequential in slot order; unrolled so that the loads of later slots overlap
+#pragma unroll 4
             for (int l = first; l <= lane; ++l) {
                 const float4 a = reinterpret_cast<const float4 *>(chunk + kPcgSlot * l)[0];
                 const float2 b = reinterpret_cast<const float2 *>(chunk + kPcgSlot * l + 4)[0];
