@@ -19,7 +19,7 @@ constexpr int kVecStride = 8;        // floats per node in PCG vectors
 constexpr int kDenseRecord = 32;     // floats per dense-term record (128 B)
 constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
-constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group
+constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group (divides 32)
 constexpr uint32_t kRefTransposed = 0x80000000u;   // entry_ref flag: lower-triangle use of a pair block
 
 // ---------------------------------------------------------------------------

@@ -788,6 +788,7 @@ __device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ void reduce_scene(const PcgArgs &A, uint32_t scene, int mode, int lane) {
     const Scene &sc = A.scenes[scene];
     double v = 0.0;
+#pragma unroll 8
     for (int c = lane; c < sc.num_chunks; c += 32) v += __ldcg(A.group_partial + sc.chunk_base + c);
     v = warp_sum(v);
     if (lane == 0) {
@@ -841,32 +842,32 @@ __device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end
     }
 }
 
-// Sum over the 16 lanes of a half warp (fixed butterfly inside the half).
-__device__ __forceinline__ double half_sum(double v) {
+// Sum over the kRowsPerGroup lanes of one group (fixed butterfly inside the group).
+__device__ __forceinline__ double group_sum(double v) {
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    for (int o = kRowsPerGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-__device__ __forceinline__ float half_sum(float v) {
+__device__ __forceinline__ float group_sum(float v) {
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    for (int o = kRowsPerGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
-// <u, v> over 6 entries in the precision of the mode, summed over the half warp's nodes.
-__device__ __forceinline__ double node_dot_half(const PcgArgs &A, const float *u, const float *v, bool valid) {
+// <u, v> over 6 entries in the precision of the mode, summed over the group's nodes.
+__device__ __forceinline__ double node_dot_group(const PcgArgs &A, const float *u, const float *v, bool valid) {
     if (A.fp64) {
         double p = 0.0;
         if (valid)
 #pragma unroll
             for (int i = 0; i < 6; ++i) p += (double)u[i] * (double)v[i];
-        return half_sum(p);
+        return group_sum(p);
     }
     float p = 0.f;
     if (valid)
 #pragma unroll
         for (int i = 0; i < 6; ++i) p += u[i] * v[i];
-    return (double)half_sum(p);
+    return (double)group_sum(p);
 }
 
 __device__ __forceinline__ void load6(const float *p, float *v) {
@@ -878,20 +879,19 @@ __device__ __forceinline__ void store6(float *p, const float *v) {
     reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
     reinterpret_cast<float2 *>(p + 4)[0] = make_float2(v[4], v[5]);
 }
-// y = M x for one node's 6x6 block (row-major).
+// y = M x for one node's 6x6 block (row-major), consumed a float4 at a time.
 __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y) {
-    float m[36];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        const float4 v = __ldg(reinterpret_cast<const float4 *>(M) + i);
-        m[4 * i] = v.x; m[4 * i + 1] = v.y; m[4 * i + 2] = v.z; m[4 * i + 3] = v.w;
-    }
+    for (int i = 0; i < 6; ++i) y[i] = 0.f;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        float a = 0.f;
+    for (int q = 0; q < 9; ++q) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(M) + q);
+        const float e4[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int c = 0; c < 6; ++c) a += m[6 * i + c] * x[c];
-        y[i] = a;
+        for (int k = 0; k < 4; ++k) {
+            const int e = 4 * q + k;
+            y[e / 6] += e4[k] * x[e % 6];
+        }
     }
 }
 
@@ -991,7 +991,15 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
     issue_chunk<kPcg>(A, vec_in, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
-    uint32_t group = g0, group_end = (g0 + 1 < A.total_groups) ? A.group_row[g0 + 1] : A.total_nodes;
+    // first rows of groups win .. win + 31 (lane i holds group win + i), reloaded as groups complete
+    uint32_t win = g0;
+    uint32_t win_row = (kPcg && g0 + lane < A.total_groups) ? A.group_row[g0 + lane] : A.total_nodes;
+    auto group_first = [&](uint32_t g) -> uint32_t {   // first row of group g (g >= win)
+        if (g >= A.total_groups) return A.total_nodes;
+        if (g - win < 32) return __shfl_sync(0xffffffffu, win_row, (int)(g - win));
+        return A.group_row[g];
+    };
+    uint32_t group = g0, group_end = kPcg ? group_first(g0 + 1) : 0u;
     for (uint32_t j = 0; j < nchunks; ++j) {
         // chunk j + 1 in flight, chunk j + 2 records requested
         PcgOperands next;
@@ -1017,27 +1025,23 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
             } else {
                 dv[0] = s0.x; dv[1] = s0.y; dv[2] = s0.z; dv[3] = s0.w; dv[4] = s1.x; dv[5] = s1.y;
             }
-            float m[36];
+            // A dv and A^T dv from one pass over the block, a float4 at a time
+            float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             const float4 *blk = reinterpret_cast<const float4 *>(mine);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) {
-                const float4 v = blk[i];
-                m[4 * i] = v.x;
-                m[4 * i + 1] = v.y;
-                m[4 * i + 2] = v.z;
-                m[4 * i + 3] = v.w;
+            for (int q = 0; q < 9; ++q) {
+                const float4 v = blk[q];
+                const float e4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e = 4 * q + k, r = e / 6, c = e % 6;
+                    a[r] += e4[k] * dv[c];
+                    t[c] += e4[k] * dv[r];
+                }
             }
             const bool tr = xref != kInvalidIndex && (xref & kRefTransposed) != 0;
 #pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                float a = 0.f, t = 0.f;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) {
-                    a += m[6 * i + c] * dv[c];
-                    t += m[6 * c + i] * dv[c];
-                }
-                p[i] = tr ? t : a;
-            }
+            for (int i = 0; i < 6; ++i) p[i] = tr ? t[i] : a[i];
             float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
             pp[0] = make_float4(p[0], p[1], p[2], p[3]);
             pp[1] = make_float4(p[4], p[5], 0.f, 0.f);
@@ -1111,7 +1115,7 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
         // groups whose rows are all done: their <d, q> partial, summed in row order
         const uint32_t done_below = cont ? last_row : last_row + 1;
         while (kPcg && group < g1 && group_end <= done_below) {
-            const uint32_t grow = A.group_row[group];
+            const uint32_t grow = group_first(group);
             double v = 0.0;
             if (grow + lane < group_end) v = gring[(grow + lane) & (kPcgRing - 1)];
             double part;
@@ -1125,7 +1129,11 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
             }
             if (lane == 0) A.group_partial[group] = part;
             ++group;
-            group_end = (group + 1 < A.total_groups) ? A.group_row[group + 1] : A.total_nodes;
+            if (group + 1 - win >= 32) {   // slide the window
+                win = group;
+                win_row = group + lane < A.total_groups ? A.group_row[group + lane] : A.total_nodes;
+            }
+            group_end = group_first(group + 1);
         }
         cur = next;
         nxt = after;
@@ -1135,20 +1143,21 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
     __syncwarp();
 }
 
-// One step of the per-node phases: lanes 0-15 take the rows of group g, lanes 16-31 those
-// of group g + 1 (fewer in a scene's last group).
+// One step of the per-node phases: lane l takes row l % kRowsPerGroup of group
+// g + l / kRowsPerGroup (a scene's last group may have fewer rows).
+constexpr int kGroupsPerStep = 32 / kRowsPerGroup;
 struct NodeStep {
     uint32_t gg, node, scene;
     bool group_ok, valid;
 };
 __device__ __forceinline__ NodeStep node_step(const PcgArgs &A, uint32_t g, uint32_t g_end, int lane) {
     NodeStep n;
-    n.gg = g + (uint32_t)(lane >> 4);
+    n.gg = g + (uint32_t)(lane / kRowsPerGroup);
     n.group_ok = n.gg < g_end;
     const uint32_t first = n.group_ok ? A.group_row[n.gg] : 0u;
     const uint32_t stop = !n.group_ok ? 0u : (n.gg + 1 < A.total_groups ? A.group_row[n.gg + 1] : A.total_nodes);
     n.scene = n.group_ok ? min(A.group_scene[n.gg], A.num_scenes - 1) : 0u;
-    n.node = first + (uint32_t)(lane & 15);
+    n.node = first + (uint32_t)(lane % kRowsPerGroup);
     n.valid = n.group_ok && n.node < stop;
     return n;
 }
@@ -1166,7 +1175,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
 
     // ---- init: r = b, s = M^-1 b, x = 0, d = 0, delta = <r, s> ----
-    for (uint32_t g = g_begin; g < g_end; g += 2) {
+    for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
         const NodeStep n = node_step(A, g, g_end, lane);
         float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (n.valid) {
@@ -1178,8 +1187,8 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
             store6(A.sd0 + 16ull * n.node + 8, zero);
             store6(A.x + 8ull * n.node, zero);
         }
-        const double part = node_dot_half(A, rv, sv, n.valid);
-        if ((lane & 15) == 0 && n.group_ok) A.group_partial[n.gg] = part;
+        const double part = node_dot_group(A, rv, sv, n.valid);
+        if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
     }
     publish_range(A, g_begin, g_end, 2, lane);
     if (!grid_barrier(A.barrier, A.err)) return;
@@ -1192,7 +1201,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         publish_range(A, g_begin, g_end, 0, lane);
         if (!grid_barrier(A.barrier, A.err)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
-        for (uint32_t g = g_begin; g < g_end; g += 2) {
+        for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
             const NodeStep n = node_step(A, g, g_end, lane);
             float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             if (n.valid) {
@@ -1212,8 +1221,8 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
                 store6(A.r + 8ull * n.node, rv);
                 store6(sd_new + 16ull * n.node, sv);
             }
-            const double part = node_dot_half(A, rv, sv, n.valid);
-            if ((lane & 15) == 0 && n.group_ok) A.group_partial[n.gg] = part;
+            const double part = node_dot_group(A, rv, sv, n.valid);
+            if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
         }
         publish_range(A, g_begin, g_end, 1, lane);
         if (!grid_barrier(A.barrier, A.err)) return;
@@ -1266,7 +1275,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 
 // Standalone y = A x over the assembled symmetric store of the last Gauss-Newton iteration
 // (x, y: 8 floats per node), with the PCG's slot-balanced warp ranges and streaming.
-__global__ void __launch_bounds__(kPcgThreads, 3) k_spmv(PcgArgs A, const float *x, float *y) {
+__global__ void __launch_bounds__(kPcgThreads, 8) k_spmv(PcgArgs A, const float *x, float *y) {
     extern __shared__ __align__(16) float pcg_smem[];
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
