@@ -126,6 +126,13 @@ int ws_get_solution(ws_solver *solver, int scene, const float **dev_node_se3, in
  * WS_PREC_MIXED the unknowns are node-centred twists (t' = t - c x w), as in the solve.
  * Asynchronous on `stream`; WS_ERR_NOT_READY before the first solve. */
 int ws_spmv(ws_solver *solver, const float *x, float *y, void *stream);
+/* The same operator applied matrix-free from the term records of the last Gauss-Newton
+ * iteration (J x per term, then J^T (J x) gathered per node over the node->term lists, plus
+ * the diagonal regulariser), without the assembled blocks.  No reference counterpart (the
+ * reference materialises A, ApplySpMVBinBlockCSR); it is the ApplySpMVBase plugin point
+ * (libs/star/pcg_solver/ApplySpMVBase.h:8-45) filled without a matrix, for callers that
+ * cannot hold one.  Allocates 16 bytes per pixel and edge of capacity on first use. */
+int ws_spmv_matrix_free(ws_solver *solver, const float *x, float *y, void *stream);
 
 /* Counts of the last index build (host copies; synchronises). */
 int ws_get_counts(ws_solver *solver, int scene, int *num_dense_terms, int *num_half_pairs, int *num_n2t_kv);

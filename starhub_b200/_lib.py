@@ -35,7 +35,7 @@ EXPORTED = [
     "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
     "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
     "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
-    "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv",
+    "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv", "ws_spmv_matrix_free",
 ]
 
 
@@ -161,6 +161,7 @@ def load() -> C.CDLL:
         "ws_server_set_warp": (i, [vp, i, vp]),
         "ws_server_get_stats": (i, [vp, C.POINTER(WsServerStats)]),
         "ws_spmv": (i, [vp, vp, vp, vp]),
+        "ws_spmv_matrix_free": (i, [vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

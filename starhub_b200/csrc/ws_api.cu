@@ -35,7 +35,7 @@ void free_all(ws::Workspace &w) {
                     w.n2t_val_alt, w.n2t_offset, w.pair_key, w.pair_key_alt, w.pair_val, w.pair_val_alt,
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
-                    w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
+                    w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.mf_ux, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
                     w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
                     w.error_flag};
     for (void *p : ptrs)
@@ -543,6 +543,23 @@ int ws_spmv(ws_solver *h, const float *x, float *y, void *stream) {
     if (!w.have_solution) return WS_ERR_NOT_READY;
     cudaSetDevice(w.device);
     return ws::gn_spmv(w, x, y, (cudaStream_t)stream) == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
+int ws_spmv_matrix_free(ws_solver *h, const float *x, float *y, void *stream) {
+    if (!h || !x || !y) return WS_ERR_INVALID_ARGUMENT;
+    ws::Workspace &w = h->w;
+    if (!w.have_solution) return WS_ERR_NOT_READY;
+    cudaSetDevice(w.device);
+    const size_t n4 = (size_t)w.cap_pixels + (size_t)w.cap_edges;
+    if (!w.mf_ux && cudaMalloc(&w.mf_ux, 16 * std::max<size_t>(1, n4)) != cudaSuccess) {
+        cudaGetLastError();
+        w.mf_ux = nullptr;
+        return WS_ERR_CAPACITY;
+    }
+    return ws::gn_spmv_matrix_free(w, x, y, w.mf_ux, w.mf_ux + 4ull * w.cap_pixels, (cudaStream_t)stream) ==
+                   cudaSuccess
+               ? WS_OK
+               : WS_ERR_CUDA;
 }
 
 int ws_get_solution(ws_solver *h, int scene, const float **dev, int *num_nodes) {

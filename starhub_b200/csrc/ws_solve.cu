@@ -1287,6 +1287,174 @@ __global__ void __launch_bounds__(kPcgThreads, 8) k_spmv(PcgArgs A, const float 
     stream_rows<false>(A, g_begin, g_end, r_begin, r_end, x, y, wsm, lane);
 }
 
+// ---------------------------------------------------------------------------
+// Matrix-free y = A x: the operator of the last Gauss-Newton iteration applied from the
+// term records, without the assembled blocks.  A = sum over terms and channels of u u^T,
+// with u the scaled Jacobian rows the assembly kernels use (lambda w J for dense terms,
+// lambda c J for smoothness edges), plus the diagonal regulariser.  Pass 1 forms per term
+// and channel  J x = sum over the term's nodes of u_node . x_node ; pass 2 gathers, per node,
+// y = sum over its terms of u_node (J x) in list order (one warp per node, fixed butterfly).
+// A term's four node ids are distinct (skinning picks distinct nodes).
+// ---------------------------------------------------------------------------
+__global__ void k_mf_dense(const Scene *scenes, const uint32_t *counts, const uint32_t *term_scene,
+                           const float *drec, const float4 *centers, int centred, const float *x, float *ux) {
+    const uint32_t n = counts[kCntDense];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const Scene &sc = scenes[term_scene[t]];
+        const float *rec = drec + (size_t)kDenseRecord * t;
+        float u[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t node = __float_as_uint(rec[26 + k]);
+            const float w = rec[22 + k];
+            const float4 x0 = *reinterpret_cast<const float4 *>(x + 8ull * node);
+            const float2 x1 = *reinterpret_cast<const float2 *>(x + 8ull * node + 4);
+            const float xv[6] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y};
+            const float4 c4 = centers[node];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                float gl[6];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) gl[q] = rec[6 * ch + q];
+                if (centred) recentre(gl, f3(c4.x, c4.y, c4.z));
+                float d = 0.f;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) d += gl[q] * xv[q];
+                u[ch] += w * d;
+            }
+        }
+        const float lam[3] = {sc.lam_depth, sc.lam_of, sc.lam_of};
+        reinterpret_cast<float4 *>(ux)[t] = make_float4(lam[0] * u[0], lam[1] * u[1], lam[2] * u[2], 0.f);
+    }
+}
+
+__global__ void k_mf_reg(const Scene *scenes, const uint32_t *edge_scene, uint32_t total_edges, const float *rrec,
+                         const float4 *centers, int centred, const float *x, float *ux) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total_edges; e += gridDim.x * blockDim.x) {
+        const Scene &sc = scenes[edge_scene[e]];
+        const float *rec = rrec + (size_t)kRegRecord * e;
+        const uint32_t ni = __float_as_uint(rec[8]), nj = __float_as_uint(rec[9]);
+        float u[3] = {0.f, 0.f, 0.f};
+        if (rec[7] != 0.f && ni != nj) {
+            const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const uint32_t node = side == 0 ? ni : nj;
+                float J[3][6];
+                reg_unit_jacobian(a3, b3, side == 0, J);
+                const float4 c4 = centers[node];
+                const float4 x0 = *reinterpret_cast<const float4 *>(x + 8ull * node);
+                const float2 x1 = *reinterpret_cast<const float2 *>(x + 8ull * node + 4);
+                const float xv[6] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y};
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    if (centred) recentre(J[ch], f3(c4.x, c4.y, c4.z));
+                    float d = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) d += J[ch][q] * xv[q];
+                    u[ch] += d;
+                }
+            }
+            const float s = sc.lam_reg * rec[6];
+            u[0] *= s;
+            u[1] *= s;
+            u[2] *= s;
+        }
+        reinterpret_cast<float4 *>(ux)[e] = make_float4(u[0], u[1], u[2], 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_mf_gather(const Scene *scenes, const Plan *plan, const uint32_t *node_scene,
+                                                   uint32_t total_nodes, const uint32_t *n2t_offset,
+                                                   const uint32_t *n2t_val, const float *drec, const float *rrec,
+                                                   const float *se3, const float4 *centers, int centred,
+                                                   const float *ux_dense, const float *ux_reg, const float *x,
+                                                   float *y) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total_nodes; g += warps) {
+        const Scene &sc = scenes[node_scene[g]];
+        const Plan &p = plan[node_scene[g]];
+        const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
+        const float4 c4 = centers[g];
+        const float3 cen = f3(c4.x, c4.y, c4.z);
+        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (uint32_t it = n2t_offset[g] + lane; it < n2t_offset[g + 1]; it += 32) {
+            const uint32_t term = n2t_val[it];
+            if (term < nd) {
+                const float *rec = drec + (size_t)kDenseRecord * (p.dense_begin + term);
+                float w = rec[22];   // weight of the last slot whose node is g
+#pragma unroll
+                for (int k = 1; k < 4; ++k) if (__float_as_uint(rec[26 + k]) == g) w = rec[22 + k];
+                const float4 u = reinterpret_cast<const float4 *>(ux_dense)[p.dense_begin + term];
+                const float uu[3] = {u.x, u.y, u.z};
+                const float lam[3] = {sc.lam_depth, sc.lam_of, sc.lam_of};
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    float gl[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) gl[q] = rec[6 * ch + q];
+                    if (centred) recentre(gl, cen);
+                    const float f = lam[ch] * w * uu[ch];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) acc[q] += f * gl[q];
+                }
+            } else if (term < nd + ne) {
+                const uint32_t e = sc.edge_base + term - nd;
+                const float *rec = rrec + (size_t)kRegRecord * e;
+                if (rec[7] == 0.f) continue;
+                float J[3][6];
+                reg_unit_jacobian(f3(rec[0], rec[1], rec[2]), f3(rec[3], rec[4], rec[5]), __float_as_uint(rec[8]) == g,
+                                  J);
+                const float4 u = reinterpret_cast<const float4 *>(ux_reg)[e];
+                const float uu[3] = {u.x, u.y, u.z};
+                const float s = sc.lam_reg * rec[6];
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    if (centred) recentre(J[ch], cen);
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) acc[q] += s * uu[ch] * J[ch][q];
+                }
+            } else if (term < nd + ne + nn && sc.lam_node != 0.f && sc.node_motion) {
+                const uint32_t nl = term - nd - ne;
+                const float scale = sc.lam_node * sc.node_motion[nl].w;
+                const float4 x0 = *reinterpret_cast<const float4 *>(x + 8ull * g);
+                const float2 x1 = *reinterpret_cast<const float2 *>(x + 8ull * g + 4);
+                const float xv[6] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y};
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    float J[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                    J[3 + ch] = scale;
+                    if (centred) recentre(J, cen);
+                    float d = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) d += J[q] * xv[q];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) acc[q] += d * J[q];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
+        if (lane == 0) {
+            // + 1e-3 S^T S x (node-centred twists) or 1e-3 x (origin twists)
+            const float4 x0 = *reinterpret_cast<const float4 *>(x + 8ull * g);
+            const float2 x1 = *reinterpret_cast<const float2 *>(x + 8ull * g + 4);
+            const float3 om = f3(x0.x, x0.y, x0.z), tr = f3(x0.w, x1.x, x1.y);
+            float r[6] = {om.x, om.y, om.z, tr.x, tr.y, tr.z};
+            if (centred) {
+                const float3 v = cross3(cen, om) + tr;   // translation part of S x
+                const float3 cv = cross3(cen, v);
+                r[0] = om.x - cv.x; r[1] = om.y - cv.y; r[2] = om.z - cv.z;
+                r[3] = v.x; r[4] = v.y; r[5] = v.z;
+            }
+            float4 *yo = reinterpret_cast<float4 *>(y + 8ull * g);
+            yo[0] = make_float4(acc[0] + 1e-3f * r[0], acc[1] + 1e-3f * r[1], acc[2] + 1e-3f * r[2], acc[3] + 1e-3f * r[3]);
+            yo[1] = make_float4(acc[4] + 1e-3f * r[4], acc[5] + 1e-3f * r[5], 0.f, 0.f);
+        }
+    }
+}
+
 // One warp per row group when that fits, else every co-resident block.
 int pcg_launch_blocks(const Workspace &w) {
     const uint32_t want = (w.total_chunks + (kPcgThreads / 32) - 1) / (kPcgThreads / 32);
@@ -1393,6 +1561,20 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     void *args[] = {&a};
     count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);
+}
+
+cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *ux_dense, float *ux_reg,
+                                cudaStream_t st) {
+    const int centred = w.precision == WS_PREC_MIXED ? 1 : 0;
+    k_mf_dense<<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(w.scenes, w.counts, w.d_scene, w.d_record,
+                                                                          w.centers, centred, x, ux_dense);
+    if (w.total_edges > 0)
+        k_mf_reg<<<grid_for(w.total_edges, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.edge_scene, w.total_edges,
+                                                                          w.r_record, w.centers, centred, x, ux_reg);
+    k_mf_gather<<<grid_for(w.total_nodes * 32u, 128, w.num_sms, 32), 128, 0, st>>>(
+        w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
+        w.centers, centred, ux_dense, ux_reg, x, y);
+    return cudaGetLastError();
 }
 
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st) {

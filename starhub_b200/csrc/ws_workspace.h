@@ -82,6 +82,8 @@ struct Workspace {
     uint32_t *entry_ref = nullptr;                           // [cap_blocks]
     uint4 *entry_info = nullptr;                             // [cap_blocks] (col, ref, row, scene) for the PCG
     uint32_t *pcg_warp_groups = nullptr;                     // [pcg_grid * warps per block + 1]
+    float *mf_ux = nullptr;             // matrix-free SpMV scratch: J x per dense term and edge (float4),
+                                        // allocated on first use
     float *diag_blocks = nullptr;                            // [cap_nodes * 36]
     float *pair_blocks = nullptr;                            // [cap_half * 36]
 
@@ -139,6 +141,8 @@ void init_warp(Workspace &w, cudaStream_t st);
 int pcg_max_blocks(int device);
 int pcg_launch_blocks(const Workspace &w);
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st);
+cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *ux_dense, float *ux_reg,
+                                cudaStream_t st);
 int pcg_warps_per_block();
 
 // Launch accounting for the measurement hooks.

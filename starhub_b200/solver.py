@@ -213,6 +213,11 @@ class WarpSolver:
         check(self._lib.ws_spmv(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), _stream_ptr(stream)),
               "ws_spmv")
 
+    def spmv_matrix_free(self, x: torch.Tensor, y: torch.Tensor, stream=None) -> None:
+        """y = A x applied from the term records (no assembled blocks)."""
+        check(self._lib.ws_spmv_matrix_free(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                            _stream_ptr(stream)), "ws_spmv_matrix_free")
+
     # -- measurement ---------------------------------------------------------
     def set_profiling(self, enable: bool) -> None:
         check(self._lib.ws_set_profiling(self._h, 1 if enable else 0), "ws_set_profiling")
