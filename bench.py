@@ -273,6 +273,7 @@ def main():
     batch = WarpSolver(max_nodes=tot_nodes, max_pixels=tot_pix, max_edges=tot_edges, max_scenes=len(ds),
                        device=local)
     batch.SetBatchInputs(ds)
+    tuning = batch.autotune(pcg_iters=PCG_ITERS, stream=stream)
     for _ in range(args.warmup):
         batch.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream, graph=True)
     batch.Sync()
@@ -316,6 +317,9 @@ def main():
     max_p = max(d.num_pixels for d in ds)
     max_e = max(d.num_edges for d in ds)
     plain = WarpSolver(max_nodes=max_n, max_pixels=max_p, max_edges=max_e, device=local)
+    mid = int(np.argsort([d.num_nodes for d in ds])[len(ds) // 2])
+    plain.SetSolverInputs(ds[mid])
+    plain_tuning = plain.autotune(pcg_iters=PCG_ITERS, stream=stream)   # on the median-size scene
     for d in ds[:2]:
         plain.SetSolverInputs(d)
         plain.SolveStreamed(GN_ITERS, PCG_ITERS, stream=stream)
@@ -466,11 +470,13 @@ def main():
                                    "surfels 130 x nodes, 640x480, 5 GN x 20 PCG, batched in one CUDA graph",
                        "scenes": len(ds), "total_nodes": tot_nodes, "dense_terms": nd_tot, "block_nnz": nnzb,
                        "precision": "fp32 bulk, fp64 pcg reductions + 6x6 cholesky",
+                       "autotuned": {k: tuning[k] for k in ("node_threads", "pair_threads", "pcg_blocks_per_sm")},
                        "l2": f"inputs larger than L2 ({tot_pix * 68 / 1e9:.2f} GB of maps per step)"},
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "lone_solve_p50": float(np.percentile(lone_ms, 50)),
                            "lone_solve_p99": float(np.percentile(lone_ms, 99))},
-            "plain": {"value": plain_rate, "unit": UNIT, "ms_for_all_scenes": plain_ms},
+            "plain": {"value": plain_rate, "unit": UNIT, "ms_for_all_scenes": plain_ms,
+                      "autotuned": {k: plain_tuning[k] for k in ("node_threads", "pair_threads", "pcg_blocks_per_sm")}},
             "served_vs_plain": value / plain_rate,
             "phases_ms_per_solve": {k: float(v) for k, v in phase_ms.items()},
             "phase_launches": {k: int(v) for k, v in phase_launch.items()},

@@ -305,6 +305,25 @@ int ws_server_copy_warp(ws_server *s, int scene_id, float *dev_out);
 int ws_server_set_warp(ws_server *s, int scene_id, const float *dev_dq);
 int ws_server_get_stats(ws_server *s, ws_server_stats *stats);
 
+/* ---- Autotuning of launch shapes ------------------------------------------------------
+ * No reference counterpart.  ws_autotune runs one Gauss-Newton iteration of the inputs set on
+ * the solver, then times, on that data, the node and pair assembly kernels at 64, 128 and
+ * 256 threads per block (the FP64 node kernel offers 64 and 128) and the persistent PCG at
+ * 1..k blocks per SM (k = what fits on an SM), which sets how many rows each warp owns; it keeps
+ * the fastest of each for the solver's later solves and reports the timings.  No choice changes
+ * a result: every sum runs in the same order at every shape.  Synchronises `stream`. */
+typedef struct ws_tuning {
+    int node_threads;           /* chosen threads per block, node assembly */
+    int pair_threads;           /* chosen threads per block, pair assembly */
+    int pcg_blocks_per_sm;      /* chosen PCG blocks per SM */
+    float node_ms[3];           /* per candidate 64 / 128 / 256 threads; < 0 = not offered */
+    float pair_ms[3];
+    float pcg_ms[8];            /* per candidate 1..8 blocks per SM; < 0 = not offered */
+} ws_tuning;
+int ws_autotune(ws_solver *solver, int pcg_iters, void *stream, ws_tuning *result);
+/* Applies a tuning (e.g. one stored from an earlier ws_autotune on the same workload). */
+int ws_set_tuning(ws_solver *solver, const ws_tuning *tuning);
+
 /* Library version / build identification. */
 int ws_version(void);
 const char *ws_error_string(int status);

@@ -35,7 +35,8 @@ EXPORTED = [
     "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
     "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
     "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
-    "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv", "ws_spmv_matrix_free",
+    "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv", "ws_spmv_matrix_free", "ws_autotune",
+    "ws_set_tuning",
 ]
 
 
@@ -101,6 +102,13 @@ class WsServerStats(C.Structure):
     ]
 
 
+class WsTuning(C.Structure):
+    _fields_ = [
+        ("node_threads", C.c_int), ("pair_threads", C.c_int), ("pcg_blocks_per_sm", C.c_int),
+        ("node_ms", C.c_float * 3), ("pair_ms", C.c_float * 3), ("pcg_ms", C.c_float * 8),
+    ]
+
+
 class WarpSolveError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
@@ -162,6 +170,8 @@ def load() -> C.CDLL:
         "ws_server_get_stats": (i, [vp, C.POINTER(WsServerStats)]),
         "ws_spmv": (i, [vp, vp, vp, vp]),
         "ws_spmv_matrix_free": (i, [vp, vp, vp, vp]),
+        "ws_autotune": (i, [vp, i, vp, C.POINTER(WsTuning)]),
+        "ws_set_tuning": (i, [vp, C.POINTER(WsTuning)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

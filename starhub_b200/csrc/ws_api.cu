@@ -562,6 +562,95 @@ int ws_spmv_matrix_free(ws_solver *h, const float *x, float *y, void *stream) {
                : WS_ERR_CUDA;
 }
 
+static void drop_graph(ws::Workspace &w) {
+    if (w.graph_exec) cudaGraphExecDestroy(w.graph_exec);
+    w.graph_exec = nullptr;
+}
+
+int ws_set_tuning(ws_solver *h, const ws_tuning *t) {
+    if (!h || !t) return WS_ERR_INVALID_ARGUMENT;
+    auto ok_nt = [](int v) { return v == 64 || v == 128 || v == 256; };
+    if (!ok_nt(t->node_threads) || !ok_nt(t->pair_threads) || t->pcg_blocks_per_sm < 1) return WS_ERR_INVALID_ARGUMENT;
+    ws::Workspace &w = h->w;
+    w.tune.node_threads = t->node_threads;
+    w.tune.pair_threads = t->pair_threads;
+    w.tune.pcg_blocks_per_sm = t->pcg_blocks_per_sm;
+    w.tune.tuned = true;
+    drop_graph(w);
+    return WS_OK;
+}
+
+int ws_autotune(ws_solver *h, int pcg_iters, void *stream, ws_tuning *out) {
+    if (!h || !out || pcg_iters < 1) return WS_ERR_INVALID_ARGUMENT;
+    ws::Workspace &w = h->w;
+    if (w.num_scenes <= 0) return WS_ERR_NOT_READY;
+    cudaSetDevice(w.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    std::memset(out, 0, sizeof(*out));
+    for (float &x : out->node_ms) x = -1.f;
+    for (float &x : out->pair_ms) x = -1.f;
+    for (float &x : out->pcg_ms) x = -1.f;
+    if (w.tables_in_flight) cudaEventSynchronize(w.tables_free);
+    // one Gauss-Newton iteration gives real records and a real matrix to time on
+    if (enqueue_solve(w, 1, pcg_iters, st) != cudaSuccess) return WS_ERR_CUDA;
+    ws::gn_eval(w, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto time_ms = [&](auto &&run) {
+        run();   // warm-up
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, st);
+            run();
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            best = std::min(best, ms);
+        }
+        return best;
+    };
+    const int nts[3] = {64, 128, 256};
+    const bool fp64 = w.precision == WS_PREC_MIXED;
+    int best_node = 128, best_pair = 128;
+    float bn = 1e30f, bp = 1e30f;
+    for (int i = 0; i < 3; ++i) {
+        if (!(fp64 && nts[i] == 256)) {
+            w.tune.node_threads = nts[i];
+            out->node_ms[i] = time_ms([&] { ws::gn_assemble_node(w, st); });
+            if (out->node_ms[i] < bn) { bn = out->node_ms[i]; best_node = nts[i]; }
+        }
+        w.tune.pair_threads = nts[i];
+        out->pair_ms[i] = time_ms([&] { ws::gn_assemble_pair(w, st); });
+        if (out->pair_ms[i] < bp) { bp = out->pair_ms[i]; best_pair = nts[i]; }
+    }
+    w.tune.node_threads = best_node;
+    w.tune.pair_threads = best_pair;
+    ws::gn_assemble_node(w, st);
+    ws::gn_assemble_pair(w, st);
+    const int max_per_sm = std::max(1, std::min(8, w.pcg_grid / std::max(1, w.num_sms)));
+    int best_b = max_per_sm;
+    float bb = 1e30f;
+    for (int b = 1; b <= max_per_sm; ++b) {
+        w.tune.pcg_blocks_per_sm = b;
+        ws::pcg_ranges(w, st);
+        out->pcg_ms[b - 1] = time_ms([&] { ws::gn_pcg(w, pcg_iters, st); });
+        if (out->pcg_ms[b - 1] < bb) { bb = out->pcg_ms[b - 1]; best_b = b; }
+    }
+    w.tune.pcg_blocks_per_sm = best_b;
+    w.tune.tuned = true;
+    ws::pcg_ranges(w, st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    drop_graph(w);
+    out->node_threads = best_node;
+    out->pair_threads = best_pair;
+    out->pcg_blocks_per_sm = best_b;
+    const int status = ws_sync_status(h);
+    return status != WS_OK ? status : (cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA);
+}
+
 int ws_get_solution(ws_solver *h, int scene, const float **dev, int *num_nodes) {
     if (!h || !dev || !num_nodes) return WS_ERR_INVALID_ARGUMENT;
     ws::Workspace &w = h->w;

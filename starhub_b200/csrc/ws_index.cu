@@ -480,10 +480,16 @@ void index_build(Workspace &w, cudaStream_t st) {
                                                                     w.error_flag);
     k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.node_scene, N, w.cap_blocks, w.colidx,
                                                              w.entry_ref, w.entry_info, w.error_flag);
+    count_launch(w, 2);
+    pcg_ranges(w, st);
+}
+
+void pcg_ranges(Workspace &w, cudaStream_t st) {
     const uint32_t warps = (uint32_t)(pcg_launch_blocks(w) * pcg_warps_per_block());
-    k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.chunk_row, w.total_chunks, N,
-                                                                      w.cap_blocks, warps, w.pcg_warp_groups);
-    count_launch(w, 3);
+    k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.chunk_row, w.total_chunks,
+                                                                      w.total_nodes, w.cap_blocks, warps,
+                                                                      w.pcg_warp_groups);
+    count_launch(w);
 }
 
 }  // namespace ws

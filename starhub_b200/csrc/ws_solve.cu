@@ -408,8 +408,10 @@ __device__ __forceinline__ void accumulate_row(DAcc *D, DAcc *B, const float *ro
     }
 }
 
-template <class DAcc>
-__global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_node(const Scene *scenes, const Plan *plan,
+// NT (threads per block) is chosen by the autotuner among 64, 128 and 256; the work of a
+// warp, and so every sum, is the same for all three.
+template <class DAcc, int NT>
+__global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *scenes, const Plan *plan,
                                                                      const uint32_t *node_scene, uint32_t total_nodes,
                                                                      const uint32_t *n2t_offset, const uint32_t *n2t_val,
                                                                      const float *drec, const float *rrec,
@@ -419,7 +421,7 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_node(const Sce
     constexpr bool kCentred = sizeof(DAcc) == 8;   // mixed precision also uses node-centred twists
     constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;
     static_assert(27 * sizeof(DAcc) <= 4 * kSlot, "a slot holds one lane's 27 partial sums");
-    __shared__ __align__(16) float stage[kAssembleThreads / 32][32 * kSlot];
+    __shared__ __align__(16) float stage[NT / 32][32 * kSlot];
     const int lane = threadIdx.x & 31;
     float *slots = stage[threadIdx.x >> 5];
     float *mine = slots + lane * kSlot;
@@ -594,14 +596,15 @@ __device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, c
         for (int j = 0; j < 6; ++j) A[6 * i + j] += a[i] * c[j];
 }
 
-__global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble_pair(
+template <int NT>
+__global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
     const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
     const float4 *centers, int centred, float *pair_blocks) {
     constexpr int kSlot = kSlotWordsF32;
     static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
-    __shared__ __align__(16) float stage[kAssembleThreads / 32][32 * kSlot];
+    __shared__ __align__(16) float stage[NT / 32][32 * kSlot];
     const int lane = threadIdx.x & 31;
     float *slots = stage[threadIdx.x >> 5];
     float *mine = slots + lane * kSlot;
@@ -1458,7 +1461,8 @@ __global__ void __launch_bounds__(128) k_mf_gather(const Scene *scenes, const Pl
 // One warp per row group when that fits, else every co-resident block.
 int pcg_launch_blocks(const Workspace &w) {
     const uint32_t want = (w.total_chunks + (kPcgThreads / 32) - 1) / (kPcgThreads / 32);
-    return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, (uint32_t)w.pcg_grid));
+    const uint32_t cap = (uint32_t)std::min(w.pcg_grid, std::max(1, w.tune.pcg_blocks_per_sm) * w.num_sms);
+    return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, cap));
 }
 int pcg_warps_per_block() { return kPcgThreads / 32; }
 
@@ -1496,27 +1500,47 @@ void gn_eval(Workspace &w, cudaStream_t st) {
     }
 }
 
+template <class DAcc, int NT>
+static void launch_assemble_node(Workspace &w, cudaStream_t st) {
+    k_assemble_node<DAcc, NT><<<grid_for(w.total_nodes * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
+        w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
+        w.centers, w.diag_blocks, w.diag64, w.jtr, w.error_flag);
+}
+
+// 256 threads of the FP64 node kernel would need 60 KB of static shared memory, so that
+// shape is offered for the FP32 kernel only.
+template <class DAcc>
+static void launch_assemble_node_nt(Workspace &w, int nt, cudaStream_t st) {
+    if (nt == 64) {
+        launch_assemble_node<DAcc, 64>(w, st);
+    } else if (nt == 256) {
+        if constexpr (sizeof(DAcc) == 4) launch_assemble_node<DAcc, 256>(w, st);
+        else launch_assemble_node<DAcc, 128>(w, st);
+    } else {
+        launch_assemble_node<DAcc, 128>(w, st);
+    }
+}
+
 void gn_assemble_node(Workspace &w, cudaStream_t st) {
-    const int ng = grid_for(w.total_nodes * 32u, kAssembleThreads, w.num_sms, 32);
-    if (w.precision == WS_PREC_FP32)
-        k_assemble_node<float><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes,
-                                                                 w.n2t_offset, w.n2t_sorted_val, w.d_record,
-                                                                 w.r_record, w.se3, w.centers, w.diag_blocks,
-                                                                 w.diag64, w.jtr, w.error_flag);
-    else
-        k_assemble_node<double><<<ng, kAssembleThreads, 0, st>>>(w.scenes, w.plan, w.node_scene, w.total_nodes,
-                                                                  w.n2t_offset, w.n2t_sorted_val, w.d_record,
-                                                                  w.r_record, w.se3, w.centers, w.diag_blocks,
-                                                                  w.diag64, w.jtr, w.error_flag);
+    if (w.precision == WS_PREC_FP32) launch_assemble_node_nt<float>(w, w.tune.node_threads, st);
+    else launch_assemble_node_nt<double>(w, w.tune.node_threads, st);
     count_launch(w);
     k_block_inverse<<<grid_for(w.total_nodes, 128, w.num_sms, 16), 128, 0, st>>>(
         w.diag64, w.diag_blocks, w.total_nodes, w.precision == WS_PREC_MIXED ? 1 : 0, w.inv_diag);
     count_launch(w);
 }
-void gn_assemble_pair(Workspace &w, cudaStream_t st) {
-    k_assemble_pair<<<grid_for(w.cap_half * 32u, kAssembleThreads, w.num_sms, 32), kAssembleThreads, 0, st>>>(
+
+template <int NT>
+static void launch_assemble_pair(Workspace &w, cudaStream_t st) {
+    k_assemble_pair<NT><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
         w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.pair_blocks);
+}
+
+void gn_assemble_pair(Workspace &w, cudaStream_t st) {
+    if (w.tune.pair_threads == 64) launch_assemble_pair<64>(w, st);
+    else if (w.tune.pair_threads == 256) launch_assemble_pair<256>(w, st);
+    else launch_assemble_pair<128>(w, st);
     count_launch(w);
 }
 

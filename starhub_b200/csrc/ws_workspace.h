@@ -22,6 +22,13 @@ struct Workspace {
     int device = 0;
     int num_sms = 0;
     int pcg_grid = 0;           // co-resident blocks for the persistent PCG kernel
+    // launch shapes picked by ws_autotune (defaults until then); none of them changes a result
+    struct Tuning {
+        int node_threads = 128;     // threads per block of the node assembly (64, 128, 256)
+        int pair_threads = 128;     // threads per block of the pair assembly
+        int pcg_blocks_per_sm = 64; // upper bound on PCG blocks per SM (capped by co-residency)
+        bool tuned = false;
+    } tune;
 
     // current batch (host mirror)
     int num_scenes = 0;
@@ -140,6 +147,7 @@ void init_warp(Workspace &w, cudaStream_t st);
 // Occupancy of the persistent PCG kernel.
 int pcg_max_blocks(int device);
 int pcg_launch_blocks(const Workspace &w);
+void pcg_ranges(Workspace &w, cudaStream_t st);
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st);
 cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *ux_dense, float *ux_reg,
                                 cudaStream_t st);

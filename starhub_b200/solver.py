@@ -218,6 +218,21 @@ class WarpSolver:
         check(self._lib.ws_spmv_matrix_free(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                                             _stream_ptr(stream)), "ws_spmv_matrix_free")
 
+    def autotune(self, pcg_iters: int = 20, stream=None) -> dict:
+        """Times the launch-shape candidates on the inputs set and keeps the fastest (ws_autotune)."""
+        from ._lib import WsTuning
+        t = WsTuning()
+        check(self._lib.ws_autotune(self._h, pcg_iters, _stream_ptr(stream), C.byref(t)), "ws_autotune")
+        return {"node_threads": t.node_threads, "pair_threads": t.pair_threads,
+                "pcg_blocks_per_sm": t.pcg_blocks_per_sm, "node_ms": list(t.node_ms), "pair_ms": list(t.pair_ms),
+                "pcg_ms": list(t.pcg_ms)}
+
+    def set_tuning(self, node_threads: int, pair_threads: int, pcg_blocks_per_sm: int) -> None:
+        from ._lib import WsTuning
+        t = WsTuning()
+        t.node_threads, t.pair_threads, t.pcg_blocks_per_sm = node_threads, pair_threads, pcg_blocks_per_sm
+        check(self._lib.ws_set_tuning(self._h, C.byref(t)), "ws_set_tuning")
+
     # -- measurement ---------------------------------------------------------
     def set_profiling(self, enable: bool) -> None:
         check(self._lib.ws_set_profiling(self._h, 1 if enable else 0), "ws_set_profiling")
