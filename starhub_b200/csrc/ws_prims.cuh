@@ -68,17 +68,22 @@ static __global__ void k_scan_tile_sums(const uint32_t *in, const uint32_t *n_de
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-static __global__ void k_scan_tile_offsets(uint32_t *tile_sums, int num_tiles) {
+// Tiles past the live count hold zero sums; only the used ones are scanned, and the total
+// goes to tile_sums[num_tiles].
+static __global__ void k_scan_tile_offsets(uint32_t *tile_sums, int num_tiles, const uint32_t *n_dev,
+                                           uint32_t n_static) {
     __shared__ uint32_t sm[32];
     __shared__ uint32_t carry;
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    const int used = min(num_tiles, (int)(n / kScanTile) + 1);
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int base = 0; base < num_tiles; base += blockDim.x) {
+    for (int base = 0; base < used; base += blockDim.x) {
         const int i = base + threadIdx.x;
-        const uint32_t v = i < num_tiles ? tile_sums[i] : 0u;
+        const uint32_t v = i < used ? tile_sums[i] : 0u;
         uint32_t total;
         const uint32_t ex = block_excl_scan_u32(v, &total, sm);
-        if (i < num_tiles) tile_sums[i] = carry + ex;
+        if (i < used) tile_sums[i] = carry + ex;
         __syncthreads();
         if (threadIdx.x == 0) carry += total;
         __syncthreads();
@@ -115,7 +120,7 @@ inline void exclusive_scan(const uint32_t *in, uint32_t *out, const uint32_t *n_
                            uint32_t cap, uint32_t *tile_sums, cudaStream_t st) {
     const int tiles = (int)((cap + kScanTile) / kScanTile);
     k_scan_tile_sums<<<tiles, kScanThreads, 0, st>>>(in, n_dev, n_static, tile_sums);
-    k_scan_tile_offsets<<<1, 1024, 0, st>>>(tile_sums, tiles);
+    k_scan_tile_offsets<<<1, 1024, 0, st>>>(tile_sums, tiles, n_dev, n_static);
     k_scan_apply<<<tiles, kScanThreads, 0, st>>>(in, n_dev, n_static, tile_sums, tiles, out);
 }
 
@@ -142,22 +147,32 @@ __global__ void k_radix_upsweep(const K *keys, const uint32_t *n_dev, uint32_t n
     hist[(size_t)threadIdx.x * max_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-static __global__ void k_radix_scan(uint32_t *hist, int max_tiles, uint32_t *digit_total) {
+// Exclusive scan of one digit's tile counts (one block per digit) over the tiles in use,
+// 1024 consecutive counts per pass (4 per thread), with the running total carried along.
+static __global__ void k_radix_scan(uint32_t *hist, int max_tiles, const uint32_t *n_dev, uint32_t n_static,
+                                    uint32_t *digit_total) {
     __shared__ uint32_t sm[32];
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    const int used = min(max_tiles, (int)((n + kSortTile - 1) / kSortTile));
     uint32_t *row = hist + (size_t)blockIdx.x * max_tiles;
-    const int per = (max_tiles + blockDim.x - 1) / blockDim.x;
-    const int b = threadIdx.x * per;
-    const int e = min(b + per, max_tiles);
-    uint32_t local = 0;
-    for (int i = b; i < e; ++i) local += row[i];
-    uint32_t total;
-    uint32_t run = block_excl_scan_u32(local, &total, sm);
-    for (int i = b; i < e; ++i) {
-        const uint32_t v = row[i];
-        row[i] = run;
-        run += v;
+    uint32_t carry = 0;
+    for (int base = 0; base < used; base += 4 * (int)blockDim.x) {
+        const int i0 = base + 4 * (int)threadIdx.x;
+        uint32_t v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = (i0 + k < used) ? row[i0 + k] : 0u;
+        const uint32_t local = v[0] + v[1] + v[2] + v[3];
+        uint32_t total;
+        uint32_t run = block_excl_scan_u32(local, &total, sm) + carry;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (i0 + k < used) row[i0 + k] = run;
+            run += v[k];
+        }
+        carry += total;
+        __syncthreads();   // sm is reused by the next pass's scan
     }
-    if (threadIdx.x == 0) digit_total[blockIdx.x] = total;
+    if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
 }
 
 template <class K>
@@ -228,7 +243,7 @@ inline bool radix_sort(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt,
         K *ko = in_alt ? keys : keys_alt;
         uint32_t *vo = in_alt ? vals : vals_alt;
         k_radix_upsweep<K><<<max_tiles, kSortThreads, 0, st>>>(ki, n_dev, n_static, shift, hist, max_tiles);
-        k_radix_scan<<<256, 256, 0, st>>>(hist, max_tiles, digit_total);
+        k_radix_scan<<<256, 256, 0, st>>>(hist, max_tiles, n_dev, n_static, digit_total);
         k_radix_scatter<K><<<max_tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_dev, n_static, shift, hist,
                                                                 max_tiles, digit_total);
         in_alt = !in_alt;
