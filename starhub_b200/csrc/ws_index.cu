@@ -152,44 +152,38 @@ __device__ __forceinline__ ushort4 clamp_knn(ushort4 k, const Scene &sc, int *er
     return k;
 }
 
-__device__ __forceinline__ int find_scene_n2t(const Plan *plan, int num_scenes, uint32_t i) {
-    int lo = 0, hi = num_scenes - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (plan[mid].n2t_base <= i) lo = mid; else hi = mid - 1;
+
+// Node->term keys and values (buildTermKeyValueKernel, examples/mono_star/opt/Node2TermsIndex.cu:6-76):
+// keys are global node ids, values are the scene-local term ids of the reference's term space
+// [dense | reg | node-motion | feature]; self edges get the invalid key.  Per scene the entries
+// sit at plan.n2t_base as [4 per dense term | 2 per edge | 1 per node | 4 per feature].  One
+// thread per dense term writes that term's 4 entries (its scene from the compaction), and
+// one block row per scene writes the scene's other entries, so no entry searches for its scene.
+__global__ void k_n2t_kv_dense(const Scene *scenes, const Plan *plan, const uint32_t *counts,
+                               const uint32_t *term_scene, const ushort4 *dense_knn, uint32_t *keys, uint32_t *vals) {
+    const uint32_t n = counts[kCntDense];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t s = term_scene[t];
+        const Plan &p = plan[s];
+        const uint32_t lt = t - p.dense_begin, base = p.n2t_base + 4u * lt, nb = scenes[s].node_base;
+        const ushort4 k4 = dense_knn[t];
+        keys[base] = nb + k4.x;
+        keys[base + 1] = nb + k4.y;
+        keys[base + 2] = nb + k4.z;
+        keys[base + 3] = nb + k4.w;
+        vals[base] = vals[base + 1] = vals[base + 2] = vals[base + 3] = lt;
     }
-    return lo;
-}
-__device__ __forceinline__ int find_scene_pair(const Plan *plan, int num_scenes, uint32_t i) {
-    int lo = 0, hi = num_scenes - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (plan[mid].pair_base <= i) lo = mid; else hi = mid - 1;
-    }
-    return lo;
 }
 
-// buildTermKeyValueKernel (examples/mono_star/opt/Node2TermsIndex.cu:6-76): keys are global
-// node ids, values are the scene-local term ids of the reference's term space
-// [dense | reg | node-motion | feature]; self edges get the invalid key.
-__global__ void k_n2t_kv(const Scene *scenes, const Plan *plan, int num_scenes, const uint32_t *counts,
-                         const ushort4 *dense_knn, uint32_t *keys, uint32_t *vals, uint32_t invalid_key, int *err) {
-    const uint32_t n = counts[kCntN2T];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int s = find_scene_n2t(plan, num_scenes, i);
-        const Scene &sc = scenes[s];
-        const Plan &p = plan[s];
-        uint32_t j = i - p.n2t_base;
-        const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
-        uint32_t key, val;
-        if (j < 4u * nd) {
-            const uint32_t t = j >> 2;
-            const ushort4 k4 = dense_knn[p.dense_begin + t];
-            const uint32_t slot = j & 3u;
-            const uint16_t id = slot == 0 ? k4.x : slot == 1 ? k4.y : slot == 2 ? k4.z : k4.w;
-            key = sc.node_base + id;
-            val = t;
-        } else if ((j -= 4u * nd) < 2u * ne) {
+__global__ void k_n2t_kv_tail(const Scene *scenes, const Plan *plan, uint32_t *keys, uint32_t *vals,
+                              uint32_t invalid_key, int *err) {
+    const Scene &sc = scenes[blockIdx.y];
+    const Plan &p = plan[blockIdx.y];
+    const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes, nf = sc.num_features;
+    const uint32_t len = 2u * ne + nn + 4u * nf, base = p.n2t_base + 4u * nd;
+    for (uint32_t j0 = blockIdx.x * blockDim.x + threadIdx.x; j0 < len; j0 += gridDim.x * blockDim.x) {
+        uint32_t j = j0, key, val;
+        if (j < 2u * ne) {
             const uint32_t e = j >> 1;
             uint16_t x, y;
             edge_ends(sc, e, x, y, err);
@@ -207,8 +201,8 @@ __global__ void k_n2t_kv(const Scene *scenes, const Plan *plan, int num_scenes, 
             key = sc.node_base + id;
             val = nd + ne + nn + f;
         }
-        keys[i] = key;
-        vals[i] = val;
+        keys[base + j0] = key;
+        vals[base + j0] = val;
     }
 }
 
@@ -243,23 +237,45 @@ __device__ __forceinline__ unsigned long long knn_pair_key(const ushort4 k4, uin
     return invalid;
 }
 
-__global__ void k_pair_kv(const Scene *scenes, const Plan *plan, int num_scenes, const uint32_t *counts,
-                          const ushort4 *dense_knn, unsigned long long *keys, uint32_t *vals, int bits,
-                          unsigned long long invalid, int *err) {
-    const uint32_t n = counts[kCntPairKV];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int s = find_scene_pair(plan, num_scenes, i);
-        const Scene &sc = scenes[s];
+// Pair keys and values.  Per scene the entries sit at plan.pair_base as [6 per dense term |
+// 1 per edge | 6 per feature].  The 6 keys of one dense term follow knn_pair_key: slot pairs
+// (i, j) with id_i < id_j, i then j ascending; fewer than 6 when ids repeat, the rest invalid.
+__global__ void k_pair_kv_dense(const Scene *scenes, const Plan *plan, const uint32_t *counts,
+                                const uint32_t *term_scene, const ushort4 *dense_knn, unsigned long long *keys,
+                                uint32_t *vals, int bits, unsigned long long invalid) {
+    const uint32_t n = counts[kCntDense];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t s = term_scene[t];
         const Plan &p = plan[s];
-        uint32_t j = i - p.pair_base;
-        const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
+        const uint32_t lt = t - p.dense_begin, base = p.pair_base + 6u * lt, nb = scenes[s].node_base;
+        const ushort4 k4 = dense_knn[t];
+        const uint16_t a[4] = {k4.x, k4.y, k4.z, k4.w};
+        unsigned long long out[6] = {invalid, invalid, invalid, invalid, invalid, invalid};
+        int q = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (a[i] < a[j] && q < 6) out[q++] = ((unsigned long long)(nb + a[i]) << bits) | (unsigned long long)(nb + a[j]);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            keys[base + k] = out[k];
+            vals[base + k] = lt;
+        }
+    }
+}
+
+__global__ void k_pair_kv_tail(const Scene *scenes, const Plan *plan, unsigned long long *keys, uint32_t *vals,
+                               int bits, unsigned long long invalid, int *err) {
+    const Scene &sc = scenes[blockIdx.y];
+    const Plan &p = plan[blockIdx.y];
+    const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes, nf = sc.num_features;
+    const uint32_t len = ne + 6u * nf, base = p.pair_base + 6u * nd;
+    for (uint32_t j0 = blockIdx.x * blockDim.x + threadIdx.x; j0 < len; j0 += gridDim.x * blockDim.x) {
+        uint32_t j = j0;
         unsigned long long key;
         uint32_t val;
-        if (j < 6u * nd) {
-            const uint32_t t = j / 6u;
-            key = knn_pair_key(dense_knn[p.dense_begin + t], j - 6u * t, sc.node_base, bits, invalid);
-            val = t;
-        } else if ((j -= 6u * nd) < ne) {
+        if (j < ne) {
             uint16_t x, y;
             edge_ends(sc, j, x, y, err);
             const uint32_t lo = min(x, y), hi = max(x, y);
@@ -272,10 +288,11 @@ __global__ void k_pair_kv(const Scene *scenes, const Plan *plan, int num_scenes,
             key = knn_pair_key(clamp_knn(sc.feature_knn[f], sc, err), j - 6u * f, sc.node_base, bits, invalid);
             val = nd + ne + nn + f;
         }
-        keys[i] = key;
-        vals[i] = val;
+        keys[base + j0] = key;
+        vals[base + j0] = val;
     }
 }
+
 
 // segmentNodePairKernel (NodePair2TermsIndex.cu:94-128): 1 at the first key of every unique pair;
 // also records the number of valid (non-invalid) keys.
@@ -433,8 +450,10 @@ void index_build(Workspace &w, cudaStream_t st) {
     count_launch(w, 2);
     // 2. node -> term
     const uint32_t n2t_invalid = (1u << w.node_bits) - 1u;
-    k_n2t_kv<<<grid_for(w.cap_n2t, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, S, w.counts, w.d_knn, w.n2t_key,
-                                                                    w.n2t_val, n2t_invalid, w.error_flag);
+    k_n2t_kv_dense<<<grid_for(w.cap_pixels, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, w.counts, w.d_scene,
+                                                                            w.d_knn, w.n2t_key, w.n2t_val);
+    k_n2t_kv_tail<<<dim3(16, S), 256, 0, st>>>(w.scenes, w.plan, w.n2t_key, w.n2t_val, n2t_invalid, w.error_flag);
+    count_launch(w);
     const bool n2t_alt = radix_sort<uint32_t>(w.n2t_key, w.n2t_val, w.n2t_key_alt, w.n2t_val_alt, w.counts + kCntN2T, 0,
                                               w.cap_n2t, w.node_bits, w.sort_hist, w.sort_digit, st);
     count_launch(w, 1 + 3 * ((w.node_bits + 7) / 8));
@@ -445,9 +464,12 @@ void index_build(Workspace &w, cudaStream_t st) {
     // 3. node pair -> term
     const int pbits = 2 * w.node_bits;
     const unsigned long long pinvalid = (pbits >= 64) ? ~0ull : ((1ull << pbits) - 1ull);
-    k_pair_kv<<<grid_for(w.cap_pair_kv, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, S, w.counts, w.d_knn,
-                                                                         w.pair_key, w.pair_val, w.node_bits, pinvalid,
-                                                                         w.error_flag);
+    k_pair_kv_dense<<<grid_for(w.cap_pixels, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, w.counts, w.d_scene,
+                                                                             w.d_knn, w.pair_key, w.pair_val,
+                                                                             w.node_bits, pinvalid);
+    k_pair_kv_tail<<<dim3(16, S), 256, 0, st>>>(w.scenes, w.plan, w.pair_key, w.pair_val, w.node_bits, pinvalid,
+                                                w.error_flag);
+    count_launch(w);
     const bool pair_alt = radix_sort<unsigned long long>(w.pair_key, w.pair_val, w.pair_key_alt, w.pair_val_alt,
                                                          w.counts + kCntPairKV, 0, w.cap_pair_kv, pbits, w.sort_hist,
                                                          w.sort_digit, st);
