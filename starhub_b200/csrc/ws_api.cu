@@ -36,7 +36,7 @@ void free_all(ws::Workspace &w) {
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
                     w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.mf_ux, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
-                    w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter, w.barrier,
+                    w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter,
                     w.error_flag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -196,16 +196,14 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.centers, w.cap_nodes));
     A(dalloc(&w.chunk_partial, w.cap_chunks));
     A(dalloc(&w.scene_scalars, 8ull * w.cap_scenes));
-    A(dalloc(&w.scene_counter, 2ull * w.cap_scenes));
-    A(dalloc(&w.barrier, 4));
+    A(dalloc(&w.scene_counter, 64ull * w.cap_scenes));
     A(dalloc(&w.error_flag, 4));
     w.h_tables_bytes = sizeof(ws::Scene) * w.cap_scenes + 4ull * (w.cap_tiles + w.cap_nodes + w.cap_edges + 2ull * w.cap_chunks);
     A(cudaMallocHost(&w.h_tables, w.h_tables_bytes));
     A(cudaEventCreateWithFlags(&w.tables_free, cudaEventDisableTiming));
     if (e == cudaSuccess) {
         A(cudaMemset(w.error_flag, 0, 4 * sizeof(int)));
-        A(cudaMemset(w.barrier, 0, 4 * sizeof(uint32_t)));
-        A(cudaMemset(w.scene_counter, 0, 2ull * w.cap_scenes * sizeof(uint32_t)));
+        A(cudaMemset(w.scene_counter, 0, 64ull * w.cap_scenes * sizeof(uint32_t)));
         A(cudaMemset(w.se3, 0, (size_t)w.cap_nodes * 8 * sizeof(float)));
     }
     if (e == cudaSuccess) {

@@ -292,7 +292,6 @@ __device__ void cholesky6_fp64(const double *in, float *out) {
 // DAcc is the accumulator type: float for WS_PREC_FP32 (the reference's FP32 sums),
 // double for WS_PREC_MIXED, where D feeds the FP64 Cholesky directly.
 // ---------------------------------------------------------------------------
-constexpr int kAssembleThreads = 128;
 
 // Per-warp staging: 32 slots, one per list entry of the current batch.  A slot holds the
 // term's record (dense 128 B, regularisation 64 B) and, after the list, the lane's partial
@@ -733,8 +732,9 @@ struct PcgArgs {
     float *sd0, *sd1;         // [node][16]: s (6, padded to 8) then d (6, padded); swapped every iteration
     double *group_partial;
     double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
-    uint32_t *scene_counter;  // per scene: [0] phase A, [1] phase B / init
-    uint32_t *barrier;        // [0] arrive count, [1] generation
+    // per scene, kSceneSync words: [0] phase-A tickets, [1] phase-B / init tickets (arrivals of
+    // row groups), [32] alpha generation, [33] delta/beta generation (bumped when published)
+    uint32_t *scene_counter;
     uint32_t cap_blocks, cap_half, total_nodes, num_scenes;
     int *err;
     float *se3;
@@ -744,38 +744,8 @@ struct PcgArgs {
 };
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // requested sleep, about two seconds
+constexpr int kSceneSync = 64;        // words per scene in scene_counter (tickets and generations on separate lines)
 
-__device__ __forceinline__ bool grid_barrier(uint32_t *bar, int *err) {
-    __syncthreads();
-    __shared__ int ok;
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile uint32_t *gen = bar + 1;
-        const uint32_t my_gen = *gen;
-        __threadfence();
-        const uint32_t arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            // exponential backoff keeps the polling of early arrivals from loading the L2 slice
-            // that holds the barrier word while other blocks are still working
-            unsigned long long waited_ns = 0;
-            unsigned sleep_ns = 64;
-            while (*gen == my_gen) {
-                if (waited_ns > kBarrierTimeoutNs) { set_err(err, WS_ERR_TIMEOUT); ok = 0; break; }
-                __nanosleep(sleep_ns);
-                waited_ns += sleep_ns;
-                sleep_ns = min(sleep_ns * 2u, 256u);
-            }
-        }
-        __threadfence();
-        if (*reinterpret_cast<volatile int *>(err) == WS_ERR_TIMEOUT) ok = 0;
-    }
-    __syncthreads();
-    return ok != 0;
-}
 
 __device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
@@ -811,12 +781,47 @@ __device__ __forceinline__ void reduce_scene(const PcgArgs &A, uint32_t scene, i
         }
         S[3] = v;
         __threadfence();
+        // every group of the scene has finished the phase and its scalar is written
+        atomicAdd(&A.scene_counter[kSceneSync * scene + 32 + (mode == 0 ? 0 : 1)], 1u);
     }
+}
+
+// Waits until every scene that owns one of the warp's groups has published generation
+// `target` of `which` (0: alpha, 1: delta and beta).  Lanes that start a run of a new
+// scene wait for that scene; the wait sleeps with backoff and gives up after about two
+// seconds of requested sleep (or at once when another warp has already timed out).
+__device__ bool wait_scenes(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, int which, uint32_t target,
+                            int lane) {
+    bool ok = true;
+    for (uint32_t base = g_begin; base < g_end; base += 32) {
+        const uint32_t g = base + lane;
+        const uint32_t sc = g < g_end ? A.group_scene[g] : kInvalidIndex;
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, sc, 1);
+        if (g < g_end && (lane == 0 || prev != sc)) {
+            const volatile uint32_t *gen = A.scene_counter + (size_t)kSceneSync * sc + 32 + which;
+            unsigned long long waited_ns = 0;
+            unsigned sleep_ns = 32;
+            while (*gen < target) {
+                if (waited_ns > kBarrierTimeoutNs || *reinterpret_cast<volatile int *>(A.err) == WS_ERR_TIMEOUT) {
+                    set_err(A.err, WS_ERR_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                __nanosleep(sleep_ns);
+                waited_ns += sleep_ns;
+                sleep_ns = min(sleep_ns * 2u, 256u);
+            }
+        }
+        __syncwarp();
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    __threadfence();   // reads of the scenes' vectors and scalars come after the generation
+    return ok;
 }
 
 __device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, int mode, int lane) {
     if (g_begin >= g_end) return;
-    if (lane == 0) __threadfence();   // this warp's group partials (written by lanes 0 and 16) first
+    __threadfence();   // every lane's vector and partial writes of the phase before the tickets
     __syncwarp();
     const uint32_t ctr = (mode == 0) ? 0u : 1u;
     for (uint32_t base = g_begin; base < g_end; base += 32) {
@@ -833,10 +838,10 @@ __device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end
             int last = 0;
             if (lane == 0) {
                 const uint32_t n = (uint32_t)(s1 - s0);
-                const uint32_t ticket = atomicAdd(&A.scene_counter[2 * scene + ctr], n);
+                const uint32_t ticket = atomicAdd(&A.scene_counter[kSceneSync * scene + ctr], n);
                 last = (ticket + n == (uint32_t)A.scenes[scene].num_chunks) ? 1 : 0;
                 if (last) {
-                    atomicExch(&A.scene_counter[2 * scene + ctr], 0u);
+                    atomicExch(&A.scene_counter[kSceneSync * scene + ctr], 0u);
                     __threadfence();
                 }
             }
@@ -1169,7 +1174,6 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     extern __shared__ __align__(16) float pcg_smem[];
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
     // this warp's contiguous range of row groups (balanced by slot count) and their rows
     const uint32_t g_begin = min(A.warp_groups[gwarp], A.total_groups);
@@ -1194,7 +1198,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
     }
     publish_range(A, g_begin, g_end, 2, lane);
-    if (!grid_barrier(A.barrier, A.err)) return;
+    if (!wait_scenes(A, g_begin, g_end, 1, 1u, lane)) return;
 
     for (int it = 0; it < A.pcg_iters; ++it) {
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
@@ -1202,7 +1206,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
         stream_rows<true>(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
         publish_range(A, g_begin, g_end, 0, lane);
-        if (!grid_barrier(A.barrier, A.err)) return;
+        if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
         for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
             const NodeStep n = node_step(A, g, g_end, lane);
@@ -1228,7 +1232,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
             if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
         }
         publish_range(A, g_begin, g_end, 1, lane);
-        if (!grid_barrier(A.barrier, A.err)) return;
+        if (it + 1 < A.pcg_iters && !wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 2u, lane)) return;
     }
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
     //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
@@ -1563,7 +1567,6 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.group_partial = w.chunk_partial;
     a.scalars = w.scene_scalars;
     a.scene_counter = w.scene_counter;
-    a.barrier = w.barrier;
     a.cap_blocks = w.cap_blocks;
     a.cap_half = std::max<uint32_t>(1u, w.cap_half);
     a.num_scenes = (uint32_t)std::max(1, w.num_scenes);
@@ -1579,9 +1582,9 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
 cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     PcgArgs a = pcg_args(w, pcg_iters);
     const int grid = pcg_launch_blocks(w);
-    // a barrier or counter left half-way by an earlier timed-out launch must not leak into this one
-    cudaMemsetAsync(w.barrier, 0, 4 * sizeof(uint32_t), st);
-    cudaMemsetAsync(w.scene_counter, 0, 2 * sizeof(uint32_t) * (size_t)w.num_scenes, st);
+    // tickets and generations start at zero every launch, so a launch that timed out half-way
+    // cannot leak into the next
+    cudaMemsetAsync(w.scene_counter, 0, sizeof(uint32_t) * kSceneSync * (size_t)w.num_scenes, st);
     void *args[] = {&a};
     count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);

@@ -105,8 +105,7 @@ struct Workspace {
     float4 *centers = nullptr;          // [cap_nodes] twist centre per node (current GN iteration)
     double *chunk_partial = nullptr;    // [cap_chunks]
     double *scene_scalars = nullptr;    // [cap_scenes * 8]: delta, alpha, beta, dq ...
-    uint32_t *scene_counter = nullptr;  // [cap_scenes * 2]
-    uint32_t *barrier = nullptr;        // [4] count, generation
+    uint32_t *scene_counter = nullptr;  // [cap_scenes * 64]: PCG tickets and generations per scene
     int *error_flag = nullptr;          // [4]
 
     // pinned host staging of the scene tables (uploaded at the start of every solve)
