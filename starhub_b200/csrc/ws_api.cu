@@ -322,6 +322,9 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
     }
     w.h_scenes.assign(hs, hs + num_scenes);
     w.num_scenes = num_scenes;
+    w.dense_channels = 1;
+    for (int s = 0; s < num_scenes; ++s)
+        if (hs[s].lam_of != 0.0f) w.dense_channels = 3;
     w.total_nodes = nb;
     w.total_edges = eb;
     w.total_features = fb;
@@ -436,8 +439,10 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
     if (!st) return WS_ERR_INVALID_ARGUMENT;   // the legacy stream cannot be captured
     w.last_stream = st;
     const uint64_t key[] = {(uint64_t)gn_iters, (uint64_t)pcg_iters, (uint64_t)w.num_scenes, w.total_nodes,
-                            w.total_edges, w.total_tiles, w.total_chunks, (uint64_t)w.node_bits};
-    bool same = w.graph_exec && w.graph_key.size() == 8 && std::equal(key, key + 8, w.graph_key.begin());
+                            w.total_edges, w.total_tiles, w.total_chunks, (uint64_t)w.node_bits,
+                            (uint64_t)w.dense_channels};
+    constexpr size_t kKey = sizeof(key) / sizeof(key[0]);
+    bool same = w.graph_exec && w.graph_key.size() == kKey && std::equal(key, key + kKey, w.graph_key.begin());
     if (same) {
         // device pointers of the inputs live in the uploaded tables, so a replay picks up new inputs;
         // the initial-warp copies are graph nodes with fixed sources, so they must match too
@@ -474,7 +479,7 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
             cudaGetLastError();
             return WS_ERR_CUDA;
         }
-        w.graph_key.assign(key, key + 8);
+        w.graph_key.assign(key, key + kKey);
         w.graph_init = w.init_ptrs;
     }
     if (cudaGraphLaunch(w.graph_exec, st) != cudaSuccess) return WS_ERR_CUDA;
@@ -743,11 +748,21 @@ int ws_get_dense_jacobian(ws_solver *h, int scene, float *residual, float *gradi
     plan_of(w, scene, p);
     *count = (int)p.dense_count;
     if ((int)p.dense_count > cap) return WS_ERR_CAPACITY;
-    const auto rec = download(w.d_record + (size_t)ws::kDenseRecord * p.dense_begin, (size_t)ws::kDenseRecord * p.dense_count);
+    // records of a batch without the flow term hold the depth channel only; the flow
+    // channels read back as zero
+    const int ch = w.dense_channels;
+    const size_t stride = ch == 3 ? ws::DenseLayout<3>::kFloats : ws::DenseLayout<1>::kFloats;
+    const auto rec = download(w.d_record + stride * p.dense_begin, stride * p.dense_count);
     for (uint32_t t = 0; t < p.dense_count; ++t) {
-        const float *r = rec.data() + (size_t)ws::kDenseRecord * t;
-        if (gradient) std::memcpy(gradient + 18ull * t, r, 18 * sizeof(float));
-        if (residual) std::memcpy(residual + 3ull * t, r + 18, 3 * sizeof(float));
+        const float *r = rec.data() + stride * t;
+        if (gradient) {
+            std::memset(gradient + 18ull * t, 0, 18 * sizeof(float));
+            std::memcpy(gradient + 18ull * t, r, 6ull * ch * sizeof(float));
+        }
+        if (residual) {
+            std::memset(residual + 3ull * t, 0, 3 * sizeof(float));
+            std::memcpy(residual + 3ull * t, r + 6 * ch, (size_t)ch * sizeof(float));
+        }
     }
     return WS_OK;
 }

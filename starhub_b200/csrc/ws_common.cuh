@@ -16,11 +16,26 @@
 namespace ws {
 
 constexpr int kVecStride = 8;        // floats per node in PCG vectors
-constexpr int kDenseRecord = 32;     // floats per dense-term record (128 B)
+constexpr int kDenseRecord = 32;     // floats per dense-term record, largest layout (128 B)
 constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
 constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group (divides 32)
 constexpr uint32_t kRefTransposed = 0x80000000u;   // entry_ref flag: lower-triangle use of a pair block
+
+// Dense-term record layouts, chosen per batch.  With the optical-flow term (some scene of the
+// batch has lambda_of != 0) a record holds C = 3 channels in 128 B: gradients 0..17 (three
+// channels of [rotation | translation]), residuals 18..20, skinning weights 22..25, global
+// node ids 26..29.  Without it only the depth channel is kept, C = 1, in 64 B: gradient 0..5,
+// residual 6, weights 8..11, node ids 12..15.  A scene with lambda_of = 0 gets bit-identical
+// sums either way: its flow rows are scaled by zero and add exact zeros.
+template <int C>
+struct DenseLayout {
+    static_assert(C == 1 || C == 3, "one or three channels");
+    static constexpr int kFloats = C == 3 ? 32 : 16;
+    static constexpr int kRes = 6 * C;
+    static constexpr int kW = C == 3 ? 22 : 8;
+    static constexpr int kIds = kW + 4;
+};
 
 // ---------------------------------------------------------------------------
 // Per-scene descriptor, device resident.  Filled on the host from ws_inputs.

@@ -200,7 +200,8 @@ __global__ void k_forward_warp(const float *se3, int num_nodes, const float4 *ve
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const ushort4 k4 = knn[i];
         const float4 s4 = sw[i], c4 = cw[i];
-        const uint16_t ids[4] = {min(k4.x, last), min(k4.y, last), min(k4.z, last), min(k4.w, last)};
+        const uint16_t ids[4] = {(uint16_t)min(k4.x, last), (uint16_t)min(k4.y, last), (uint16_t)min(k4.z, last),
+                                 (uint16_t)min(k4.w, last)};
         const float wv[4] = {s4.x * c4.x, s4.y * c4.y, s4.z * c4.z, s4.w * c4.w};
         DQf avg;
         avg.q0 = make_float4(0.f, 0.f, 0.f, 0.f);

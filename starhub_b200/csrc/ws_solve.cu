@@ -39,10 +39,11 @@ __global__ void k_copy_init_warp(const float *init, uint32_t node_base, uint32_t
 // ---------------------------------------------------------------------------
 // Dense depth + optical-flow term (computeDenseImageJacobianKernel,
 // examples/mono_star/opt/DenseImageJacobianResidual.cu:164-308, with :12-25 and :77-115).
-// One thread per compacted term; writes a 128-byte record:
-//   [0,18) gradient (3 channels x [rotation | translation]), [18,21) residual,
-//   [22,26) knn weights (spatial * connect), [26,30) global knn node ids.
+// One thread per compacted term; writes one record in the batch's layout (DenseLayout<C>):
+// the gradients and residuals of the depth channel (and of the two flow channels when C = 3),
+// the knn weights (spatial * connect) and the global knn node ids.
 // ---------------------------------------------------------------------------
+template <int C>
 __global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const uint32_t *counts,
                                                      const ushort4 *pixels, const ushort4 *knn, const float4 *sw,
                                                      const float4 *cw, const uint32_t *term_scene, const float *se3,
@@ -107,7 +108,7 @@ __global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const u
                 const float3 row0 = f3(W.m[0][0], W.m[0][1], W.m[0][2]);
                 const float3 row1 = f3(W.m[1][0], W.m[1][1], W.m[1][2]);
                 const float ex = dot3(row0, diff), ey = dot3(row1, diff);
-                if (!(sqrtf(ex * ex + ey * ey) < 1e-6f)) {
+                if (C == 3 && !(sqrtf(ex * ex + ey * ey) < 1e-6f)) {
                     res[1] = ex;
                     res[2] = ey;
                     const float3 mv = f3(-vw.x, -vw.y, -vw.z);
@@ -122,15 +123,23 @@ __global__ void __launch_bounds__(256) k_eval_dense(const Scene *scenes, const u
                 }
             }
         }
-        float4 *out = reinterpret_cast<float4 *>(record + (size_t)kDenseRecord * t);
-        out[0] = make_float4(gr[0], gr[1], gr[2], gr[3]);
-        out[1] = make_float4(gr[4], gr[5], gr[6], gr[7]);
-        out[2] = make_float4(gr[8], gr[9], gr[10], gr[11]);
-        out[3] = make_float4(gr[12], gr[13], gr[14], gr[15]);
-        out[4] = make_float4(gr[16], gr[17], res[0], res[1]);
-        out[5] = make_float4(res[2], 0.f, w[0], w[1]);
-        out[6] = make_float4(w[2], w[3], __uint_as_float(g[0]), __uint_as_float(g[1]));
-        out[7] = make_float4(__uint_as_float(g[2]), __uint_as_float(g[3]), 0.f, 0.f);
+        float4 *out = reinterpret_cast<float4 *>(record + (size_t)DenseLayout<C>::kFloats * t);
+        if constexpr (C == 3) {
+            out[0] = make_float4(gr[0], gr[1], gr[2], gr[3]);
+            out[1] = make_float4(gr[4], gr[5], gr[6], gr[7]);
+            out[2] = make_float4(gr[8], gr[9], gr[10], gr[11]);
+            out[3] = make_float4(gr[12], gr[13], gr[14], gr[15]);
+            out[4] = make_float4(gr[16], gr[17], res[0], res[1]);
+            out[5] = make_float4(res[2], 0.f, w[0], w[1]);
+            out[6] = make_float4(w[2], w[3], __uint_as_float(g[0]), __uint_as_float(g[1]));
+            out[7] = make_float4(__uint_as_float(g[2]), __uint_as_float(g[3]), 0.f, 0.f);
+        } else {
+            out[0] = make_float4(gr[0], gr[1], gr[2], gr[3]);
+            out[1] = make_float4(gr[4], gr[5], res[0], 0.f);
+            out[2] = make_float4(w[0], w[1], w[2], w[3]);
+            out[3] = make_float4(__uint_as_float(g[0]), __uint_as_float(g[1]), __uint_as_float(g[2]),
+                                 __uint_as_float(g[3]));
+        }
     }
 }
 
@@ -300,15 +309,17 @@ constexpr int kSlotWordsF32 = 36;   // 144 B: a dense record, or 27 (node) / 36 
 constexpr int kSlotWordsF64 = 60;   // 240 B: a dense record, or 27 double partial sums
 
 // Copies the records of the warp's 32 terms into their slots.  Lane l names its record by
-// `src` (16-byte units) and `parts` (8 dense, 4 regularisation, 0 none); in pass j the lanes
-// of group l / 8 move record 4 j + l / 8, one 16-byte part each (cp.async, no registers), so
-// every pass reads four whole records on 128-byte lines.  The caller syncs the warp after.
-template <int kSlotWords>
+// `src` (16-byte units) and `parts` (at most kParts, 0 for none); kParts is 8 for 128-byte
+// and 4 for 64-byte dense records.  In pass j the kParts lanes of group q = l / kParts move
+// record j + q * kParts, one 16-byte part each (cp.async, no registers), so every pass reads
+// 32 / kParts whole records.  The caller syncs the warp after.
+template <int kSlotWords, int kParts = 8>
 __device__ __forceinline__ void fetch_records(float *slots, int lane, const float4 *src, int parts) {
-    const int part = lane & 7;
+    static_assert(kParts == 4 || kParts == 8, "64- or 128-byte records");
+    const int part = lane & (kParts - 1);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int r = 4 * j + (lane >> 3);
+    for (int j = 0; j < kParts; ++j) {
+        const int r = j + (lane / kParts) * kParts;
         const float4 *p = reinterpret_cast<const float4 *>(
             __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), r));
         const int np = __shfl_sync(0xffffffffu, parts, r);
@@ -320,21 +331,35 @@ __device__ __forceinline__ void fetch_records(float *slots, int lane, const floa
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Dense record fields (k_eval_dense): gradient rows 0..17 (three channels of 6), residuals
-// 18..20, skinning weights 22..25, node ids 26..29.
+// Dense record fields in the layout DenseLayout<C> (k_eval_dense).
+template <int C>
 __device__ __forceinline__ void read_weights(const float *slot, float *wk, uint32_t *ids) {
-    const float4 a = *reinterpret_cast<const float4 *>(slot + 20);
-    const float4 b = *reinterpret_cast<const float4 *>(slot + 24);
-    const float2 c = *reinterpret_cast<const float2 *>(slot + 28);
-    wk[0] = a.z;
-    wk[1] = a.w;
-    wk[2] = b.x;
-    wk[3] = b.y;
-    ids[0] = __float_as_uint(b.z);
-    ids[1] = __float_as_uint(b.w);
-    ids[2] = __float_as_uint(c.x);
-    ids[3] = __float_as_uint(c.y);
+    if constexpr (C == 3) {
+        const float4 a = *reinterpret_cast<const float4 *>(slot + 20);
+        const float4 b = *reinterpret_cast<const float4 *>(slot + 24);
+        const float2 c = *reinterpret_cast<const float2 *>(slot + 28);
+        wk[0] = a.z;
+        wk[1] = a.w;
+        wk[2] = b.x;
+        wk[3] = b.y;
+        ids[0] = __float_as_uint(b.z);
+        ids[1] = __float_as_uint(b.w);
+        ids[2] = __float_as_uint(c.x);
+        ids[3] = __float_as_uint(c.y);
+    } else {
+        const float4 a = *reinterpret_cast<const float4 *>(slot + 8);
+        const float4 b = *reinterpret_cast<const float4 *>(slot + 12);
+        wk[0] = a.x;
+        wk[1] = a.y;
+        wk[2] = a.z;
+        wk[3] = a.w;
+        ids[0] = __float_as_uint(b.x);
+        ids[1] = __float_as_uint(b.y);
+        ids[2] = __float_as_uint(b.z);
+        ids[3] = __float_as_uint(b.w);
+    }
 }
+template <int C>
 __device__ __forceinline__ float read_channel(const float *slot, int ch, float *g) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -342,7 +367,7 @@ __device__ __forceinline__ float read_channel(const float *slot, int ch, float *
         g[2 * q] = v.x;
         g[2 * q + 1] = v.y;
     }
-    return slot[18 + ch];
+    return slot[DenseLayout<C>::kRes + ch];
 }
 
 // Reads one record of `n4` 16-byte parts back from a slot.
@@ -409,7 +434,7 @@ __device__ __forceinline__ void accumulate_row(DAcc *D, DAcc *B, const float *ro
 
 // NT (threads per block) is chosen by the autotuner among 64, 128 and 256; the work of a
 // warp, and so every sum, is the same for all three.
-template <class DAcc, int NT>
+template <class DAcc, int NT, int C>
 __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *scenes, const Plan *plan,
                                                                      const uint32_t *node_scene, uint32_t total_nodes,
                                                                      const uint32_t *n2t_offset, const uint32_t *n2t_val,
@@ -434,7 +459,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
         const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
         const float lam_d = sc.lam_depth, lam_of = sc.lam_of, lam_r = sc.lam_reg, lam_n = sc.lam_node;
         const bool motion = lam_n != 0.f && sc.node_motion != nullptr;
-        const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * p.dense_begin);
+        const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)DenseLayout<C>::kFloats * p.dense_begin);
         const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
         const float4 c4 = centers[g];
         const float3 cen = f3(c4.x, c4.y, c4.z);
@@ -454,8 +479,8 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
             int parts = 0;
             if (term < nd) {
                 kind = 1;
-                src = dbase + (size_t)(kDenseRecord / 4) * term;
-                parts = kDenseRecord / 4;
+                src = dbase + (size_t)(DenseLayout<C>::kFloats / 4) * term;
+                parts = DenseLayout<C>::kFloats / 4;
             } else if (term < nd + ne) {
                 kind = 2;
                 src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
@@ -463,20 +488,20 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
             } else if (term < nd + ne + nn && motion) {
                 kind = 3;
             }
-            fetch_records<kSlot>(slots, lane, src, parts);
+            fetch_records<kSlot, C == 3 ? 8 : 4>(slots, lane, src, parts);
             __syncwarp();
             if (kind == 1) {
                 // point-to-plane + optical-flow rows (libs/star/opt/dense_image_jacobian.cuh:9-20)
                 float wk[4];
                 uint32_t ids[4];
-                read_weights(mine, wk, ids);
+                read_weights<C>(mine, wk, ids);
                 float w = wk[0];   // weight of the last slot whose node is g
 #pragma unroll
                 for (int k = 1; k < 4; ++k) if (ids[k] == g) w = wk[k];
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
+                for (int ch = 0; ch < C; ++ch) {
                     float gl[6];
-                    const float res = read_channel(mine, ch, gl);
+                    const float res = read_channel<C>(mine, ch, gl);
                     if (kCentred) recentre(gl, cen);
                     const float scale = (ch == 0 ? lam_d : lam_of) * w;
                     accumulate_row(D, B, gl, scale, -(scale * res));
@@ -595,7 +620,7 @@ __device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, c
         for (int j = 0; j < 6; ++j) A[6 * i + j] += a[i] * c[j];
 }
 
-template <int NT>
+template <int NT, int C>
 __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
@@ -617,7 +642,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges;
         const float lam_d = sc.lam_depth, lam_of = sc.lam_of, lam_r = sc.lam_reg;
-        const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)kDenseRecord * p.dense_begin);
+        const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)DenseLayout<C>::kFloats * p.dense_begin);
         const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
         const float4 cr4 = centers[row], cc4 = centers[col];
         const float3 c_row = f3(cr4.x, cr4.y, cr4.z), c_col = f3(cc4.x, cc4.y, cc4.z);
@@ -633,19 +658,19 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
             int parts = 0;
             if (term < nd) {
                 kind = 1;
-                src = dbase + (size_t)(kDenseRecord / 4) * term;
-                parts = kDenseRecord / 4;
+                src = dbase + (size_t)(DenseLayout<C>::kFloats / 4) * term;
+                parts = DenseLayout<C>::kFloats / 4;
             } else if (term < nd + ne) {
                 kind = 2;
                 src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
                 parts = kRegRecord / 4;
             }
-            fetch_records<kSlot>(slots, lane, src, parts);
+            fetch_records<kSlot, C == 3 ? 8 : 4>(slots, lane, src, parts);
             __syncwarp();
             if (kind == 1) {
                 float wk[4];
                 uint32_t ids[4];
-                read_weights(mine, wk, ids);
+                read_weights<C>(mine, wk, ids);
                 float wi = wk[0], wj = wk[0];   // last matching slots
 #pragma unroll
                 for (int k = 1; k < 4; ++k) {
@@ -653,9 +678,9 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
                     if (ids[k] == col) wj = wk[k];
                 }
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
+                for (int ch = 0; ch < C; ++ch) {
                     float gr[6], gc[6];
-                    read_channel(mine, ch, gr);
+                    read_channel<C>(mine, ch, gr);
 #pragma unroll
                     for (int q = 0; q < 6; ++q) gc[q] = gr[q];
                     if (centred) {
@@ -1303,23 +1328,25 @@ __global__ void __launch_bounds__(kPcgThreads, 8) k_spmv(PcgArgs A, const float 
 // y = sum over its terms of u_node (J x) in list order (one warp per node, fixed butterfly).
 // A term's four node ids are distinct (skinning picks distinct nodes).
 // ---------------------------------------------------------------------------
+template <int C>
 __global__ void k_mf_dense(const Scene *scenes, const uint32_t *counts, const uint32_t *term_scene,
                            const float *drec, const float4 *centers, int centred, const float *x, float *ux) {
+    using L = DenseLayout<C>;
     const uint32_t n = counts[kCntDense];
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const Scene &sc = scenes[term_scene[t]];
-        const float *rec = drec + (size_t)kDenseRecord * t;
+        const float *rec = drec + (size_t)L::kFloats * t;
         float u[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const uint32_t node = __float_as_uint(rec[26 + k]);
-            const float w = rec[22 + k];
+            const uint32_t node = __float_as_uint(rec[L::kIds + k]);
+            const float w = rec[L::kW + k];
             const float4 x0 = *reinterpret_cast<const float4 *>(x + 8ull * node);
             const float2 x1 = *reinterpret_cast<const float2 *>(x + 8ull * node + 4);
             const float xv[6] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y};
             const float4 c4 = centers[node];
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
+            for (int ch = 0; ch < C; ++ch) {
                 float gl[6];
 #pragma unroll
                 for (int q = 0; q < 6; ++q) gl[q] = rec[6 * ch + q];
@@ -1371,6 +1398,7 @@ __global__ void k_mf_reg(const Scene *scenes, const uint32_t *edge_scene, uint32
     }
 }
 
+template <int C>
 __global__ void __launch_bounds__(128) k_mf_gather(const Scene *scenes, const Plan *plan, const uint32_t *node_scene,
                                                    uint32_t total_nodes, const uint32_t *n2t_offset,
                                                    const uint32_t *n2t_val, const float *drec, const float *rrec,
@@ -1389,15 +1417,16 @@ __global__ void __launch_bounds__(128) k_mf_gather(const Scene *scenes, const Pl
         for (uint32_t it = n2t_offset[g] + lane; it < n2t_offset[g + 1]; it += 32) {
             const uint32_t term = n2t_val[it];
             if (term < nd) {
-                const float *rec = drec + (size_t)kDenseRecord * (p.dense_begin + term);
-                float w = rec[22];   // weight of the last slot whose node is g
+                using L = DenseLayout<C>;
+                const float *rec = drec + (size_t)L::kFloats * (p.dense_begin + term);
+                float w = rec[L::kW];   // weight of the last slot whose node is g
 #pragma unroll
-                for (int k = 1; k < 4; ++k) if (__float_as_uint(rec[26 + k]) == g) w = rec[22 + k];
+                for (int k = 1; k < 4; ++k) if (__float_as_uint(rec[L::kIds + k]) == g) w = rec[L::kW + k];
                 const float4 u = reinterpret_cast<const float4 *>(ux_dense)[p.dense_begin + term];
                 const float uu[3] = {u.x, u.y, u.z};
                 const float lam[3] = {sc.lam_depth, sc.lam_of, sc.lam_of};
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
+                for (int ch = 0; ch < C; ++ch) {
                     float gl[6];
 #pragma unroll
                     for (int q = 0; q < 6; ++q) gl[q] = rec[6 * ch + q];
@@ -1494,8 +1523,12 @@ void gn_eval(Workspace &w, cudaStream_t st) {
     k_node_centers<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.node_scene, w.total_nodes,
                                                                            w.se3, w.centers);
     count_launch(w);
-    k_eval_dense<<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
-        w.scenes, w.counts, w.d_pixels, w.d_knn, w.d_sw, w.d_cw, w.d_scene, w.se3, w.d_record);
+    if (w.dense_channels == 3)
+        k_eval_dense<3><<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
+            w.scenes, w.counts, w.d_pixels, w.d_knn, w.d_sw, w.d_cw, w.d_scene, w.se3, w.d_record);
+    else
+        k_eval_dense<1><<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
+            w.scenes, w.counts, w.d_pixels, w.d_knn, w.d_sw, w.d_cw, w.d_scene, w.se3, w.d_record);
     count_launch(w);
     if (w.total_edges > 0) {
         k_eval_reg<<<grid_for(w.total_edges, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.edge_scene, w.total_edges,
@@ -1504,11 +1537,17 @@ void gn_eval(Workspace &w, cudaStream_t st) {
     }
 }
 
-template <class DAcc, int NT>
-static void launch_assemble_node(Workspace &w, cudaStream_t st) {
-    k_assemble_node<DAcc, NT><<<grid_for(w.total_nodes * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
+template <class DAcc, int NT, int C>
+static void launch_assemble_node_c(Workspace &w, cudaStream_t st) {
+    k_assemble_node<DAcc, NT, C><<<grid_for(w.total_nodes * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
         w.centers, w.diag_blocks, w.diag64, w.jtr, w.error_flag);
+}
+
+template <class DAcc, int NT>
+static void launch_assemble_node(Workspace &w, cudaStream_t st) {
+    if (w.dense_channels == 3) launch_assemble_node_c<DAcc, NT, 3>(w, st);
+    else launch_assemble_node_c<DAcc, NT, 1>(w, st);
 }
 
 // 256 threads of the FP64 node kernel would need 60 KB of static shared memory, so that
@@ -1534,11 +1573,17 @@ void gn_assemble_node(Workspace &w, cudaStream_t st) {
     count_launch(w);
 }
 
-template <int NT>
-static void launch_assemble_pair(Workspace &w, cudaStream_t st) {
-    k_assemble_pair<NT><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
+template <int NT, int C>
+static void launch_assemble_pair_c(Workspace &w, cudaStream_t st) {
+    k_assemble_pair<NT, C><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
         w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.pair_blocks);
+}
+
+template <int NT>
+static void launch_assemble_pair(Workspace &w, cudaStream_t st) {
+    if (w.dense_channels == 3) launch_assemble_pair_c<NT, 3>(w, st);
+    else launch_assemble_pair_c<NT, 1>(w, st);
 }
 
 void gn_assemble_pair(Workspace &w, cudaStream_t st) {
@@ -1593,12 +1638,17 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
 cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *ux_dense, float *ux_reg,
                                 cudaStream_t st) {
     const int centred = w.precision == WS_PREC_MIXED ? 1 : 0;
-    k_mf_dense<<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(w.scenes, w.counts, w.d_scene, w.d_record,
-                                                                          w.centers, centred, x, ux_dense);
+    if (w.dense_channels == 3)
+        k_mf_dense<3><<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
+            w.scenes, w.counts, w.d_scene, w.d_record, w.centers, centred, x, ux_dense);
+    else
+        k_mf_dense<1><<<grid_for(w.cap_pixels, 256, w.num_sms, 16), 256, 0, st>>>(
+            w.scenes, w.counts, w.d_scene, w.d_record, w.centers, centred, x, ux_dense);
     if (w.total_edges > 0)
         k_mf_reg<<<grid_for(w.total_edges, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.edge_scene, w.total_edges,
                                                                           w.r_record, w.centers, centred, x, ux_reg);
-    k_mf_gather<<<grid_for(w.total_nodes * 32u, 128, w.num_sms, 32), 128, 0, st>>>(
+    auto gather = w.dense_channels == 3 ? k_mf_gather<3> : k_mf_gather<1>;
+    gather<<<grid_for(w.total_nodes * 32u, 128, w.num_sms, 32), 128, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
         w.centers, centred, ux_dense, ux_reg, x, y);
     return cudaGetLastError();

@@ -58,6 +58,7 @@ struct Workspace {
     float4 *d_sw = nullptr, *d_cw = nullptr;
     uint32_t *d_scene = nullptr;        // [cap_pixels]
     float *d_record = nullptr;          // [cap_pixels * kDenseRecord]
+    int dense_channels = 3;             // 3 when a scene of the batch has the flow term, else 1 (64-byte records)
     float *r_record = nullptr;          // [cap_edges * kRegRecord]
 
     // node->term

@@ -10,6 +10,8 @@
 * A NaN in the inputs that reaches the right-hand side is reported as WS_ERR_NAN
   (the reference calls exit(-1), WarpSolverPCG.cu:21-31).
 * Counts beyond the 16-bit node ids and beyond the solver's capacities are refused up front.
+* A depth-only scene gets the same result bit for bit with the 64-byte dense records of a
+  depth-only batch and with the 128-byte records of a batch that holds a flow scene.
 """
 import ctypes as C
 import dataclasses
@@ -127,3 +129,20 @@ def test_counts_beyond_limits_are_refused(ws, tiny_scene, small_scene):
     assert lib.ws_set_batch(s._h, arr, 1) == WS_ERR_CAPACITY
     arr = (WsInputs * 2)(ds.to_inputs(), ds.to_inputs())   # more scenes than max_scenes
     assert lib.ws_set_batch(s._h, arr, 2) == WS_ERR_CAPACITY
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_depth_only_scene_same_in_a_batch_with_flow(ws, tiny_scene, precision):
+    import sys
+    from pathlib import Path
+    from starhub_b200.solver import DeviceScene
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import make_golden
+    d = dict(np.load(Path(__file__).resolve().parent / "golden" / "torus_small_flow.npz"))
+    flow = DeviceScene.from_scene(make_golden.scene_from_arrays(d))
+    assert flow.lambda_of > 0
+    depth = DeviceScene.from_scene(tiny_scene)
+    assert depth.lambda_of == 0
+    (alone,) = _solve([depth], precision=precision)
+    mixed = _solve([flow, depth], precision=precision)
+    np.testing.assert_array_equal(mixed[1], alone)
