@@ -35,7 +35,7 @@ void free_all(ws::Workspace &w) {
                     w.n2t_val_alt, w.n2t_offset, w.pair_key, w.pair_key_alt, w.pair_val, w.pair_val_alt,
                     w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
-                    w.col_key_alt, w.col_val_alt, w.colidx, w.entry_ref, w.entry_info, w.pcg_warp_groups, w.mf_ux, w.diag_blocks, w.pair_blocks, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
+                    w.col_key_alt, w.col_val_alt, w.colidx, w.item_ptr, w.item_info, w.sym_blocks, w.contrib, w.pcg_warp_groups, w.mf_ux, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
                     w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter,
                     w.error_flag};
     for (void *p : ptrs)
@@ -134,8 +134,9 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     w.cap_n2t = 4u * w.cap_pixels + 2u * w.cap_edges + w.cap_nodes + 4u * w.cap_features;
     w.cap_pair_kv = 6u * w.cap_pixels + w.cap_edges + 6u * w.cap_features;
     w.cap_half = std::min<uint32_t>(w.cap_pair_kv, 64u * w.cap_nodes);
-    w.cap_half = std::min<uint32_t>(w.cap_half, ws::kRefTransposed - 1u);
+    w.cap_half = std::min<uint32_t>(w.cap_half, (0xFFFFFFF0u - w.cap_nodes) / 2u);
     w.cap_blocks = w.cap_nodes + 2u * w.cap_half;
+    w.cap_items = w.cap_nodes + w.cap_half;
     const uint32_t sort_cap = std::max(std::max(w.cap_n2t, w.cap_pair_kv), w.cap_half);
     const uint32_t scan_cap = std::max(std::max(w.cap_pair_kv, w.cap_nodes), w.cap_tiles) + 1;
     cudaError_t e = cudaSuccess;
@@ -184,10 +185,10 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.col_key_alt, w.cap_half));
     A(dalloc(&w.col_val_alt, w.cap_half));
     A(dalloc(&w.colidx, w.cap_blocks));
-    A(dalloc(&w.entry_ref, w.cap_blocks));
-    A(dalloc(&w.entry_info, w.cap_blocks));
-    A(dalloc(&w.diag_blocks, (size_t)w.cap_nodes * 36));
-    A(dalloc(&w.pair_blocks, (size_t)std::max<uint32_t>(1u, w.cap_half) * 36));
+    A(dalloc(&w.item_ptr, (size_t)w.cap_nodes + 1));
+    A(dalloc(&w.item_info, w.cap_items));
+    A(dalloc(&w.sym_blocks, (size_t)w.cap_items * 36));
+    A(dalloc(&w.contrib, (size_t)std::max<uint32_t>(1u, w.cap_half) * 8));
     A(dalloc(&w.inv_diag, (size_t)w.cap_nodes * 36));
     A(dalloc(&w.diag64, (size_t)w.cap_nodes * 21));
     for (float **v : {&w.jtr, &w.x, &w.r, &w.q}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
@@ -832,28 +833,32 @@ int ws_get_system(ws_solver *h, int scene, uint32_t *rowptr, uint32_t *cols, flo
         for (uint32_t i = 0; i < e - b; ++i) cols[i] = ci[i] - (uint32_t)sc.node_base;
     }
     if (blocks) {
-        // expand the symmetric store (diagonal per node, one block per pair) into full block-CSR rows
-        const auto ref = download(w.entry_ref + b, e - b);
-        const auto diag = download(w.diag_blocks + 36ull * sc.node_base, 36ull * sc.num_nodes);
-        uint32_t hmin = 0xFFFFFFFFu, hmax = 0;
-        for (uint32_t r : ref)
-            if (r != ws::kInvalidIndex) {
-                hmin = std::min(hmin, r & ~ws::kRefTransposed);
-                hmax = std::max(hmax, r & ~ws::kRefTransposed);
+        // expand the symmetric store (per row: the diagonal, then the upper pairs in column
+        // order) into full block-CSR rows; a lower slot is the transpose of an upper item
+        const auto ci = download(w.colidx + b, e - b);
+        const auto ip = download(w.item_ptr + sc.node_base, (size_t)sc.num_nodes + 1);
+        const uint32_t ub = ip.front(), ue = ip.back();
+        const auto sb = download(w.sym_blocks + 36ull * ub, 36ull * (ue - ub));
+        const auto info = download(w.item_info + ub, (size_t)(ue - ub));
+        const uint32_t nb = (uint32_t)sc.node_base;
+        auto upper = [&](uint32_t i, uint32_t col) -> const float * {   // local row i, global column
+            uint32_t lo = ip[i] + 1, hi = ip[i + 1];
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (info[mid - ub].x < col) lo = mid + 1; else hi = mid;
             }
-        std::vector<float> pb;
-        if (hmin <= hmax) pb = download(w.pair_blocks + 36ull * hmin, 36ull * (hmax - hmin + 1));
+            if (lo >= ip[i + 1] || info[lo - ub].x != col) return nullptr;
+            return sb.data() + 36ull * (lo - ub);
+        };
         for (int i = 0; i < sc.num_nodes; ++i)
             for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
                 float *out = blocks + 36ull * (k - b);
-                if (k == rp[i]) {
-                    std::copy(diag.begin() + 36ull * i, diag.begin() + 36ull * (i + 1), out);
-                    continue;
-                }
-                const uint32_t r = ref[k - b];
-                if (r == ws::kInvalidIndex) return WS_ERR_CAPACITY;
-                const float *src = pb.data() + 36ull * ((r & ~ws::kRefTransposed) - hmin);
-                const bool tr = (r & ws::kRefTransposed) != 0;
+                const uint32_t col = ci[k - b];
+                const bool tr = col < nb + (uint32_t)i;
+                const float *src = k == rp[i] ? sb.data() + 36ull * (ip[i] - ub)
+                                   : tr       ? upper(col - nb, nb + (uint32_t)i)
+                                              : upper((uint32_t)i, col);
+                if (!src) return WS_ERR_CAPACITY;
                 for (int a = 0; a < 6; ++a)
                     for (int c = 0; c < 6; ++c) out[6 * a + c] = tr ? src[6 * c + a] : src[6 * a + c];
             }

@@ -20,7 +20,6 @@ constexpr int kDenseRecord = 32;     // floats per dense-term record, largest la
 constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
 constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group (divides 32)
-constexpr uint32_t kRefTransposed = 0x80000000u;   // entry_ref flag: lower-triangle use of a pair block
 
 // Dense-term record layouts, chosen per batch.  With the optical-flow term (some scene of the
 // batch has lambda_of != 0) a record holds C = 3 channels in 128 B: gradients 0..17 (three

@@ -344,9 +344,12 @@ __global__ void k_row_first(const uint32_t *half_row, const uint32_t *counts, ui
         if (h == 0 || half_row[h - 1] != half_row[h]) row_first[half_row[h]] = h;
 }
 
-__global__ void k_row_len(const uint32_t *up, const uint32_t *lo, uint32_t total_nodes, uint32_t *len) {
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x)
+__global__ void k_row_len(const uint32_t *up, const uint32_t *lo, uint32_t total_nodes, uint32_t *len,
+                          uint32_t *items) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         len[g] = 1u + up[g] + lo[g];
+        items[g] = 1u + up[g];   // stored blocks of the row: the diagonal and the upper pairs
+    }
 }
 
 __global__ void k_col_kv(const uint32_t *half_col, const uint32_t *counts, uint32_t *keys, uint32_t *vals) {
@@ -360,11 +363,14 @@ __global__ void k_col_kv(const uint32_t *half_col, const uint32_t *counts, uint3
 // Block-CSR slots: every row is [diagonal, columns < row ascending, columns > row ascending],
 // which is the sorted symmetric pair order of computeSymmetricNodePairKernel + sort
 // (NodePair2TermsIndex.cu:171-192, 656-675) with the diagonal block placed first as in the
-// Bin-Blocked CSR (NodePairRowColumnIndex.cu:110-124).
+// Bin-Blocked CSR (NodePairRowColumnIndex.cu:110-124).  Also the item record of every pair
+// h = (row, col) of the symmetric store (item h + row + 1): its lower entry is its position
+// k among the pairs sorted by column (then row).
 __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, const uint32_t *counts,
                         const uint32_t *half_row, const uint32_t *half_col, const uint32_t *row_first,
-                        const uint32_t *row_cnt_lo, const uint32_t *rowptr, uint32_t cap_blocks,
-                        uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx, uint32_t *entry_ref, int *err) {
+                        const uint32_t *row_cnt_lo, const uint32_t *rowptr, const uint32_t *node_scene,
+                        uint32_t cap_blocks, uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx,
+                        uint4 *item_info, int *err) {
     const uint32_t n = counts[kCntHalf];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t col = sorted_col[k];
@@ -387,33 +393,29 @@ __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, co
         slot_up[h] = s_up;
         colidx[s_lo] = row;
         colidx[s_up] = half_col[h];
-        entry_ref[s_up] = h;
-        entry_ref[s_lo] = h | kRefTransposed;
+        item_info[h + row + 1u] = make_uint4(half_col[h], k, row, node_scene[row]);
     }
 }
 
 // Diagonal slot of every row, plus the packed (col, ref, row, scene) record of each slot of
 // the row that the PCG streams.
-__global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *node_scene, uint32_t total_nodes,
-                            uint32_t cap_blocks, uint32_t *colidx, uint32_t *entry_ref, uint4 *entry_info, int *err) {
+__global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *item_ptr, const uint32_t *node_scene,
+                            uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx, uint4 *item_info, int *err) {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         const uint32_t s = rowptr[g];
-        const uint32_t e = min(rowptr[g + 1], cap_blocks);
-        const uint32_t scene = node_scene[g];
-        if (s < cap_blocks) {
-            colidx[s] = g;
-            entry_ref[s] = kInvalidIndex;   // the diagonal block lives in diag_blocks[g]
-        }
-        for (uint32_t k = s; k < e; ++k) entry_info[k] = make_uint4(colidx[k], entry_ref[k], g, scene);
+        if (s < cap_blocks) colidx[s] = g;
+        // the row's first item is its diagonal block
+        item_info[item_ptr[g]] = make_uint4(g, kInvalidIndex, g, node_scene[g]);
         if (g + 1 == total_nodes && rowptr[total_nodes] > cap_blocks) set_error(err, WS_ERR_CAPACITY);
     }
 }
 
-// First row group of every PCG warp, chosen so that the warps' slot ranges are about equal:
-// warp w starts at the first group whose first slot is at or past w / warps of all slots.
-__global__ void k_pcg_ranges(const uint32_t *rowptr, const uint32_t *group_row, uint32_t groups,
-                             uint32_t total_nodes, uint32_t cap_blocks, uint32_t warps, uint32_t *warp_groups) {
-    const uint32_t total = min(rowptr[total_nodes], cap_blocks);
+// First row group of every PCG warp, chosen so that the warps' stored blocks (items) are
+// about equal: warp w starts at the first group whose first item is at or past w / warps
+// of all items.
+__global__ void k_pcg_ranges(const uint32_t *item_ptr, const uint32_t *group_row, uint32_t groups,
+                             uint32_t total_nodes, uint32_t cap_items, uint32_t warps, uint32_t *warp_groups) {
+    const uint32_t total = min(item_ptr[total_nodes], cap_items);
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w <= warps; w += gridDim.x * blockDim.x) {
         if (w == warps) {
             warp_groups[w] = groups;
@@ -423,7 +425,7 @@ __global__ void k_pcg_ranges(const uint32_t *rowptr, const uint32_t *group_row, 
         uint32_t lo = 0, hi = groups;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (rowptr[min(group_row[mid], total_nodes)] < target) lo = mid + 1;
+            if (item_ptr[min(group_row[mid], total_nodes)] < target) lo = mid + 1;
             else hi = mid;
         }
         warp_groups[w] = lo;
@@ -488,28 +490,29 @@ void index_build(Workspace &w, cudaStream_t st) {
     count_launch(w, 1 + 3 + 1);
     // 4. block CSR
     k_row_first<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_row, w.counts, w.row_first);
-    k_row_len<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.row_cnt_up, w.row_cnt_lo, N, w.rowptr);
+    k_row_len<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.row_cnt_up, w.row_cnt_lo, N, w.rowptr, w.item_ptr);
     exclusive_scan(w.rowptr, w.rowptr, nullptr, N, w.cap_nodes, w.scan_tmp, st);
+    exclusive_scan(w.item_ptr, w.item_ptr, nullptr, N, w.cap_nodes, w.scan_tmp, st);
     k_col_kv<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_col, w.counts, w.col_key, w.col_val);
     const bool col_alt = radix_sort<uint32_t>(w.col_key, w.col_val, w.col_key_alt, w.col_val_alt, w.counts + kCntHalf,
                                               0, w.cap_half, w.node_bits, w.sort_hist, w.sort_digit, st);
-    count_launch(w, 1 + 1 + 3 + 1 + 3 * ((w.node_bits + 7) / 8));
+    count_launch(w, 1 + 1 + 3 + 3 + 1 + 3 * ((w.node_bits + 7) / 8));
     const uint32_t *scol = col_alt ? w.col_key_alt : w.col_key;
     const uint32_t *sh = col_alt ? w.col_val_alt : w.col_val;
     k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,
-                                                                    w.row_first, w.row_cnt_lo, w.rowptr, w.cap_blocks,
-                                                                    w.half_slot_up, w.half_slot_lo, w.colidx, w.entry_ref,
-                                                                    w.error_flag);
-    k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.node_scene, N, w.cap_blocks, w.colidx,
-                                                             w.entry_ref, w.entry_info, w.error_flag);
+                                                                    w.row_first, w.row_cnt_lo, w.rowptr, w.node_scene,
+                                                                    w.cap_blocks, w.half_slot_up, w.half_slot_lo, w.colidx,
+                                                                    w.item_info, w.error_flag);
+    k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.item_ptr, w.node_scene, N, w.cap_blocks,
+                                                             w.colidx, w.item_info, w.error_flag);
     count_launch(w, 2);
     pcg_ranges(w, st);
 }
 
 void pcg_ranges(Workspace &w, cudaStream_t st) {
     const uint32_t warps = (uint32_t)(pcg_launch_blocks(w) * pcg_warps_per_block());
-    k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.chunk_row, w.total_chunks,
-                                                                      w.total_nodes, w.cap_blocks, warps,
+    k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.item_ptr, w.chunk_row, w.total_chunks,
+                                                                      w.total_nodes, w.cap_items, warps,
                                                                       w.pcg_warp_groups);
     count_launch(w);
 }

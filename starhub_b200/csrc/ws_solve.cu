@@ -440,7 +440,8 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
                                                                      const uint32_t *n2t_offset, const uint32_t *n2t_val,
                                                                      const float *drec, const float *rrec,
                                                                      const float *se3, const float4 *centers,
-                                                                     float *diag_blocks, double *diag64, float *jtr,
+                                                                     const uint32_t *item_ptr, uint32_t cap_items,
+                                                                     float *sym_blocks, double *diag64, float *jtr,
                                                                      int *err) {
     constexpr bool kCentred = sizeof(DAcc) == 8;   // mixed precision also uses node-centred twists
     constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;
@@ -553,7 +554,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
         __syncwarp();
         if (lane < 21) {
             acc += regulariser_entry<DAcc>(ea, ec, cen, kCentred);
-            float *blk = diag_blocks + 36ull * g;
+            float *blk = sym_blocks + 36ull * min(item_ptr[g], cap_items - 1);   // the row's first item
             blk[6 * ea + ec] = (float)acc;
             blk[6 * ec + ea] = (float)acc;
             if (kCentred) diag64[21ull * g + lane] = (double)acc;
@@ -570,7 +571,8 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
 // accumulated block (mixed precision) or the reference's FP32 Gauss-Jordan with
 // partial pivoting of the stored block (BlockDiagonalPreconditionerInverse.cuh:14-73).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, const float *diag_blocks,
+__global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, const float *sym_blocks,
+                                                       const uint32_t *item_ptr, uint32_t cap_items,
                                                        uint32_t total_nodes, int fp64, float *inv_diag) {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         float inv[36];
@@ -589,7 +591,7 @@ __global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, con
         } else {
             float full[36];
 #pragma unroll
-            for (int i = 0; i < 36; ++i) full[i] = diag_blocks[36ull * g + i];
+            for (int i = 0; i < 36; ++i) full[i] = sym_blocks[36ull * min(item_ptr[g], cap_items - 1) + i];
             gauss_jordan6(full, inv);
         }
         float4 *o = reinterpret_cast<float4 *>(inv_diag + 36ull * g);
@@ -625,7 +627,7 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
     const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
-    const float4 *centers, int centred, float *pair_blocks) {
+    const float4 *centers, int centred, float *sym_blocks) {
     constexpr int kSlot = kSlotWordsF32;
     static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
     __shared__ __align__(16) float stage[NT / 32][32 * kSlot];
@@ -723,7 +725,9 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
             if (lane < 4) acc1 += slots[l * kSlot + 32 + lane];
         }
         __syncwarp();
-        float *blk = pair_blocks + 36ull * h;   // row-major, rows of node `row`, columns of node `col`
+        // item h + row + 1 of the symmetric store: the row's diagonal item and its earlier pairs
+        // precede it; row-major, rows of node `row`, columns of node `col`
+        float *blk = sym_blocks + 36ull * (h + row + 1);
         blk[lane] = acc0;
         if (lane < 4) blk[32 + lane] = acc1;
     }
@@ -734,25 +738,31 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
 // libs/star/pcg_solver/BlockPCG.cuh:67-190, 325-484) for every scene of the batch.
 //
 // Rows (nodes) are grouped in scene-aligned groups of kRowsPerGroup; every warp
-// owns a fixed set of groups (grid-stride over warps) and walks their rows one at
-// a time, with no block-level synchronisation inside a phase.
+// owns a contiguous range of groups (balanced by stored blocks) and walks their rows,
+// with no block-level synchronisation.
 // Per iteration: phase A  d = s + beta d (recomputed for neighbours from s and the
-// previous d), q = A d, <d, q>;  phase B  alpha, x += alpha d, r -= alpha q,
-// s = M^-1 r, <r, s>.  A warp keeps its group's partial in FP64 registers, stores
-// it, and the last group of a scene to finish (a fenced atomic ticket) sums that
-// scene's group partials in group order and publishes alpha or beta; the sums
-// therefore never depend on the rest of the batch.  One bounded grid barrier
-// ends each phase; a timed-out wait sets WS_ERR_TIMEOUT and every block leaves.
+// previous d), q = A d from each stored block read once (the transposed products go
+// to the lower rows through a contribution buffer), <d, A d>;  phase B  alpha,
+// q += the row's contributions, x += alpha d, r -= alpha q, s = M^-1 r, <r, s>.
+// A warp keeps its group's partial in FP64 registers, stores it, and the last group
+// of a scene to finish (a fenced atomic ticket) sums that scene's group partials in
+// group order, publishes alpha or beta and bumps the scene's generation counter; the
+// sums therefore never depend on the rest of the batch.  After each phase a warp waits
+// only for the scenes of its own rows; a wait is bounded, and a timed-out wait sets
+// WS_ERR_TIMEOUT and the warp leaves.
 // ---------------------------------------------------------------------------
 
 struct PcgArgs {
     const Scene *scenes;
     const uint32_t *group_scene, *group_row;
     uint32_t total_groups;
-    const uint32_t *rowptr, *colidx, *entry_ref;
-    const uint4 *entry_info;
+    const uint32_t *rowptr;        // block-CSR row pointers (lower slots follow the diagonal)
+    const uint32_t *item_ptr;      // [nodes + 1] first item of every row in the symmetric store
+    const uint4 *item_info;        // per item: column, CSR slot of the transposed use, row, scene
     const uint32_t *warp_groups;   // [warps + 1] first row group of each warp
-    const float *diag_blocks, *pair_blocks, *inv_diag, *jtr;
+    const float *sym_blocks;       // per item: the 6x6 block, row-major
+    const float *inv_diag, *jtr;
+    float *contrib;                // per lower entry (row j, column i < j): B^T v_i left for row j
     float *x, *r, *q;
     float *sd0, *sd1;         // [node][16]: s (6, padded to 8) then d (6, padded); swapped every iteration
     double *group_partial;
@@ -760,7 +770,7 @@ struct PcgArgs {
     // per scene, kSceneSync words: [0] phase-A tickets, [1] phase-B / init tickets (arrivals of
     // row groups), [32] alpha generation, [33] delta/beta generation (bumped when published)
     uint32_t *scene_counter;
-    uint32_t cap_blocks, cap_half, total_nodes, num_scenes;
+    uint32_t cap_blocks, cap_half, cap_items, total_nodes, num_scenes;
     int *err;
     float *se3;
     const float4 *centers;
@@ -929,29 +939,42 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 }
 
 // ---------------------------------------------------------------------------
-// Phase A of a PCG iteration over one warp's rows: d = s + beta d_old, q = A d and the
-// per-row <d, q>.  The warp streams its contiguous slot range 32 slots at a time:
-//   * the packed slot records of chunk j + 2 are loaded while chunk j is computed;
-//   * the 6x6 blocks of chunk j + 1 are copied into shared memory with cp.async and its
-//     s / d_old vectors and beta are loaded into registers, also while chunk j is computed;
-//   * lane l multiplies slot l's block (transposed for a lower-triangle slot) with d of the
-//     slot's column, and the lane that ends a row sums the row's products in slot order,
-//     continuing a row that began in an earlier chunk from a carried partial sum.
-// Each row's sum therefore runs over its slots in a fixed order whatever the chunk
-// alignment, so results do not depend on which warp handled the row or on the batch.
+// Symmetric block SpMV over one warp's rows, each stored block read once.
+// The block store holds, row by row, the diagonal block and then the blocks of the row's
+// upper pairs (column > row) in column order; these are the row's items
+// u = item_ptr[row] .. item_ptr[row + 1).  For item (i, j) with block B (rows of node i,
+// columns of node j) the lane forms a = B v_j, which is added to row i, and, off the
+// diagonal, t = B^T v_i, which it stores as lower entry (row j, column i); lower entries
+// are numbered by row, then column, so the owner of row j adds its contributions
+// afterwards from one contiguous range, in column order (the CSR slot order).
+// A warp's items are contiguous, so its blocks stream in as whole lines:
+//   * the item records of chunk j + 2 are loaded while chunk j is computed;
+//   * the blocks (9 x 16 B each, contiguous) and the column vector records of chunk j + 1
+//     are copied into shared memory with cp.async, also while chunk j is computed;
+//   * a row's diagonal item (always its first) publishes v_i through a ring in shared
+//     memory, where the row's later items, in this chunk or a later one, read it;
+//   * the lane that ends a row sums the row's products in item order, continuing a row
+//     that began in an earlier chunk from a carried partial sum.
+// kPcg: phase A of a PCG iteration: v = d = s + beta d_old (recomputed for every column
+// from the s/d record of the previous iteration), q without its lower part, and per row
+// <d_i, (A d)_i> summed over the row's items as d_i . a, twice for an off-diagonal item
+// (it stands for both orientations).  Otherwise the first pass of y = A x.
+// Each row's sums run over its items in a fixed order whatever the chunk alignment, so
+// results do not depend on which warp handled the row or on the batch.
 // ---------------------------------------------------------------------------
 constexpr int kPcgThreads = 128;                              // 4 warps per block
-constexpr int kPcgSlot = 52;                                  // block (36) + s/d record (16) per slot
+constexpr int kPcgSlot = 52;                                  // block (36) + column vector record (16) per item
 constexpr int kPcgChunkFloats = 32 * kPcgSlot;
 constexpr int kPcgRing = 64;                                  // rows kept in the per-warp rings
 constexpr int kPcgWarpFloats = 2 * kPcgChunkFloats + kPcgRing * 8 + 2 * kPcgRing;
 constexpr size_t kPcgSmemBytes = sizeof(float) * kPcgWarpFloats * (kPcgThreads / 32);
 
-// Packed slot record (col, ref, row, scene); row = kInvalidIndex past the end of the range.
-// Loaded raw and only read one chunk later, so the load never stalls the warp.
-__device__ __forceinline__ uint4 load_slot(const uint4 *info, uint32_t k, uint32_t end) {
+// Item record (column, lower entry of the transposed use or kInvalidIndex for the diagonal,
+// row, scene); row = kInvalidIndex past the end of the range.  Loaded raw and only read
+// one chunk later, so the load never stalls the warp.
+__device__ __forceinline__ uint4 load_item(const uint4 *info, uint32_t u, uint32_t end) {
     uint4 v = make_uint4(0u, kInvalidIndex, kInvalidIndex, 0u);
-    if (k < end) v = __ldg(info + k);
+    if (u < end) v = __ldg(info + u);
     return v;
 }
 
@@ -962,40 +985,33 @@ __device__ __forceinline__ void cp_async16(float *dst, const float *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Operands of one chunk held in registers: the slot record, s and d_old of its column, beta.
+// Operands of one chunk held in registers: the item record and (PCG) beta of its scene.
 struct PcgOperands {
-    uint4 slot;
+    uint4 item;
     double beta;
 };
 
-__device__ __forceinline__ const float *slot_block(const PcgArgs &A, uint32_t col, uint32_t ref) {
-    return ref == kInvalidIndex ? A.diag_blocks + 36ull * col
-                                : A.pair_blocks + 36ull * min(ref & ~kRefTransposed, A.cap_half - 1);
-}
-
-// Starts a chunk: copies of each slot's block and of its column's vector record into
-// `stage`, and (PCG) a register load of beta.  The PCG's vector record is the column's s/d
-// pair (64 B); a plain SpMV's is x of the column (32 B).  The chunk's 16-byte parts (9 per
-// block, 4 or 2 per vector record) are spread flat over the lanes, so each copy
-// instruction reads a few whole blocks or records instead of one piece of 32 of them.
+// Starts the chunk of items u .. u + 31 (those below u_end): copies of the blocks and of
+// each item's column vector record into `stage`, and (PCG) a register load of beta.  The
+// PCG's vector record is the column's s/d pair (64 B); a plain SpMV's is x of the column
+// (32 B).  The 16-byte parts (9 per block, 4 or 2 per vector record) are spread flat over
+// the lanes, so every copy instruction of the blocks reads 512 contiguous bytes.
 template <bool kPcg>
-__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_in, uint4 x, float *stage, int lane,
-                                           PcgOperands &op) {
+__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_in, uint32_t u, uint32_t u_end, uint4 x,
+                                           float *stage, int lane, PcgOperands &op) {
     constexpr int kVecParts = kPcg ? 4 : 2;
-    op.slot = x;
-    const float *blk = nullptr, *vec = nullptr;
+    op.item = x;
+    const float *vec = nullptr;
     if (x.z != kInvalidIndex) {
-        const uint32_t col = min(x.x, A.total_nodes - 1);
-        blk = slot_block(A, col, x.y);
-        vec = vec_in + (kPcg ? 16ull : 8ull) * col;
+        vec = vec_in + (kPcg ? 16ull : 8ull) * min(x.x, A.total_nodes - 1);
         if (kPcg) op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
     }
+    const uint32_t nparts = u < u_end ? 9u * min(32u, u_end - u) : 0u;
+    const float *src = A.sym_blocks + 36ull * u;
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
-        const int part = 32 * p + lane, e = part / 9, piece = part - 9 * e;
-        const float *b = reinterpret_cast<const float *>(
-            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(blk), e));
-        if (b) cp_async16(stage + kPcgSlot * e + 4 * piece, b + 4 * piece);
+        const uint32_t part = 32u * p + lane, e = part / 9u, piece = part - 9u * e;
+        if (part < nparts) cp_async16(stage + kPcgSlot * e + 4 * piece, src + 4ull * part);
     }
 #pragma unroll
     for (int p = 0; p < kVecParts; ++p) {
@@ -1007,22 +1023,20 @@ __device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_i
     cp_async_commit();
 }
 
-// kPcg: phase A of a PCG iteration (vec_in = s/d records of the previous iteration, out =
-// the s/d records whose d this iteration writes, plus q and the group partials of <d, q>).
-// Otherwise a plain y = A x over the warp's rows (vec_in = x, out = y, 8 floats per node).
 template <bool kPcg>
-__device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
-                            float *out, float *wsm, int lane) {
+__device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
+                             float *out, float *wsm, int lane) {
     if (g0 >= g1) return;
     float *stage[2] = {wsm, wsm + kPcgChunkFloats};
-    float *dring = wsm + 2 * kPcgChunkFloats;                 // [kPcgRing][8] d of the row, by row
-    double *gring = reinterpret_cast<double *>(dring + kPcgRing * 8);   // [kPcgRing] <d, q> by row
-    const uint32_t e0 = A.rowptr[r0], e1 = min(A.rowptr[r1], A.cap_blocks);
-    const uint32_t nchunks = e1 > e0 ? (e1 - e0 + 31) / 32 : 0;
-    uint4 nxt = load_slot(A.entry_info, e0 + 32 + lane, e1);
+    float *vring = wsm + 2 * kPcgChunkFloats;                           // [kPcgRing][8] v of the row, by row
+    double *gring = reinterpret_cast<double *>(vring + kPcgRing * 8);   // [kPcgRing] <d, A d> by row
+    const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
+    const uint32_t nchunks = u1 > u0 ? (u1 - u0 + 31) / 32 : 0;
+    uint4 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
     PcgOperands cur;
-    issue_chunk<kPcg>(A, vec_in, load_slot(A.entry_info, e0 + lane, e1), stage[0], lane, cur);
+    issue_chunk<kPcg>(A, vec_in, u0, u1, load_item(A.item_info, u0 + lane, u1), stage[0], lane, cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    double carry_dot = 0.0;
     uint32_t carry_row = kInvalidIndex;
     // first rows of groups win .. win + 31 (lane i holds group win + i), reloaded as groups complete
     uint32_t win = g0;
@@ -1036,29 +1050,40 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
     for (uint32_t j = 0; j < nchunks; ++j) {
         // chunk j + 1 in flight, chunk j + 2 records requested
         PcgOperands next;
-        issue_chunk<kPcg>(A, vec_in, nxt, stage[(j + 1) & 1], lane, next);
-        const uint4 after = load_slot(A.entry_info, e0 + 32 * (j + 2) + lane, e1);
+        issue_chunk<kPcg>(A, vec_in, u0 + 32 * (j + 1), u1, nxt, stage[(j + 1) & 1], lane, next);
+        const uint4 after = load_item(A.item_info, u0 + 32 * (j + 2) + lane, u1);
         cp_async_wait_prior();
         __syncwarp();
-        const bool valid = cur.slot.z != kInvalidIndex;
-        const uint32_t xrow = valid ? min(cur.slot.z, A.total_nodes - 1) : kInvalidIndex;
-        const uint32_t xref = cur.slot.y;
-        float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const bool valid = cur.item.z != kInvalidIndex;
+        const uint32_t xrow = valid ? min(cur.item.z, A.total_nodes - 1) : kInvalidIndex;
+        const uint32_t tslot = cur.item.y;
+        const bool diag = tslot == kInvalidIndex;
         float *mine = stage[j & 1] + kPcgSlot * lane;
+        float vc[6];   // v of the item's column
         if (valid) {
-            float dv[6];
             const float4 s0 = reinterpret_cast<const float4 *>(mine + 36)[0];
             const float2 s1 = reinterpret_cast<const float2 *>(mine + 40)[0];
             if (kPcg) {
                 const float beta = (float)cur.beta;
                 const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
                 const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
-                dv[0] = s0.x + beta * d0.x; dv[1] = s0.y + beta * d0.y; dv[2] = s0.z + beta * d0.z;
-                dv[3] = s0.w + beta * d0.w; dv[4] = s1.x + beta * d1.x; dv[5] = s1.y + beta * d1.y;
+                vc[0] = s0.x + beta * d0.x; vc[1] = s0.y + beta * d0.y; vc[2] = s0.z + beta * d0.z;
+                vc[3] = s0.w + beta * d0.w; vc[4] = s1.x + beta * d1.x; vc[5] = s1.y + beta * d1.y;
             } else {
-                dv[0] = s0.x; dv[1] = s0.y; dv[2] = s0.z; dv[3] = s0.w; dv[4] = s1.x; dv[5] = s1.y;
+                vc[0] = s0.x; vc[1] = s0.y; vc[2] = s0.z; vc[3] = s0.w; vc[4] = s1.x; vc[5] = s1.y;
             }
-            // A dv and A^T dv from one pass over the block, a float4 at a time
+            if (diag) {
+                float4 *vr = reinterpret_cast<float4 *>(vring + 8 * (xrow & (kPcgRing - 1)));
+                vr[0] = make_float4(vc[0], vc[1], vc[2], vc[3]);
+                vr[1] = make_float4(vc[4], vc[5], 0.f, 0.f);
+            }
+        }
+        __syncwarp();
+        if (valid) {
+            const float4 v0 = reinterpret_cast<const float4 *>(vring + 8 * (xrow & (kPcgRing - 1)))[0];
+            const float2 v1 = reinterpret_cast<const float2 *>(vring + 8 * (xrow & (kPcgRing - 1)) + 4)[0];
+            const float vr[6] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y};   // v of the item's row
+            // B v_col and B^T v_row from one pass over the block, a float4 at a time
             float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             const float4 *blk = reinterpret_cast<const float4 *>(mine);
 #pragma unroll
@@ -1068,25 +1093,36 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int e = 4 * q + k, r = e / 6, c = e % 6;
-                    a[r] += e4[k] * dv[c];
-                    t[c] += e4[k] * dv[r];
+                    a[r] += e4[k] * vc[c];
+                    t[c] += e4[k] * vr[r];
                 }
             }
-            const bool tr = xref != kInvalidIndex && (xref & kRefTransposed) != 0;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) p[i] = tr ? t[i] : a[i];
-            float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
-            pp[0] = make_float4(p[0], p[1], p[2], p[3]);
-            pp[1] = make_float4(p[4], p[5], 0.f, 0.f);
-            if (kPcg && xref == kInvalidIndex) {   // diagonal slot: d of the row itself
-                float4 *dd = reinterpret_cast<float4 *>(dring + 8 * (xrow & (kPcgRing - 1)));
-                dd[0] = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                dd[1] = make_float4(dv[4], dv[5], 0.f, 0.f);
+            if (!diag) {
+                float4 *co = reinterpret_cast<float4 *>(A.contrib + 8ull * min(tslot, A.cap_half - 1));
+                co[0] = make_float4(t[0], t[1], t[2], t[3]);
+                co[1] = make_float4(t[4], t[5], 0.f, 0.f);
             }
+            double dot = 0.0;
+            if (kPcg) {
+                if (A.fp64) {
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) dot += (double)vr[i] * (double)a[i];
+                    if (!diag) dot *= 2.0;
+                } else {
+                    float f = 0.f;
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) f += vr[i] * a[i];
+                    dot = (double)(diag ? f : 2.f * f);
+                }
+            }
+            float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
+            pp[0] = make_float4(a[0], a[1], a[2], a[3]);
+            reinterpret_cast<float2 *>(mine + 4)[0] = make_float2(a[4], a[5]);
+            reinterpret_cast<double *>(mine + 6)[0] = dot;
         }
         __syncwarp();
         // row segments of this chunk
-        const uint32_t next_first = __shfl_sync(0xffffffffu, next.slot.z, 0);
+        const uint32_t next_first = __shfl_sync(0xffffffffu, next.item.z, 0);
         const uint32_t row_up = __shfl_up_sync(0xffffffffu, xrow, 1);
         const uint32_t row_dn = __shfl_down_sync(0xffffffffu, xrow, 1);
         const uint32_t following = (lane == 31) ? next_first : row_dn;
@@ -1097,14 +1133,16 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
         const bool ends_row = valid && following != xrow;
         const bool owner = valid && (ends_row || lane == last);
         float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        double dsum = 0.0;
         if (owner) {
             const int first = 31 - __clz(start_mask & (0xffffffffu >> (31 - lane)));
             if (first == 0 && xrow == carry_row) {
 #pragma unroll
                 for (int i = 0; i < 6; ++i) sum[i] = carry[i];
+                dsum = carry_dot;
             }
             const float *chunk = stage[j & 1];
-            // sequential in slot order; unrolled so that the loads of later slots overlap
+            // sequential in item order; unrolled so that the loads of later items overlap
 #pragma unroll 4
             for (int l = first; l <= lane; ++l) {
                 const float4 a = reinterpret_cast<const float4 *>(chunk + kPcgSlot * l)[0];
@@ -1115,37 +1153,32 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
                 sum[3] += a.w;
                 sum[4] += b.x;
                 sum[5] += b.y;
+                if (kPcg) dsum += reinterpret_cast<const double *>(chunk + kPcgSlot * l + 6)[0];
             }
             if (ends_row && !kPcg) {
                 float4 *yo = reinterpret_cast<float4 *>(out + 8ull * xrow);
                 yo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
                 yo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
             } else if (ends_row) {
-                const float *dn = dring + 8 * (xrow & (kPcgRing - 1));
-                double dot = 0.0;
-                float dotf = 0.f;
-#pragma unroll
-                for (int i = 0; i < 6; ++i) {
-                    dot += (double)dn[i] * (double)sum[i];
-                    dotf += dn[i] * sum[i];
-                }
+                const float *dn = vring + 8 * (xrow & (kPcgRing - 1));
                 float4 *qo = reinterpret_cast<float4 *>(A.q + 8ull * xrow);
                 float4 *dno = reinterpret_cast<float4 *>(out + 16ull * xrow + 8);
                 qo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
                 qo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
                 dno[0] = make_float4(dn[0], dn[1], dn[2], dn[3]);
                 dno[1] = make_float4(dn[4], dn[5], 0.f, 0.f);
-                gring[xrow & (kPcgRing - 1)] = A.fp64 ? dot : (double)dotf;
+                gring[xrow & (kPcgRing - 1)] = A.fp64 ? dsum : (double)(float)dsum;
             }
         }
-        // partial sum of a row that continues into the next chunk
+        // partial sums of a row that continues into the next chunk
         const bool cont = __shfl_sync(0xffffffffu, owner && !ends_row ? 1 : 0, last) != 0;
 #pragma unroll
         for (int i = 0; i < 6; ++i) carry[i] = __shfl_sync(0xffffffffu, sum[i], last);
+        carry_dot = __shfl_sync(0xffffffffu, dsum, last);
         const uint32_t last_row = __shfl_sync(0xffffffffu, xrow, last);
         carry_row = cont ? last_row : kInvalidIndex;
         __syncwarp();
-        // groups whose rows are all done: their <d, q> partial, summed in row order
+        // groups whose rows are all done: their <d, A d> partial, summed in row order
         const uint32_t done_below = cont ? last_row : last_row + 1;
         while (kPcg && group < g1 && group_end <= done_below) {
             const uint32_t grow = group_first(group);
@@ -1174,6 +1207,26 @@ __device__ void stream_rows(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t
     // drain the last (empty) copy group before the stage buffers are reused
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
+}
+
+// Adds to v the contributions B^T v_i that the upper items of the rows i < row left as the
+// row's lower entries, in column order.  The rows before `row` hold rowptr[row] blocks, of
+// which item_ptr[row] are stored items, so the row's lower entries start at the difference.
+__device__ __forceinline__ void add_lower(const PcgArgs &A, uint32_t row, float *v) {
+    const uint32_t s0 = A.rowptr[row] - A.item_ptr[row];
+    uint32_t n = (A.rowptr[row + 1] - A.rowptr[row]) - (A.item_ptr[row + 1] - A.item_ptr[row]);
+    n = s0 < A.cap_half ? min(n, A.cap_half - s0) : 0u;
+#pragma unroll 4
+    for (uint32_t k = 0; k < n; ++k) {
+        const float4 a = __ldcg(reinterpret_cast<const float4 *>(A.contrib + 8ull * (s0 + k)));
+        const float2 b = __ldcg(reinterpret_cast<const float2 *>(A.contrib + 8ull * (s0 + k) + 4));
+        v[0] += a.x;
+        v[1] += a.y;
+        v[2] += a.z;
+        v[3] += a.w;
+        v[4] += b.x;
+        v[5] += b.y;
+    }
 }
 
 // One step of the per-node phases: lane l takes row l % kRowsPerGroup of group
@@ -1229,7 +1282,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
         float *sd_new = (it & 1) ? A.sd0 : A.sd1;
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
-        stream_rows<true>(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
+        stream_items<true>(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
         publish_range(A, g_begin, g_end, 0, lane);
         if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
@@ -1243,6 +1296,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
                 load6(sd_new + 16ull * n.node + 8, dv);
                 load6(A.r + 8ull * n.node, rv);
                 load6(A.q + 8ull * n.node, qv);
+                add_lower(A, n.node, qv);
 #pragma unroll
                 for (int i = 0; i < 6; ++i) {
                     xv[i] += alpha * dv[i];
@@ -1306,7 +1360,9 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 }
 
 // Standalone y = A x over the assembled symmetric store of the last Gauss-Newton iteration
-// (x, y: 8 floats per node), with the PCG's slot-balanced warp ranges and streaming.
+// (x, y: 8 floats per node), with the PCG's warp ranges and streaming: pass 1 (k_spmv)
+// writes the diagonal and upper part of every row and the transposed contributions;
+// pass 2 (k_spmv_lower) adds each row's contributions.
 __global__ void __launch_bounds__(kPcgThreads, 8) k_spmv(PcgArgs A, const float *x, float *y) {
     extern __shared__ __align__(16) float pcg_smem[];
     const int lane = threadIdx.x & 31;
@@ -1316,7 +1372,16 @@ __global__ void __launch_bounds__(kPcgThreads, 8) k_spmv(PcgArgs A, const float 
     const uint32_t g_end = max(g_begin, min(A.warp_groups[gwarp + 1], A.total_groups));
     const uint32_t r_begin = g_begin < A.total_groups ? A.group_row[g_begin] : A.total_nodes;
     const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
-    stream_rows<false>(A, g_begin, g_end, r_begin, r_end, x, y, wsm, lane);
+    stream_items<false>(A, g_begin, g_end, r_begin, r_end, x, y, wsm, lane);
+}
+
+__global__ void __launch_bounds__(256) k_spmv_lower(PcgArgs A, float *y) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < A.total_nodes; row += gridDim.x * blockDim.x) {
+        float v[6];
+        load6(y + 8ull * row, v);
+        add_lower(A, row, v);
+        store6(y + 8ull * row, v);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1541,7 +1606,7 @@ template <class DAcc, int NT, int C>
 static void launch_assemble_node_c(Workspace &w, cudaStream_t st) {
     k_assemble_node<DAcc, NT, C><<<grid_for(w.total_nodes * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
-        w.centers, w.diag_blocks, w.diag64, w.jtr, w.error_flag);
+        w.centers, w.item_ptr, w.cap_items, w.sym_blocks, w.diag64, w.jtr, w.error_flag);
 }
 
 template <class DAcc, int NT>
@@ -1569,7 +1634,8 @@ void gn_assemble_node(Workspace &w, cudaStream_t st) {
     else launch_assemble_node_nt<double>(w, w.tune.node_threads, st);
     count_launch(w);
     k_block_inverse<<<grid_for(w.total_nodes, 128, w.num_sms, 16), 128, 0, st>>>(
-        w.diag64, w.diag_blocks, w.total_nodes, w.precision == WS_PREC_MIXED ? 1 : 0, w.inv_diag);
+        w.diag64, w.sym_blocks, w.item_ptr, w.cap_items, w.total_nodes, w.precision == WS_PREC_MIXED ? 1 : 0,
+        w.inv_diag);
     count_launch(w);
 }
 
@@ -1577,7 +1643,7 @@ template <int NT, int C>
 static void launch_assemble_pair_c(Workspace &w, cudaStream_t st) {
     k_assemble_pair<NT, C><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
-        w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.pair_blocks);
+        w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.sym_blocks);
 }
 
 template <int NT>
@@ -1600,12 +1666,11 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.group_row = w.chunk_row;
     a.total_groups = w.total_chunks;
     a.rowptr = w.rowptr;
-    a.colidx = w.colidx;
-    a.entry_ref = w.entry_ref;
-    a.entry_info = w.entry_info;
+    a.item_ptr = w.item_ptr;
+    a.item_info = w.item_info;
+    a.contrib = w.contrib;
     a.warp_groups = w.pcg_warp_groups;
-    a.diag_blocks = w.diag_blocks;
-    a.pair_blocks = w.pair_blocks;
+    a.sym_blocks = w.sym_blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
     a.x = w.x; a.r = w.r; a.q = w.q; a.sd0 = w.sd0; a.sd1 = w.sd1;
@@ -1613,6 +1678,7 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.scalars = w.scene_scalars;
     a.scene_counter = w.scene_counter;
     a.cap_blocks = w.cap_blocks;
+    a.cap_items = w.cap_items;
     a.cap_half = std::max<uint32_t>(1u, w.cap_half);
     a.num_scenes = (uint32_t)std::max(1, w.num_scenes);
     a.total_nodes = w.total_nodes;
@@ -1657,6 +1723,7 @@ cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *u
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st) {
     const PcgArgs a = pcg_args(w, 0);
     k_spmv<<<pcg_launch_blocks(w), kPcgThreads, kPcgSmemBytes, st>>>(a, x, y);
+    k_spmv_lower<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(a, y);
     return cudaGetLastError();
 }
 

@@ -84,16 +84,19 @@ struct Workspace {
     uint32_t *rowptr = nullptr;                              // [cap_nodes + 1]
     uint32_t *col_key = nullptr, *col_val = nullptr, *col_key_alt = nullptr, *col_val_alt = nullptr; // [cap_half]
     uint32_t *colidx = nullptr;                              // [cap_blocks]
-    // Symmetric block storage: one 6x6 block per node (diagonal) and one per unordered pair
-    // (row < col orientation); entry_ref maps an off-diagonal CSR slot to its pair block,
-    // with kRefTransposed set for the lower-triangle entry.
-    uint32_t *entry_ref = nullptr;                           // [cap_blocks]
-    uint4 *entry_info = nullptr;                             // [cap_blocks] (col, ref, row, scene) for the PCG
+    // Symmetric block store: row by row, the diagonal block and then one block per upper pair
+    // (row < col, column order).  These are the row's items, item_ptr[row] .. item_ptr[row + 1);
+    // pair h is item h + row + 1.  item_info holds per item (column, lower entry of the
+    // transposed use or kInvalidIndex, row, scene); lower entries are numbered by row, then
+    // column, and contrib holds one 8-float vector per lower entry for the SpMV.
+    uint32_t cap_items = 0;                                  // cap_nodes + cap_half
+    uint32_t *item_ptr = nullptr;                            // [cap_nodes + 1]
+    uint4 *item_info = nullptr;                              // [cap_items]
+    float *sym_blocks = nullptr;                             // [cap_items * 36]
+    float *contrib = nullptr;                                // [cap_half * 8]
     uint32_t *pcg_warp_groups = nullptr;                     // [pcg_grid * warps per block + 1]
     float *mf_ux = nullptr;             // matrix-free SpMV scratch: J x per dense term and edge (float4),
                                         // allocated on first use
-    float *diag_blocks = nullptr;                            // [cap_nodes * 36]
-    float *pair_blocks = nullptr;                            // [cap_half * 36]
 
     // per-node system and PCG state (stride kVecStride)
     float *inv_diag = nullptr;          // [cap_nodes * 36]
