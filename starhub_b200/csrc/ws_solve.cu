@@ -308,24 +308,44 @@ __device__ void cholesky6_fp64(const double *in, float *out) {
 constexpr int kSlotWordsF32 = 36;   // 144 B: a dense record, or 27 (node) / 36 (pair) partial sums
 constexpr int kSlotWordsF64 = 60;   // 240 B: a dense record, or 27 double partial sums
 
-// Copies the records of the warp's 32 terms into their slots.  Lane l names its record by
-// `src` (16-byte units) and `parts` (at most kParts, 0 for none); kParts is 8 for 128-byte
-// and 4 for 64-byte dense records.  In pass j the kParts lanes of group q = l / kParts move
-// record j + q * kParts, one 16-byte part each (cp.async, no registers), so every pass reads
-// 32 / kParts whole records.  The caller syncs the warp after.
-template <int kSlotWords, int kParts = 8>
-__device__ __forceinline__ void fetch_records(float *slots, int lane, const float4 *src, int parts) {
+// Staging of term records for the assembly kernels.  A batch holds kTPL records per lane:
+// record r = 32 t + l is lane l's t-th term, at stage + r * kRec (kRec words: a record plus
+// padding that keeps 16-byte accesses by consecutive lanes on distinct banks).  Lane l
+// names its t-th record through locate(t, src, parts): src in 16-byte units and parts at
+// most kParts, 0 for none; kParts is 8 for 128-byte and 4 for 64-byte dense records.  Only
+// the first `groups` groups of 32 are fetched.  In pass j of group t
+// the kParts lanes of q = l / kParts move record 32 t + j + q kParts, one 16-byte part each
+// (cp.async, no registers), so every pass reads 32 / kParts whole records.  Lane l then
+// sums its terms in the order l, 32 + l, 64 + l, ..., the same order for every kTPL.
+template <int C>
+__host__ __device__ constexpr int record_stride() { return C == 3 ? 36 : 20; }
+// Records per lane and batch: as many as fit in 40 KB of staging per block, at most 4.
+__host__ __device__ constexpr int terms_per_lane(int nt, int rec_words) {
+    return (10240 / (nt / 32)) / (32 * rec_words) >= 4 ? 4 : (10240 / (nt / 32)) / (32 * rec_words) >= 2 ? 2 : 1;
+}
+__host__ __device__ constexpr int max_int(int a, int b) { return a > b ? a : b; }
+
+template <int kRec, int kParts, int kTPL, class Locate>
+__device__ __forceinline__ void fetch_records(float *stage, int lane, int groups, Locate locate) {
     static_assert(kParts == 4 || kParts == 8, "64- or 128-byte records");
     const int part = lane & (kParts - 1);
 #pragma unroll
-    for (int j = 0; j < kParts; ++j) {
-        const int r = j + (lane / kParts) * kParts;
-        const float4 *p = reinterpret_cast<const float4 *>(
-            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), r));
-        const int np = __shfl_sync(0xffffffffu, parts, r);
-        if (part < np) {
-            const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(slots + r * kSlotWords + 4 * part));
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(p + part) : "memory");
+    for (int t = 0; t < kTPL; ++t) {
+        if (t >= groups) break;   // warp-uniform: the batch's last groups may be past the list
+        const float4 *src;
+        int parts;
+        locate(t, src, parts);
+#pragma unroll
+        for (int j = 0; j < kParts; ++j) {
+            const int r = j + (lane / kParts) * kParts;
+            const float4 *p = reinterpret_cast<const float4 *>(
+                __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), r));
+            const int np = __shfl_sync(0xffffffffu, parts, r);
+            if (part < np) {
+                const unsigned dst =
+                    static_cast<unsigned>(__cvta_generic_to_shared(stage + (32 * t + r) * kRec + 4 * part));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(p + part) : "memory");
+            }
         }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -444,9 +464,11 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
                                                                      float *sym_blocks, double *diag64, float *jtr,
                                                                      int *err) {
     constexpr bool kCentred = sizeof(DAcc) == 8;   // mixed precision also uses node-centred twists
-    constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;
+    constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;   // per-lane partial sums at the end
     static_assert(27 * sizeof(DAcc) <= 4 * kSlot, "a slot holds one lane's 27 partial sums");
-    __shared__ __align__(16) float stage[NT / 32][32 * kSlot];
+    constexpr int kRec = record_stride<C>();
+    constexpr int kTPL = terms_per_lane(NT, kRec);
+    __shared__ __align__(16) float stage[NT / 32][max_int(kTPL * 32 * kRec, 32 * kSlot)];
     const int lane = threadIdx.x & 31;
     float *slots = stage[threadIdx.x >> 5];
     float *mine = slots + lane * kSlot;
@@ -455,6 +477,8 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total_nodes; g += warps) {
         const uint32_t s = node_scene[g];
+        const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
+        const float4 c4 = centers[g];
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
@@ -462,79 +486,89 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
         const bool motion = lam_n != 0.f && sc.node_motion != nullptr;
         const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)DenseLayout<C>::kFloats * p.dense_begin);
         const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
-        const float4 c4 = centers[g];
         const float3 cen = f3(c4.x, c4.y, c4.z);
-        const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
         DAcc D[21], B[6];
 #pragma unroll
         for (int i = 0; i < 21; ++i) D[i] = DAcc(0);
 #pragma unroll
         for (int i = 0; i < 6; ++i) B[i] = DAcc(0);
-        for (uint32_t base = beg; base < end; base += 32) {
-            const uint32_t it = base + lane;
-            const uint32_t term = it < end ? n2t_val[it] : kInvalidIndex;
+        for (uint32_t base = beg; base < end; base += 32 * kTPL) {
             // 1 dense, 2 regularisation edge, 3 node motion; feature terms have a zero Jacobian
             // (PreconditionerRhsBuilder.cu:214-219)
-            int kind = 0;
-            const float4 *src = nullptr;
-            int parts = 0;
-            if (term < nd) {
-                kind = 1;
-                src = dbase + (size_t)(DenseLayout<C>::kFloats / 4) * term;
-                parts = DenseLayout<C>::kFloats / 4;
-            } else if (term < nd + ne) {
-                kind = 2;
-                src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
-                parts = kRegRecord / 4;
-            } else if (term < nd + ne + nn && motion) {
-                kind = 3;
-            }
-            fetch_records<kSlot, C == 3 ? 8 : 4>(slots, lane, src, parts);
-            __syncwarp();
-            if (kind == 1) {
-                // point-to-plane + optical-flow rows (libs/star/opt/dense_image_jacobian.cuh:9-20)
-                float wk[4];
-                uint32_t ids[4];
-                read_weights<C>(mine, wk, ids);
-                float w = wk[0];   // weight of the last slot whose node is g
-#pragma unroll
-                for (int k = 1; k < 4; ++k) if (ids[k] == g) w = wk[k];
-#pragma unroll
-                for (int ch = 0; ch < C; ++ch) {
-                    float gl[6];
-                    const float res = read_channel<C>(mine, ch, gl);
-                    if (kCentred) recentre(gl, cen);
-                    const float scale = (ch == 0 ? lam_d : lam_of) * w;
-                    accumulate_row(D, B, gl, scale, -(scale * res));
+            auto classify = [&](uint32_t term, const float4 *&src, int &parts) -> int {
+                src = nullptr;
+                parts = 0;
+                if (term < nd) {
+                    src = dbase + (size_t)(DenseLayout<C>::kFloats / 4) * term;
+                    parts = DenseLayout<C>::kFloats / 4;
+                    return 1;
                 }
-            } else if (kind == 2) {
-                // regularisation rows (node_graph_reg_jacobian.cuh:85-106, 193-233)
-                float rec[kRegRecord];
-                read_slot<kRegRecord / 4>(mine, rec);
-                if (rec[7] != 0.f) {
-                    const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
-                    float J[3][6];
-                    reg_unit_jacobian(a3, b3, __float_as_uint(rec[8]) == g, J);
-                    const float scale = lam_r * rec[6];
+                if (term < nd + ne) {
+                    src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
+                    parts = kRegRecord / 4;
+                    return 2;
+                }
+                return (term < nd + ne + nn && motion) ? 3 : 0;
+            };
+            const int groups = (int)min((uint32_t)kTPL, (end - base + 31) / 32);
+            fetch_records<kRec, C == 3 ? 8 : 4, kTPL>(slots, lane, groups, [&](int t, const float4 *&src, int &parts) {
+                const uint32_t it = base + 32 * t + lane;
+                classify(it < end ? n2t_val[it] : kInvalidIndex, src, parts);
+            });
+            __syncwarp();
+#pragma unroll 1
+            for (int t = 0; t < groups; ++t) {
+                const uint32_t it = base + 32 * t + lane;
+                const uint32_t term = it < end ? n2t_val[it] : kInvalidIndex;
+                const float4 *src_unused;
+                int parts_unused;
+                const int kind = classify(term, src_unused, parts_unused);
+                const float *rec_t = slots + (32 * t + lane) * kRec;
+                if (kind == 1) {
+                    // point-to-plane + optical-flow rows (libs/star/opt/dense_image_jacobian.cuh:9-20)
+                    float wk[4];
+                    uint32_t ids[4];
+                    read_weights<C>(rec_t, wk, ids);
+                    float w = wk[0];   // weight of the last slot whose node is g
+#pragma unroll
+                    for (int k = 1; k < 4; ++k) if (ids[k] == g) w = wk[k];
+#pragma unroll
+                    for (int ch = 0; ch < C; ++ch) {
+                        float gl[6];
+                        const float res = read_channel<C>(rec_t, ch, gl);
+                        if (kCentred) recentre(gl, cen);
+                        const float scale = (ch == 0 ? lam_d : lam_of) * w;
+                        accumulate_row(D, B, gl, scale, -(scale * res));
+                    }
+                } else if (kind == 2) {
+                    // regularisation rows (node_graph_reg_jacobian.cuh:85-106, 193-233)
+                    float rec[kRegRecord];
+                    read_slot<kRegRecord / 4>(rec_t, rec);
+                    if (rec[7] != 0.f) {
+                        const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
+                        float J[3][6];
+                        reg_unit_jacobian(a3, b3, __float_as_uint(rec[8]) == g, J);
+                        const float scale = lam_r * rec[6];
+#pragma unroll
+                        for (int ch = 0; ch < 3; ++ch) {
+                            if (kCentred) recentre(J[ch], cen);
+                            accumulate_row(D, B, J[ch], scale, -(scale * rec[10 + ch]));
+                        }
+                    }
+                } else if (kind == 3) {
+                    // node-motion rows (node_motion_jacobian.cuh:7-36), lambda_node = 0 by default
+                    const uint32_t nl = term - nd - ne;
+                    const float4 pred = sc.node_motion[nl];
+                    const SE3f T = dq_se3(load_dq(se3 + 8ull * (sc.node_base + nl)));
+                    const float res3[3] = {T.t.x - pred.x, T.t.y - pred.y, T.t.z - pred.z};
+                    const float scale = lam_n * pred.w;
 #pragma unroll
                     for (int ch = 0; ch < 3; ++ch) {
-                        if (kCentred) recentre(J[ch], cen);
-                        accumulate_row(D, B, J[ch], scale, -(scale * rec[10 + ch]));
+                        float J[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                        J[3 + ch] = 1.f;
+                        if (kCentred) recentre(J, cen);
+                        accumulate_row(D, B, J, scale, -(scale * res3[ch]));
                     }
-                }
-            } else if (kind == 3) {
-                // node-motion rows (node_motion_jacobian.cuh:7-36), lambda_node = 0 by default
-                const uint32_t nl = term - nd - ne;
-                const float4 pred = sc.node_motion[nl];
-                const SE3f T = dq_se3(load_dq(se3 + 8ull * (sc.node_base + nl)));
-                const float res3[3] = {T.t.x - pred.x, T.t.y - pred.y, T.t.z - pred.z};
-                const float scale = lam_n * pred.w;
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    float J[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                    J[3 + ch] = 1.f;
-                    if (kCentred) recentre(J, cen);
-                    accumulate_row(D, B, J, scale, -(scale * res3[ch]));
                 }
             }
             __syncwarp();
@@ -605,10 +639,23 @@ __global__ void __launch_bounds__(128) k_block_inverse(const double *diag64, con
 // (computeDenseImageJtJBlockJacobian, dense_image_jacobian.cuh:82-126; computeRegJtJLocalBlock,
 // node_graph_reg_jacobian.cuh:273-358), stored once per pair; the lower-triangle CSR entry reads
 // it transposed.
-// Each term gives three row pairs (u_i, u_j), the scaled Jacobian rows of the two nodes, and
-// A = sum u_i u_j^T.  Lanes take terms, sum their products in registers, and the 36 entries
-// are then summed over the lanes in lane order through shared memory.
+// A dense term's Jacobian rows for the two nodes are the same gradient g scaled by the
+// nodes' skinning weights, so the dense part of the block is  sum s g_i g_j^T  with
+// s = lambda^2 w_i w_j.  With node-centred twists g_j = S g_i, S = [[I, -[c_j - c_i]x], [0, I]]
+// (g_i, g_j: g centred at the row and column nodes), hence the block is  M S^T  with the
+// symmetric  M = sum s g_i g_i^T.  Lanes take terms and sum the 21 entries of M in registers;
+// the lanes' sums are added in lane order through shared memory, M S^T is formed once per
+// pair, and the pair's smoothness terms (at most one per edge direction) are added last, in
+// list order, by the whole warp.
 // ---------------------------------------------------------------------------
+// v[i] for a run-time i < 6, by selects (no local-memory array).
+__device__ __forceinline__ float pick6(const float *v, int i) {
+    float r = v[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k) r = i == k ? v[k] : r;
+    return r;
+}
+
 __device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, const float *uc, float si, float sj) {
     float a[6], c[6];
 #pragma unroll
@@ -623,22 +670,29 @@ __device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, c
 }
 
 template <int NT, int C>
-__global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
+__global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
     const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
-    const float4 *centers, int centred, float *sym_blocks) {
-    constexpr int kSlot = kSlotWordsF32;
+    const float4 *centers, int centred, float *sym_blocks, int *err) {
+    constexpr int kSlot = kSlotWordsF32;   // per-lane partial sums at the end
     static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
-    __shared__ __align__(16) float stage[NT / 32][32 * kSlot];
+    constexpr int kRec = record_stride<C>();
+    // at most 2 records per lane: the staging then leaves room for 32 warps per SM, which
+    // this latency-bound kernel needs more than deeper batches (pair lists are short)
+    constexpr int kTPL = terms_per_lane(NT, kRec) < 2 ? terms_per_lane(NT, kRec) : 2;
+    constexpr int kStageWords = max_int(kTPL * 32 * kRec, 32 * kSlot);
+    constexpr int kStash = 4;   // smoothness terms per pair: one per edge direction, so at most 2
+    __shared__ __align__(16) float stage[NT / 32][kStageWords + kStash * kRegRecord];
     const int lane = threadIdx.x & 31;
     float *slots = stage[threadIdx.x >> 5];
+    float *stash = slots + kStageWords;   // the pair's smoothness records, in list order
     float *mine = slots + lane * kSlot;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nhalf = counts[kCntHalf];
     for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < nhalf; h += warps) {
         if (slot_up[h] == kInvalidIndex) continue;   // capacity overflow, already flagged
-        const uint32_t row = half_row[h], col = half_col[h];
+        const uint32_t row = half_row[h], col = half_col[h], beg = half_begin[h], end = half_end[h];
         const uint32_t s = node_scene[row];
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
@@ -648,31 +702,58 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
         const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
         const float4 cr4 = centers[row], cc4 = centers[col];
         const float3 c_row = f3(cr4.x, cr4.y, cr4.z), c_col = f3(cc4.x, cc4.y, cc4.z);
-        const uint32_t end = half_end[h];
-        float A[36];
+        float M[21];
 #pragma unroll
-        for (int i = 0; i < 36; ++i) A[i] = 0.f;
-        for (uint32_t base = half_begin[h]; base < end; base += 32) {
-            const uint32_t it = base + lane;
-            const uint32_t term = it < end ? pair_val[it] : kInvalidIndex;
-            int kind = 0;   // 1 dense, 2 regularisation edge; node-motion terms own no pairs
-            const float4 *src = nullptr;
-            int parts = 0;
-            if (term < nd) {
-                kind = 1;
-                src = dbase + (size_t)(DenseLayout<C>::kFloats / 4) * term;
-                parts = DenseLayout<C>::kFloats / 4;
-            } else if (term < nd + ne) {
-                kind = 2;
-                src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
-                parts = kRegRecord / 4;
-            }
-            fetch_records<kSlot, C == 3 ? 8 : 4>(slots, lane, src, parts);
+        for (int i = 0; i < 21; ++i) M[i] = 0.f;
+        int nreg = 0;   // warp-uniform: smoothness records stashed so far
+        for (uint32_t base = beg; base < end; base += 32 * kTPL) {
+            // 1 dense, 2 regularisation edge (stashed, added after the dense sums); node-motion
+            // terms own no pairs
+            auto classify = [&](uint32_t term, const float4 *&src, int &parts) -> int {
+                src = nullptr;
+                parts = 0;
+                if (term < nd) {
+                    src = dbase + (size_t)(DenseLayout<C>::kFloats / 4) * term;
+                    parts = DenseLayout<C>::kFloats / 4;
+                    return 1;
+                }
+                if (term < nd + ne) {
+                    src = rbase + (size_t)(kRegRecord / 4) * (term - nd);
+                    parts = kRegRecord / 4;
+                    return 2;
+                }
+                return 0;
+            };
+            const int groups = (int)min((uint32_t)kTPL, (end - base + 31) / 32);
+            fetch_records<kRec, C == 3 ? 8 : 4, kTPL>(slots, lane, groups, [&](int t, const float4 *&src, int &parts) {
+                const uint32_t it = base + 32 * t + lane;
+                classify(it < end ? pair_val[it] : kInvalidIndex, src, parts);
+            });
             __syncwarp();
-            if (kind == 1) {
+#pragma unroll 1
+            for (int t = 0; t < groups; ++t) {
+                const uint32_t it = base + 32 * t + lane;
+                const float4 *src_unused;
+                int parts_unused;
+                const int kind = classify(it < end ? pair_val[it] : kInvalidIndex, src_unused, parts_unused);
+                const float *rec_t = slots + (32 * t + lane) * kRec;
+                const unsigned regs = __ballot_sync(0xffffffffu, kind == 2);
+                if (kind == 2) {
+                    const int k = nreg + __popc(regs & ((1u << lane) - 1u));
+                    if (k < kStash) {
+#pragma unroll
+                        for (int q = 0; q < kRegRecord / 4; ++q)
+                            reinterpret_cast<float4 *>(stash + kRegRecord * k)[q] =
+                                reinterpret_cast<const float4 *>(rec_t)[q];
+                    } else {
+                        set_err(err, WS_ERR_CAPACITY);
+                    }
+                }
+                nreg += __popc(regs);
+                if (kind != 1) continue;
                 float wk[4];
                 uint32_t ids[4];
-                read_weights<C>(mine, wk, ids);
+                read_weights<C>(rec_t, wk, ids);
                 float wi = wk[0], wj = wk[0];   // last matching slots
 #pragma unroll
                 for (int k = 1; k < 4; ++k) {
@@ -681,48 +762,74 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_pair(
                 }
 #pragma unroll
                 for (int ch = 0; ch < C; ++ch) {
-                    float gr[6], gc[6];
-                    read_channel<C>(mine, ch, gr);
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) gc[q] = gr[q];
-                    if (centred) {
-                        recentre(gr, c_row);
-                        recentre(gc, c_col);
-                    }
+                    float g[6], u[6];
+                    read_channel<C>(rec_t, ch, g);
+                    if (centred) recentre(g, c_row);
                     const float lam = ch == 0 ? lam_d : lam_of;
-                    accumulate_pair_row(A, gr, gc, lam * wi, lam * wj);
-                }
-            } else if (kind == 2) {
-                float rec[kRegRecord];
-                read_slot<kRegRecord / 4>(mine, rec);
-                if (rec[7] != 0.f) {
-                    const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
-                    const uint32_t ei = __float_as_uint(rec[8]);
-                    float Jr[3][6], Jc[3][6];
-                    reg_unit_jacobian(a3, b3, row == ei, Jr);
-                    reg_unit_jacobian(a3, b3, col == ei, Jc);
-                    const float scale = lam_r * rec[6];
+                    const float sc2 = (lam * wi) * (lam * wj);
 #pragma unroll
-                    for (int ch = 0; ch < 3; ++ch) {
-                        if (centred) {
-                            recentre(Jr[ch], c_row);
-                            recentre(Jc[ch], c_col);
-                        }
-                        accumulate_pair_row(A, Jr[ch], Jc[ch], scale, scale);
-                    }
+                    for (int q = 0; q < 6; ++q) u[q] = sc2 * g[q];
+#pragma unroll
+                    for (int i = 0; i < 6; ++i)
+#pragma unroll
+                        for (int j = i; j < 6; ++j) M[tri_index(i, j)] += u[i] * g[j];
                 }
             }
             __syncwarp();
         }
+        // lane sums of M -> slots; lane e < 21 sums entry e over the lanes in lane order
 #pragma unroll
-        for (int i = 0; i < 9; ++i)
-            *reinterpret_cast<float4 *>(mine + 4 * i) = make_float4(A[4 * i], A[4 * i + 1], A[4 * i + 2], A[4 * i + 3]);
+        for (int i = 0; i < 21; ++i) mine[i] = M[i];
         __syncwarp();
-        float acc0 = 0.f, acc1 = 0.f;   // entries lane and 32 + lane (lanes 0..3)
+        float m = 0.f;
+        if (lane < 21) {
 #pragma unroll 8
-        for (int l = 0; l < 32; ++l) {
-            acc0 += slots[l * kSlot + lane];
-            if (lane < 4) acc1 += slots[l * kSlot + 32 + lane];
+            for (int l = 0; l < 32; ++l) m += slots[l * kSlot + lane];
+        }
+        __syncwarp();
+        if (lane < 21) {   // the full symmetric M, row-major, in slots[0, 36)
+            int ea = 0, ec = 0;
+            tri_decode(lane, ea, ec);
+            slots[6 * ea + ec] = m;
+            slots[6 * ec + ea] = m;
+        }
+        __syncwarp();
+        // A = M S^T: A[:, 0:3] = M[:, 0:3] + M[:, 3:6] [c_col - c_row]x, A[:, 3:6] = M[:, 3:6]
+        const float3 dc = f3(c_col.x - c_row.x, c_col.y - c_row.y, c_col.z - c_row.z);
+        auto entry = [&](int e) -> float {
+            const int r = e / 6, c = e % 6;
+            float v = slots[e];
+            if (centred && c < 3) {
+                const float *mr = slots + 6 * r + 3;
+                // column c of [d]x = [[0, -dz, dy], [dz, 0, -dx], [-dy, dx, 0]]
+                const float k0 = c == 0 ? 0.f : (c == 1 ? -dc.z : dc.y);
+                const float k1 = c == 0 ? dc.z : (c == 1 ? 0.f : -dc.x);
+                const float k2 = c == 0 ? -dc.y : (c == 1 ? dc.x : 0.f);
+                v += mr[0] * k0 + mr[1] * k1 + mr[2] * k2;
+            }
+            return v;
+        };
+        float acc0 = entry(lane), acc1 = lane < 4 ? entry(32 + lane) : 0.f;   // entries lane, 32 + lane
+        // smoothness rows (node_graph_reg_jacobian.cuh:85-106, 193-233), in list order
+        const int r0 = lane / 6, c0 = lane % 6, r1 = (32 + lane) / 6, c1 = (32 + lane) % 6;
+        for (int k = 0; k < min(nreg, kStash); ++k) {
+            const float *rec = stash + kRegRecord * k;
+            if (rec[7] == 0.f) continue;   // validity
+            const float3 a3 = f3(rec[0], rec[1], rec[2]), b3 = f3(rec[3], rec[4], rec[5]);
+            const uint32_t ei = __float_as_uint(rec[8]);
+            float Jr[3][6], Jc[3][6];
+            reg_unit_jacobian(a3, b3, row == ei, Jr);
+            reg_unit_jacobian(a3, b3, col == ei, Jc);
+            const float scale = lam_r * rec[6];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                if (centred) {
+                    recentre(Jr[ch], c_row);
+                    recentre(Jc[ch], c_col);
+                }
+                acc0 += (scale * pick6(Jr[ch], r0)) * (scale * pick6(Jc[ch], c0));
+                if (lane < 4) acc1 += (scale * pick6(Jr[ch], r1)) * (scale * pick6(Jc[ch], c1));
+            }
         }
         __syncwarp();
         // item h + row + 1 of the symmetric store: the row's diagonal item and its earlier pairs
@@ -1643,7 +1750,8 @@ template <int NT, int C>
 static void launch_assemble_pair_c(Workspace &w, cudaStream_t st) {
     k_assemble_pair<NT, C><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
-        w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.sym_blocks);
+        w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.sym_blocks,
+        w.error_flag);
 }
 
 template <int NT>
