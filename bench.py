@@ -165,19 +165,30 @@ def measure_spmv(solver, n_nodes, stored, stream, dev, launches=20, warmup=3):
     y = torch.empty_like(x)
     for _ in range(warmup):
         solver.spmv(x, y, stream=stream)
+    torch.cuda.synchronize(dev)
+    # the launches are replayed from a CUDA graph, so the events time the device work and not
+    # the Python call overhead of each product
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        for _ in range(launches):
+            solver.spmv(x, y, stream=stream)
+    with torch.cuda.stream(stream):
+        graph.replay()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
     e0.record(stream)
-    for _ in range(launches):
-        solver.spmv(x, y, stream=stream)
+    with torch.cuda.stream(stream):
+        graph.replay()
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    del graph
     ms = e0.elapsed_time(e1) / launches
     bytes_ = stored * (144 + 4) + n_nodes * (24 + 24) + 4 * (n_nodes + 1)
     peak, kind = measured_peak_hbm()
     gbs = bytes_ / (ms / 1e3) / 1e9
     return {"nodes": n_nodes, "stored_blocks": int(stored), "algorithmic_bytes": int(bytes_), "ms_per_launch": ms,
-            "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak, "peak_kind": kind}
+            "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak, "peak_kind": kind,
+            "exceeds_l2": bool(bytes_ > 126e6), "timing": "CUDA graph of back-to-back launches"}
 
 
 def cpu_solve_rate(sample, threads, precision):
