@@ -1062,10 +1062,10 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 //     memory, where the row's later items, in this chunk or a later one, read it;
 //   * the lane that ends a row sums the row's products in item order, continuing a row
 //     that began in an earlier chunk from a carried partial sum.
-// kPcg: phase A of a PCG iteration: v = d = s + beta d_old (recomputed for every column
+// This is phase A of a PCG iteration: v = d = s + beta d_old (recomputed for every column
 // from the s/d record of the previous iteration), q without its lower part, and per row
 // <d_i, (A d)_i> summed over the row's items as d_i . a, twice for an off-diagonal item
-// (it stands for both orientations).  Otherwise the first pass of y = A x.
+// (it stands for both orientations).
 // Each row's sums run over its items in a fixed order whatever the chunk alignment, so
 // results do not depend on which warp handled the row or on the batch.
 // ---------------------------------------------------------------------------
@@ -1099,19 +1099,17 @@ struct PcgOperands {
 };
 
 // Starts the chunk of items u .. u + 31 (those below u_end): copies of the blocks and of
-// each item's column vector record into `stage`, and (PCG) a register load of beta.  The
-// PCG's vector record is the column's s/d pair (64 B); a plain SpMV's is x of the column
-// (32 B).  The 16-byte parts (9 per block, 4 or 2 per vector record) are spread flat over
-// the lanes, so every copy instruction of the blocks reads 512 contiguous bytes.
-template <bool kPcg>
+// each item's column s/d record (64 B) into `stage`, and a register load of beta.  The
+// 16-byte parts (9 per block, 4 per record) are spread flat over the lanes, so every copy
+// instruction of the blocks reads 512 contiguous bytes.
 __device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_in, uint32_t u, uint32_t u_end, uint4 x,
                                            float *stage, int lane, PcgOperands &op) {
-    constexpr int kVecParts = kPcg ? 4 : 2;
+    constexpr int kVecParts = 4;
     op.item = x;
     const float *vec = nullptr;
     if (x.z != kInvalidIndex) {
-        vec = vec_in + (kPcg ? 16ull : 8ull) * min(x.x, A.total_nodes - 1);
-        if (kPcg) op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
+        vec = vec_in + 16ull * min(x.x, A.total_nodes - 1);
+        op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
     }
     const uint32_t nparts = u < u_end ? 9u * min(32u, u_end - u) : 0u;
     const float *src = A.sym_blocks + 36ull * u;
@@ -1130,7 +1128,6 @@ __device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_i
     cp_async_commit();
 }
 
-template <bool kPcg>
 __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
                              float *out, float *wsm, int lane) {
     if (g0 >= g1) return;
@@ -1141,23 +1138,23 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
     const uint32_t nchunks = u1 > u0 ? (u1 - u0 + 31) / 32 : 0;
     uint4 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
     PcgOperands cur;
-    issue_chunk<kPcg>(A, vec_in, u0, u1, load_item(A.item_info, u0 + lane, u1), stage[0], lane, cur);
+    issue_chunk(A, vec_in, u0, u1, load_item(A.item_info, u0 + lane, u1), stage[0], lane, cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     double carry_dot = 0.0;
     uint32_t carry_row = kInvalidIndex;
     // first rows of groups win .. win + 31 (lane i holds group win + i), reloaded as groups complete
     uint32_t win = g0;
-    uint32_t win_row = (kPcg && g0 + lane < A.total_groups) ? A.group_row[g0 + lane] : A.total_nodes;
+    uint32_t win_row = g0 + lane < A.total_groups ? A.group_row[g0 + lane] : A.total_nodes;
     auto group_first = [&](uint32_t g) -> uint32_t {   // first row of group g (g >= win)
         if (g >= A.total_groups) return A.total_nodes;
         if (g - win < 32) return __shfl_sync(0xffffffffu, win_row, (int)(g - win));
         return A.group_row[g];
     };
-    uint32_t group = g0, group_end = kPcg ? group_first(g0 + 1) : 0u;
+    uint32_t group = g0, group_end = group_first(g0 + 1);
     for (uint32_t j = 0; j < nchunks; ++j) {
         // chunk j + 1 in flight, chunk j + 2 records requested
         PcgOperands next;
-        issue_chunk<kPcg>(A, vec_in, u0 + 32 * (j + 1), u1, nxt, stage[(j + 1) & 1], lane, next);
+        issue_chunk(A, vec_in, u0 + 32 * (j + 1), u1, nxt, stage[(j + 1) & 1], lane, next);
         const uint4 after = load_item(A.item_info, u0 + 32 * (j + 2) + lane, u1);
         cp_async_wait_prior();
         __syncwarp();
@@ -1170,15 +1167,11 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
         if (valid) {
             const float4 s0 = reinterpret_cast<const float4 *>(mine + 36)[0];
             const float2 s1 = reinterpret_cast<const float2 *>(mine + 40)[0];
-            if (kPcg) {
-                const float beta = (float)cur.beta;
-                const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
-                const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
-                vc[0] = s0.x + beta * d0.x; vc[1] = s0.y + beta * d0.y; vc[2] = s0.z + beta * d0.z;
-                vc[3] = s0.w + beta * d0.w; vc[4] = s1.x + beta * d1.x; vc[5] = s1.y + beta * d1.y;
-            } else {
-                vc[0] = s0.x; vc[1] = s0.y; vc[2] = s0.z; vc[3] = s0.w; vc[4] = s1.x; vc[5] = s1.y;
-            }
+            const float beta = (float)cur.beta;
+            const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
+            const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
+            vc[0] = s0.x + beta * d0.x; vc[1] = s0.y + beta * d0.y; vc[2] = s0.z + beta * d0.z;
+            vc[3] = s0.w + beta * d0.w; vc[4] = s1.x + beta * d1.x; vc[5] = s1.y + beta * d1.y;
             if (diag) {
                 float4 *vr = reinterpret_cast<float4 *>(vring + 8 * (xrow & (kPcgRing - 1)));
                 vr[0] = make_float4(vc[0], vc[1], vc[2], vc[3]);
@@ -1210,17 +1203,15 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
                 co[1] = make_float4(t[4], t[5], 0.f, 0.f);
             }
             double dot = 0.0;
-            if (kPcg) {
-                if (A.fp64) {
+            if (A.fp64) {
 #pragma unroll
-                    for (int i = 0; i < 6; ++i) dot += (double)vr[i] * (double)a[i];
-                    if (!diag) dot *= 2.0;
-                } else {
-                    float f = 0.f;
+                for (int i = 0; i < 6; ++i) dot += (double)vr[i] * (double)a[i];
+                if (!diag) dot *= 2.0;
+            } else {
+                float f = 0.f;
 #pragma unroll
-                    for (int i = 0; i < 6; ++i) f += vr[i] * a[i];
-                    dot = (double)(diag ? f : 2.f * f);
-                }
+                for (int i = 0; i < 6; ++i) f += vr[i] * a[i];
+                dot = (double)(diag ? f : 2.f * f);
             }
             float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
             pp[0] = make_float4(a[0], a[1], a[2], a[3]);
@@ -1260,13 +1251,9 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
                 sum[3] += a.w;
                 sum[4] += b.x;
                 sum[5] += b.y;
-                if (kPcg) dsum += reinterpret_cast<const double *>(chunk + kPcgSlot * l + 6)[0];
+                dsum += reinterpret_cast<const double *>(chunk + kPcgSlot * l + 6)[0];
             }
-            if (ends_row && !kPcg) {
-                float4 *yo = reinterpret_cast<float4 *>(out + 8ull * xrow);
-                yo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
-                yo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
-            } else if (ends_row) {
+            if (ends_row) {
                 const float *dn = vring + 8 * (xrow & (kPcgRing - 1));
                 float4 *qo = reinterpret_cast<float4 *>(A.q + 8ull * xrow);
                 float4 *dno = reinterpret_cast<float4 *>(out + 16ull * xrow + 8);
@@ -1287,7 +1274,7 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
         __syncwarp();
         // groups whose rows are all done: their <d, A d> partial, summed in row order
         const uint32_t done_below = cont ? last_row : last_row + 1;
-        while (kPcg && group < g1 && group_end <= done_below) {
+        while (group < g1 && group_end <= done_below) {
             const uint32_t grow = group_first(group);
             double v = 0.0;
             if (grow + lane < group_end) v = gring[(grow + lane) & (kPcgRing - 1)];
@@ -1389,7 +1376,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
         float *sd_new = (it & 1) ? A.sd0 : A.sd1;
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
-        stream_items<true>(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
+        stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
         publish_range(A, g_begin, g_end, 0, lane);
         if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
@@ -1467,19 +1454,121 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 }
 
 // Standalone y = A x over the assembled symmetric store of the last Gauss-Newton iteration
-// (x, y: 8 floats per node), with the PCG's warp ranges and streaming: pass 1 (k_spmv)
-// writes the diagonal and upper part of every row and the transposed contributions;
-// pass 2 (k_spmv_lower) adds each row's contributions.
-__global__ void __launch_bounds__(kPcgThreads, 8) k_spmv(PcgArgs A, const float *x, float *y) {
-    extern __shared__ __align__(16) float pcg_smem[];
+// (x, y: 8 floats per node).  Pass 1 (k_spmv) writes the diagonal and upper part of every
+// row and the transposed contributions; pass 2 (k_spmv_lower) adds each row's contributions.
+// Pass 1 keeps no staging buffers: a warp's blocks are contiguous, so lane l loads item l's
+// block straight into registers (nine 16-byte loads) together with x of the item's column,
+// and the item records are loaded a chunk ahead.  Only the ring of the rows' x and the
+// lanes' products for the row sums sit in shared memory (3 KB per warp), so registers, not
+// shared memory, set the number of warps per SM.  Warp v takes half of PCG range v / 2 (by
+// row groups), so the ranges are the PCG's, at twice the warps.
+constexpr int kSpmvRing = 64;
+constexpr int kSpmvBlocksPerSm = 6;   // twice the PCG's 3 blocks per SM: one wave
+__global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs A, const float *x, float *y) {
+    __shared__ __align__(16) float ring_all[kPcgThreads / 32][kSpmvRing * 8];   // x of recent rows, by row
+    __shared__ __align__(16) float prod_all[kPcgThreads / 32][32 * 8];          // each lane's B x_col
     const int lane = threadIdx.x & 31;
-    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
-    const uint32_t g_begin = min(A.warp_groups[gwarp], A.total_groups);
-    const uint32_t g_end = max(g_begin, min(A.warp_groups[gwarp + 1], A.total_groups));
-    const uint32_t r_begin = g_begin < A.total_groups ? A.group_row[g_begin] : A.total_nodes;
-    const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
-    stream_items<false>(A, g_begin, g_end, r_begin, r_end, x, y, wsm, lane);
+    float *ring = ring_all[threadIdx.x >> 5];
+    float *prod = prod_all[threadIdx.x >> 5];
+    const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t pg0 = min(A.warp_groups[v >> 1], A.total_groups);
+    const uint32_t pg1 = max(pg0, min(A.warp_groups[(v >> 1) + 1], A.total_groups));
+    const uint32_t mid = pg0 + (pg1 - pg0 + 1) / 2;
+    const uint32_t g0 = (v & 1) ? mid : pg0, g1 = (v & 1) ? pg1 : mid;
+    if (g0 >= g1) return;
+    const uint32_t r0 = A.group_row[g0], r1 = g1 < A.total_groups ? A.group_row[g1] : A.total_nodes;
+    const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
+    uint4 nxt = load_item(A.item_info, u0 + lane, u1);
+    float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    uint32_t carry_row = kInvalidIndex;
+    for (uint32_t u = u0; u < u1; u += 32) {
+        const uint4 cur = nxt;
+        nxt = load_item(A.item_info, u + 32 + lane, u1);
+        const bool valid = cur.z != kInvalidIndex;
+        const uint32_t xrow = valid ? min(cur.z, A.total_nodes - 1) : kInvalidIndex;
+        const bool diag = cur.y == kInvalidIndex;
+        float4 b[9];
+        float xc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (valid) {
+            const float4 *src = reinterpret_cast<const float4 *>(A.sym_blocks + 36ull * (u + lane));
+#pragma unroll
+            for (int q = 0; q < 9; ++q) b[q] = __ldcs(src + q);
+            const uint32_t col = min(cur.x, A.total_nodes - 1);
+            const float4 x0 = __ldg(reinterpret_cast<const float4 *>(x + 8ull * col));
+            const float2 x1 = __ldg(reinterpret_cast<const float2 *>(x + 8ull * col + 4));
+            xc[0] = x0.x; xc[1] = x0.y; xc[2] = x0.z; xc[3] = x0.w; xc[4] = x1.x; xc[5] = x1.y;
+            if (diag) {   // a row's first item: publish x of the row for its later items
+                float4 *rr = reinterpret_cast<float4 *>(ring + 8 * (xrow & (kSpmvRing - 1)));
+                rr[0] = x0;
+                rr[1] = make_float4(x1.x, x1.y, 0.f, 0.f);
+            }
+        }
+        __syncwarp();
+        if (valid) {
+            const float4 v0 = reinterpret_cast<const float4 *>(ring + 8 * (xrow & (kSpmvRing - 1)))[0];
+            const float2 v1 = reinterpret_cast<const float2 *>(ring + 8 * (xrow & (kSpmvRing - 1)) + 4)[0];
+            const float vr[6] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y};
+            float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                const float e4[4] = {b[q].x, b[q].y, b[q].z, b[q].w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e = 4 * q + k, r = e / 6, c = e % 6;
+                    a[r] += e4[k] * xc[c];
+                    t[c] += e4[k] * vr[r];
+                }
+            }
+            if (!diag) {
+                float4 *co = reinterpret_cast<float4 *>(A.contrib + 8ull * min(cur.y, A.cap_half - 1));
+                co[0] = make_float4(t[0], t[1], t[2], t[3]);
+                co[1] = make_float4(t[4], t[5], 0.f, 0.f);
+            }
+            reinterpret_cast<float4 *>(prod + 8 * lane)[0] = make_float4(a[0], a[1], a[2], a[3]);
+            reinterpret_cast<float2 *>(prod + 8 * lane + 4)[0] = make_float2(a[4], a[5]);
+        }
+        __syncwarp();
+        // row segments of this chunk, summed in item order by the lane that ends them
+        const uint32_t next_first = __shfl_sync(0xffffffffu, nxt.z, 0);
+        const uint32_t row_up = __shfl_up_sync(0xffffffffu, xrow, 1);
+        const uint32_t row_dn = __shfl_down_sync(0xffffffffu, xrow, 1);
+        const uint32_t following = (lane == 31) ? next_first : row_dn;
+        const bool starts = valid && (lane == 0 || row_up != xrow);
+        const unsigned start_mask = __ballot_sync(0xffffffffu, starts);
+        const unsigned valid_mask = __ballot_sync(0xffffffffu, valid);
+        const int last = 31 - __clz(valid_mask);
+        const bool ends_row = valid && following != xrow;
+        const bool owner = valid && (ends_row || lane == last);
+        float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (owner) {
+            const int first = 31 - __clz(start_mask & (0xffffffffu >> (31 - lane)));
+            if (first == 0 && xrow == carry_row) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) sum[i] = carry[i];
+            }
+#pragma unroll 4
+            for (int l = first; l <= lane; ++l) {
+                const float4 p0 = reinterpret_cast<const float4 *>(prod + 8 * l)[0];
+                const float2 p1 = reinterpret_cast<const float2 *>(prod + 8 * l + 4)[0];
+                sum[0] += p0.x;
+                sum[1] += p0.y;
+                sum[2] += p0.z;
+                sum[3] += p0.w;
+                sum[4] += p1.x;
+                sum[5] += p1.y;
+            }
+            if (ends_row) {
+                float4 *yo = reinterpret_cast<float4 *>(y + 8ull * xrow);
+                yo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
+                yo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
+            }
+        }
+        const bool cont = __shfl_sync(0xffffffffu, owner && !ends_row ? 1 : 0, last) != 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) carry[i] = __shfl_sync(0xffffffffu, sum[i], last);
+        carry_row = cont ? __shfl_sync(0xffffffffu, xrow, last) : kInvalidIndex;
+        __syncwarp();
+    }
 }
 
 __global__ void __launch_bounds__(256) k_spmv_lower(PcgArgs A, float *y) {
@@ -1674,7 +1763,6 @@ int pcg_warps_per_block() { return kPcgThreads / 32; }
 int pcg_max_blocks(int device) {
     int per_sm = 0, sms = 0;
     cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmemBytes);
-    cudaFuncSetAttribute(k_spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPcgSmemBytes);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, kPcgSmemBytes);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per_sm) * std::max(1, sms);
@@ -1830,7 +1918,7 @@ cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *u
 
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st) {
     const PcgArgs a = pcg_args(w, 0);
-    k_spmv<<<pcg_launch_blocks(w), kPcgThreads, kPcgSmemBytes, st>>>(a, x, y);
+    k_spmv<<<2 * pcg_launch_blocks(w), kPcgThreads, 0, st>>>(a, x, y);
     k_spmv_lower<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(a, y);
     return cudaGetLastError();
 }
