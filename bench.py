@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--spmv-replicas", type=int, default=6,
                    help="replicate the scene batch this many times for the >1 GB SpMV measurement; 1 skips it")
+    p.add_argument("--serving-executors", type=int, default=2, help="solver workspaces of the serving run")
     p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the serving run (32 frame streams, 1k-16k nodes); 0 skips it")
     return p.parse_args()
@@ -464,7 +465,7 @@ def main():
         counts = np.exp(srng.uniform(np.log(1000), np.log(16000), 32)).astype(int)
         streams = serving.build_streams(counts, frames=8, seed=args.seed + 4 + 1000 * rank)
         budget = 40e9
-        with serving.Server(memory_budget=int(budget), executors=2, max_batch_scenes=32,
+        with serving.Server(memory_budget=int(budget), executors=args.serving_executors, max_batch_scenes=32,
                             max_batch_nodes=int(counts.sum()) + 1024, max_batch_pixels=32 * 640 * 480,
                             max_batch_edges=int(sum(x.ds.num_edges for x in streams)) + 1024,
                             gn_iters=GN_ITERS, pcg_iters=PCG_ITERS, device=local) as srv:
@@ -472,7 +473,11 @@ def main():
         serving_out = {"streams": 32, "node_counts": "log-uniform [1000, 16000]",
                        "arrivals": "every 33 ms + Exp(5 ms) per stream", "requests": r["requests"],
                        "solved": r["solved"], "solves_per_s": r["solves_per_s"], "p50_ms": r["p50_ms"],
-                       "p99_ms": r["p99_ms"], "mean_batch_scenes": r["mean_batch_scenes"], "executors": 2,
+                       "p99_ms": r["p99_ms"], "mean_batch_scenes": r["mean_batch_scenes"],
+                       "lone_p50_ms": r.get("lone_p50_ms"), "lone_p99_ms": r.get("lone_p99_ms"),
+                       "latency_over_lone_p50": r.get("latency_over_lone_p50"),
+                       "latency_over_lone_p99": r.get("latency_over_lone_p99"),
+                       "executors": args.serving_executors,
                        "budget_gb": budget / 1e9, "executor_gb": r["executor_bytes"] / 1e9,
                        "resident_gb": r["resident_bytes"] / 1e9}
         del streams

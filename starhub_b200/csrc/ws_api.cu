@@ -332,6 +332,13 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
     w.total_tiles = tb;
     w.total_chunks = cb;
     w.node_bits = ws::bits_for(nb);
+    {
+        int max_nodes = 1;
+        for (int s = 0; s < num_scenes; ++s) max_nodes = std::max(max_nodes, hs[s].num_nodes);
+        const int lb = ws::bits_for((uint64_t)max_nodes - 1u), sb = ws::bits_for((uint64_t)num_scenes - 1u);
+        w.pair_local_bits = (sb + 2 * lb <= 32) ? lb : 0;
+        w.pair_key_bits = (sb + 2 * lb <= 32) ? sb + 2 * lb : 0;
+    }
     w.have_inputs = true;
     w.have_solution = false;
     return WS_OK;
@@ -441,7 +448,7 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
     w.last_stream = st;
     const uint64_t key[] = {(uint64_t)gn_iters, (uint64_t)pcg_iters, (uint64_t)w.num_scenes, w.total_nodes,
                             w.total_edges, w.total_tiles, w.total_chunks, (uint64_t)w.node_bits,
-                            (uint64_t)w.dense_channels};
+                            (uint64_t)w.dense_channels, (uint64_t)w.pair_local_bits, (uint64_t)w.pair_key_bits};
     constexpr size_t kKey = sizeof(key) / sizeof(key[0]);
     bool same = w.graph_exec && w.graph_key.size() == kKey && std::equal(key, key + kKey, w.graph_key.begin());
     if (same) {

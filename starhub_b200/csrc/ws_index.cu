@@ -220,10 +220,40 @@ __global__ void k_n2t_offsets(const uint32_t *sorted_keys, const uint32_t *count
     }
 }
 
+// Node-pair sort keys.  Wide form (64-bit): (global row << bits) | global col.  Narrow form
+// (32-bit), used when the scene id and two scene-local ids fit in 32 bits: (scene << 2 bits) |
+// (local row << bits) | local col.  The scenes of a batch hold consecutive global ids, so both
+// forms order the pairs by (global row, global column); the narrow one halves the key bytes
+// and saves radix passes.  A pair's row id is below its column id, so a valid key is never
+// all ones, which marks an unused entry.
+template <class K>
+struct PairKey {
+    int bits;    // global node bits (wide) or scene-local node bits (narrow)
+    K invalid;
+    __device__ __forceinline__ K make(uint32_t scene, uint32_t node_base, uint32_t lo, uint32_t hi) const {
+        if constexpr (sizeof(K) == 8)
+            return ((K)(node_base + lo) << bits) | (K)(node_base + hi);
+        else
+            return ((K)scene << (2 * bits)) | ((K)lo << bits) | (K)hi;
+    }
+    __device__ __forceinline__ void split(K k, const Scene *scenes, uint32_t &row, uint32_t &col) const {
+        const K mask = ((K)1 << bits) - (K)1;
+        if constexpr (sizeof(K) == 8) {
+            row = (uint32_t)(k >> bits);
+            col = (uint32_t)(k & mask);
+        } else {
+            const uint32_t nb = (uint32_t)scenes[k >> (2 * bits)].node_base;
+            row = nb + (uint32_t)((k >> bits) & mask);
+            col = nb + (uint32_t)(k & mask);
+        }
+    }
+};
+
 // computeKVNodePairKNN / buildKeyValuePairKernel (NodePair2TermsIndex.cu:11-92): 6 (i<j) pairs per
 // dense term in i-major order, one per non-self reg edge, feature terms like dense terms.
-__device__ __forceinline__ unsigned long long knn_pair_key(const ushort4 k4, uint32_t q, uint32_t base, int bits,
-                                                            unsigned long long invalid) {
+template <class K>
+__device__ __forceinline__ K knn_pair_key(const ushort4 k4, uint32_t q, uint32_t scene, uint32_t base,
+                                          const PairKey<K> &pk) {
     const uint16_t a[4] = {k4.x, k4.y, k4.z, k4.w};
     uint32_t off = 0;
 #pragma unroll
@@ -231,18 +261,19 @@ __device__ __forceinline__ unsigned long long knn_pair_key(const ushort4 k4, uin
 #pragma unroll
         for (int j = 0; j < 4; ++j)
             if (a[i] < a[j]) {
-                if (off == q) return ((unsigned long long)(base + a[i]) << bits) | (unsigned long long)(base + a[j]);
+                if (off == q) return pk.make(scene, base, a[i], a[j]);
                 ++off;
             }
-    return invalid;
+    return pk.invalid;
 }
 
 // Pair keys and values.  Per scene the entries sit at plan.pair_base as [6 per dense term |
 // 1 per edge | 6 per feature].  The 6 keys of one dense term follow knn_pair_key: slot pairs
 // (i, j) with id_i < id_j, i then j ascending; fewer than 6 when ids repeat, the rest invalid.
+template <class K>
 __global__ void k_pair_kv_dense(const Scene *scenes, const Plan *plan, const uint32_t *counts,
-                                const uint32_t *term_scene, const ushort4 *dense_knn, unsigned long long *keys,
-                                uint32_t *vals, int bits, unsigned long long invalid) {
+                                const uint32_t *term_scene, const ushort4 *dense_knn, K *keys, uint32_t *vals,
+                                PairKey<K> pk) {
     const uint32_t n = counts[kCntDense];
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const uint32_t s = term_scene[t];
@@ -250,13 +281,13 @@ __global__ void k_pair_kv_dense(const Scene *scenes, const Plan *plan, const uin
         const uint32_t lt = t - p.dense_begin, base = p.pair_base + 6u * lt, nb = scenes[s].node_base;
         const ushort4 k4 = dense_knn[t];
         const uint16_t a[4] = {k4.x, k4.y, k4.z, k4.w};
-        unsigned long long out[6] = {invalid, invalid, invalid, invalid, invalid, invalid};
+        K out[6] = {pk.invalid, pk.invalid, pk.invalid, pk.invalid, pk.invalid, pk.invalid};
         int q = 0;
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (a[i] < a[j] && q < 6) out[q++] = ((unsigned long long)(nb + a[i]) << bits) | (unsigned long long)(nb + a[j]);
+                if (a[i] < a[j] && q < 6) out[q++] = pk.make(s, nb, a[i], a[j]);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             keys[base + k] = out[k];
@@ -265,27 +296,27 @@ __global__ void k_pair_kv_dense(const Scene *scenes, const Plan *plan, const uin
     }
 }
 
-__global__ void k_pair_kv_tail(const Scene *scenes, const Plan *plan, unsigned long long *keys, uint32_t *vals,
-                               int bits, unsigned long long invalid, int *err) {
+template <class K>
+__global__ void k_pair_kv_tail(const Scene *scenes, const Plan *plan, K *keys, uint32_t *vals, PairKey<K> pk,
+                               int *err) {
     const Scene &sc = scenes[blockIdx.y];
     const Plan &p = plan[blockIdx.y];
     const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes, nf = sc.num_features;
     const uint32_t len = ne + 6u * nf, base = p.pair_base + 6u * nd;
     for (uint32_t j0 = blockIdx.x * blockDim.x + threadIdx.x; j0 < len; j0 += gridDim.x * blockDim.x) {
         uint32_t j = j0;
-        unsigned long long key;
+        K key;
         uint32_t val;
         if (j < ne) {
             uint16_t x, y;
             edge_ends(sc, j, x, y, err);
             const uint32_t lo = min(x, y), hi = max(x, y);
-            key = (x != y) ? (((unsigned long long)(sc.node_base + lo) << bits) | (unsigned long long)(sc.node_base + hi))
-                           : invalid;
+            key = (x != y) ? pk.make(blockIdx.y, sc.node_base, lo, hi) : pk.invalid;
             val = nd + j;
         } else {
             j -= ne;
             const uint32_t f = j / 6u;
-            key = knn_pair_key(clamp_knn(sc.feature_knn[f], sc, err), j - 6u * f, sc.node_base, bits, invalid);
+            key = knn_pair_key<K>(clamp_knn(sc.feature_knn[f], sc, err), j - 6u * f, blockIdx.y, sc.node_base, pk);
             val = nd + ne + nn + f;
         }
         keys[base + j0] = key;
@@ -296,11 +327,11 @@ __global__ void k_pair_kv_tail(const Scene *scenes, const Plan *plan, unsigned l
 
 // segmentNodePairKernel (NodePair2TermsIndex.cu:94-128): 1 at the first key of every unique pair;
 // also records the number of valid (non-invalid) keys.
-__global__ void k_pair_marks(const unsigned long long *keys, const uint32_t *counts, uint32_t *marks,
-                             unsigned long long invalid, uint32_t *counts_out) {
+template <class K>
+__global__ void k_pair_marks(const K *keys, const uint32_t *counts, uint32_t *marks, K invalid, uint32_t *counts_out) {
     const uint32_t n = counts[kCntPairKV];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const unsigned long long k = keys[i];
+        const K k = keys[i];
         const bool valid = k != invalid;
         marks[i] = (valid && (i == 0 || keys[i - 1] != k)) ? 1u : 0u;
         if (valid && (i + 1 == n || keys[i + 1] == invalid)) counts_out[kCntPairValid] = i + 1;
@@ -310,8 +341,9 @@ __global__ void k_pair_marks(const unsigned long long *keys, const uint32_t *cou
 }
 
 // compactNodePairKeyKernel (NodePair2TermsIndex.cu:130-169): unique pairs and their term ranges.
-__global__ void k_half_fill(const unsigned long long *keys, const uint32_t *head_off,
-                            uint32_t *counts, int bits, uint32_t cap_half, uint32_t *half_row, uint32_t *half_col,
+template <class K>
+__global__ void k_half_fill(const K *keys, const uint32_t *head_off, const Scene *scenes, uint32_t *counts,
+                            PairKey<K> pk, uint32_t cap_half, uint32_t *half_row, uint32_t *half_col,
                             uint32_t *half_begin, uint32_t *half_end, uint32_t *row_cnt_up, uint32_t *row_cnt_lo,
                             int *err) {
     const uint32_t n = counts[kCntPairKV];
@@ -321,13 +353,12 @@ __global__ void k_half_fill(const unsigned long long *keys, const uint32_t *head
         counts[kCntHalf] = min(nhalf, cap_half);
         if (nhalf > cap_half) set_error(err, WS_ERR_CAPACITY);
     }
-    const unsigned long long mask = (1ull << bits) - 1ull;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t h = head_off[i];
         if (head_off[i + 1] == h) continue;        // not the first key of a unique pair
         if (h >= cap_half) continue;
-        const unsigned long long k = keys[i];
-        const uint32_t row = (uint32_t)(k >> bits), col = (uint32_t)(k & mask);
+        uint32_t row, col;
+        pk.split(keys[i], scenes, row, col);
         half_row[h] = row;
         half_col[h] = col;
         half_begin[h] = i;
@@ -438,6 +469,32 @@ static inline int grid_for(uint32_t n, int threads, int num_sms) {
     return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, cap));
 }
 
+// Pair keys and values, their stable sort, and the unique pairs with their term ranges.
+template <class K>
+static void pair_index(Workspace &w, PairKey<K> pk, int key_bits, cudaStream_t st) {
+    const int S = w.num_scenes;
+    K *keys = reinterpret_cast<K *>(w.pair_key), *keys_alt = reinterpret_cast<K *>(w.pair_key_alt);
+    k_pair_kv_dense<K><<<grid_for(w.cap_pixels, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, w.counts, w.d_scene,
+                                                                                w.d_knn, keys, w.pair_val, pk);
+    k_pair_kv_tail<K><<<dim3(16, S), 256, 0, st>>>(w.scenes, w.plan, keys, w.pair_val, pk, w.error_flag);
+    count_launch(w);
+    const bool pair_alt = radix_sort<K>(keys, w.pair_val, keys_alt, w.pair_val_alt, w.counts + kCntPairKV, 0,
+                                        w.cap_pair_kv, key_bits, w.sort_hist, w.sort_digit, st);
+    count_launch(w, 1 + 3 * ((key_bits + 7) / 8));
+    const K *sorted = pair_alt ? keys_alt : keys;
+    w.pair_sorted_val = pair_alt ? w.pair_val_alt : w.pair_val;
+    const int pg = grid_for(w.cap_pair_kv, 256, w.num_sms);
+    k_pair_marks<K><<<pg, 256, 0, st>>>(sorted, w.counts, w.pair_head, pk.invalid, w.counts);
+    exclusive_scan(w.pair_head, w.pair_head, w.counts + kCntPairKV, 0, w.cap_pair_kv, w.scan_tmp, st);
+    // pair_head now holds exclusive offsets; a unique pair starts where two consecutive offsets differ
+    cudaMemsetAsync(w.row_cnt_up, 0, sizeof(uint32_t) * w.cap_nodes, st);
+    cudaMemsetAsync(w.row_cnt_lo, 0, sizeof(uint32_t) * w.cap_nodes, st);
+    k_half_fill<K><<<pg, 256, 0, st>>>(sorted, w.pair_head, w.scenes, w.counts, pk, w.cap_half, w.half_row,
+                                       w.half_col, w.half_begin, w.half_end, w.row_cnt_up, w.row_cnt_lo,
+                                       w.error_flag);
+    count_launch(w, 1 + 3 + 1);
+}
+
 void index_build(Workspace &w, cudaStream_t st) {
     const int S = w.num_scenes;
     const int T = (int)w.total_tiles;
@@ -464,30 +521,15 @@ void index_build(Workspace &w, cudaStream_t st) {
     k_n2t_offsets<<<grid_for(N + 1, 256, w.num_sms), 256, 0, st>>>(w.n2t_sorted_key, w.counts, N, w.n2t_offset);
     count_launch(w);
     // 3. node pair -> term
-    const int pbits = 2 * w.node_bits;
-    const unsigned long long pinvalid = (pbits >= 64) ? ~0ull : ((1ull << pbits) - 1ull);
-    k_pair_kv_dense<<<grid_for(w.cap_pixels, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, w.counts, w.d_scene,
-                                                                             w.d_knn, w.pair_key, w.pair_val,
-                                                                             w.node_bits, pinvalid);
-    k_pair_kv_tail<<<dim3(16, S), 256, 0, st>>>(w.scenes, w.plan, w.pair_key, w.pair_val, w.node_bits, pinvalid,
-                                                w.error_flag);
-    count_launch(w);
-    const bool pair_alt = radix_sort<unsigned long long>(w.pair_key, w.pair_val, w.pair_key_alt, w.pair_val_alt,
-                                                         w.counts + kCntPairKV, 0, w.cap_pair_kv, pbits, w.sort_hist,
-                                                         w.sort_digit, st);
-    count_launch(w, 1 + 3 * ((pbits + 7) / 8));
-    w.pair_sorted_key = pair_alt ? w.pair_key_alt : w.pair_key;
-    w.pair_sorted_val = pair_alt ? w.pair_val_alt : w.pair_val;
-    const int pg = grid_for(w.cap_pair_kv, 256, w.num_sms);
-    k_pair_marks<<<pg, 256, 0, st>>>(w.pair_sorted_key, w.counts, w.pair_head, pinvalid, w.counts);
-    exclusive_scan(w.pair_head, w.pair_head, w.counts + kCntPairKV, 0, w.cap_pair_kv, w.scan_tmp, st);
-    // pair_head now holds exclusive offsets; a unique pair starts where two consecutive offsets differ
-    cudaMemsetAsync(w.row_cnt_up, 0, sizeof(uint32_t) * w.cap_nodes, st);
-    cudaMemsetAsync(w.row_cnt_lo, 0, sizeof(uint32_t) * w.cap_nodes, st);
-    k_half_fill<<<pg, 256, 0, st>>>(w.pair_sorted_key, w.pair_head, w.counts, w.node_bits, w.cap_half,
-                                    w.half_row, w.half_col, w.half_begin, w.half_end, w.row_cnt_up, w.row_cnt_lo,
-                                    w.error_flag);
-    count_launch(w, 1 + 3 + 1);
+    if (w.pair_local_bits > 0) {
+        const int kb = w.pair_key_bits;
+        const uint32_t inv = kb >= 32 ? 0xFFFFFFFFu : ((1u << kb) - 1u);
+        pair_index<uint32_t>(w, PairKey<uint32_t>{w.pair_local_bits, inv}, kb, st);
+    } else {
+        const int kb = 2 * w.node_bits;
+        const unsigned long long inv = kb >= 64 ? ~0ull : ((1ull << kb) - 1ull);
+        pair_index<unsigned long long>(w, PairKey<unsigned long long>{w.node_bits, inv}, kb, st);
+    }
     // 4. block CSR
     k_row_first<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_row, w.counts, w.row_first);
     k_row_len<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.row_cnt_up, w.row_cnt_lo, N, w.rowptr, w.item_ptr);

@@ -34,6 +34,9 @@ struct Workspace {
     int num_scenes = 0;
     uint32_t total_nodes = 0, total_edges = 0, total_tiles = 0, total_chunks = 0, total_features = 0;
     int node_bits = 1;
+    // narrow (32-bit) node-pair sort keys: scene-local id bits, 0 when the batch needs wide keys;
+    // pair_key_bits = scene bits + 2 local bits
+    int pair_local_bits = 0, pair_key_bits = 0;
     std::vector<Scene> h_scenes;
     bool have_inputs = false;
     bool have_solution = false;
@@ -71,7 +74,6 @@ struct Workspace {
     // pair->term
     unsigned long long *pair_key = nullptr, *pair_key_alt = nullptr;   // [cap_pair_kv]
     uint32_t *pair_val = nullptr, *pair_val_alt = nullptr;
-    const unsigned long long *pair_sorted_key = nullptr;
     const uint32_t *pair_sorted_val = nullptr;
     uint32_t *pair_head = nullptr;                           // [cap_pair_kv + 1] marks, then offsets
     uint32_t *half_row = nullptr, *half_col = nullptr;       // [cap_half]

@@ -254,12 +254,29 @@ def build_streams(node_counts, frames: int = 8, seed: int = 4, device: str = "cu
 
 
 def run_streams(server: Server, streams: List[FrameStream], requests: int, period_ms: float = 33.0,
-                jitter_ms: float = 5.0, seed: int = 0) -> dict:
+                jitter_ms: float = 5.0, seed: int = 0, lone: bool = True) -> dict:
     """Frames arrive per stream every period_ms + Exp(jitter_ms); each is submitted at its
     arrival time and solved by the server.  Returns solves/s over the run and latency
-    percentiles (submit -> solved)."""
+    percentiles (submit -> solved).  With `lone`, each stream's frame 0 is first solved alone
+    on the idle server (twice; the second latency counts) and its warp restored, which gives
+    every request a lone-solve latency of its own scene to be compared with."""
     rng = np.random.default_rng(seed)
     ids = [server.add_scene(s.ds) for s in streams]
+    lone_ms = None
+    if lone:
+        lone_ms = []
+        for sid, s in zip(ids, streams):
+            start = server.warp(sid).clone()
+            fr = s.frame(0)
+            t = 0.0
+            for _ in range(2):
+                server.set_warp(sid, start)
+                rid = server.submit(sid, fr.measure_vertex, fr.measure_normal, s.ds.reference_vertex,
+                                    s.ds.reference_normal, s.ds.index_map)
+                t = server.wait(rid)["latency_ms"]
+                server.forget(rid)
+            server.set_warp(sid, start)
+            lone_ms.append(t)
     heap = [(float(rng.exponential(jitter_ms)) + i * period_ms / len(streams), i, 0) for i in range(len(streams))]
     heapq.heapify(heap)
     submitted = []
@@ -273,21 +290,27 @@ def run_streams(server: Server, streams: List[FrameStream], requests: int, perio
         fr = s.frame(k)
         rid = server.submit(ids[i], fr.measure_vertex, fr.measure_normal, s.ds.reference_vertex,
                             s.ds.reference_normal, s.ds.index_map)
-        submitted.append(rid)
+        submitted.append((rid, i))
         heapq.heappush(heap, (t_arr + period_ms + float(rng.exponential(jitter_ms)), i, k + 1))
-    infos = [server.wait(r) for r in submitted]
+    infos = [server.wait(r) for r, _ in submitted]
     t1 = time.perf_counter()
-    for r in submitted:
+    for r, _ in submitted:
         server.forget(r)
     lat = np.array([x["latency_ms"] for x in infos])
     ok = sum(1 for x in infos if x["status"] == WS_OK)
     st = server.stats()
     for sid in ids:
         server.remove_scene(sid)
-    return {"requests": len(infos), "solved": ok, "wall_s": t1 - t0, "solves_per_s": ok / (t1 - t0),
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "mean_batch_scenes": st["mean_batch_scenes"], "batches": st["batches"],
-            "executor_bytes": st["executor_bytes"], "resident_bytes": st["resident_bytes"]}
+    out = {"requests": len(infos), "solved": ok, "wall_s": t1 - t0, "solves_per_s": ok / (t1 - t0),
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "mean_ms": float(lat.mean()), "mean_batch_scenes": st["mean_batch_scenes"], "batches": st["batches"],
+           "executor_bytes": st["executor_bytes"], "resident_bytes": st["resident_bytes"]}
+    if lone_ms is not None:
+        ratio = lat / np.array([lone_ms[i] for _, i in submitted])
+        out.update({"lone_p50_ms": float(np.percentile(lone_ms, 50)), "lone_p99_ms": float(np.percentile(lone_ms, 99)),
+                    "latency_over_lone_p50": float(np.percentile(ratio, 50)),
+                    "latency_over_lone_p99": float(np.percentile(ratio, 99))})
+    return out
 
 
 def main():

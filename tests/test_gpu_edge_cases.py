@@ -12,6 +12,7 @@
 * Counts beyond the 16-bit node ids and beyond the solver's capacities are refused up front.
 * A depth-only scene gets the same result bit for bit with the 64-byte dense records of a
   depth-only batch and with the 128-byte records of a batch that holds a flow scene.
+* A batch that needs 64-bit node-pair sort keys gives each scene its result with 32-bit keys.
 """
 import ctypes as C
 import dataclasses
@@ -146,3 +147,22 @@ def test_depth_only_scene_same_in_a_batch_with_flow(ws, tiny_scene, precision):
     (alone,) = _solve([depth], precision=precision)
     mixed = _solve([flow, depth], precision=precision)
     np.testing.assert_array_equal(mixed[1], alone)
+
+
+def test_wide_pair_keys_give_the_narrow_results(ws, tiny_scene):
+    """Node-pair sort keys are 32-bit (scene, local row, local column) when they fit and 64-bit
+    (global row, global column) otherwise.  65 scenes (7 scene bits) with a 5k-node one (13
+    local bits) need 33 bits, so this batch sorts with 64-bit keys, while each scene alone
+    sorts with 32-bit keys: the results must agree bit for bit."""
+    from starhub_b200 import scenes
+    from starhub_b200.solver import DeviceScene, GpuGeometry
+    big = scenes.make_scene(scenes.spec_for_nodes(5000, scenes.config_spec(2)), GpuGeometry(), seed=77)
+    assert big.num_nodes > 4096
+    b = DeviceScene.from_scene(big)
+    t = DeviceScene.from_scene(tiny_scene)
+    batch = _solve([t] * 64 + [b], gn=2, pcg=5)
+    (solo_b,) = _solve([b], gn=2, pcg=5)
+    (solo_t,) = _solve([t], gn=2, pcg=5)
+    np.testing.assert_array_equal(batch[-1], solo_b)
+    np.testing.assert_array_equal(batch[0], solo_t)
+    np.testing.assert_array_equal(batch[63], solo_t)
