@@ -298,15 +298,17 @@ __device__ void cholesky6_fp64(const double *in, float *out) {
 // term's products in registers; at the end of the list the 27 entries are summed over the
 // lanes in lane order through shared memory.  The order is fixed by the list, so results do
 // not depend on what else is in the batch.
-// DAcc is the accumulator type: float for WS_PREC_FP32 (the reference's FP32 sums),
-// double for WS_PREC_MIXED, where D feeds the FP64 Cholesky directly.
+// Each lane sums its own terms (a few per node) in FP32.  DAcc is the type of the sum over the
+// lanes: float for WS_PREC_FP32 (the reference's FP32 sums), double for WS_PREC_MIXED, where D
+// feeds the FP64 Cholesky directly.  The FP32 lane sums cost about as much accuracy as storing
+// the block in FP32, which the SpMV does anyway, and free the registers that 27 FP64 sums
+// would hold, which lets more warps hide the gathers' latency.
 // ---------------------------------------------------------------------------
 
-// Per-warp staging: 32 slots, one per list entry of the current batch.  A slot holds the
-// term's record (dense 128 B, regularisation 64 B) and, after the list, the lane's partial
-// sums.  Slot strides keep 16-byte accesses by consecutive lanes on distinct banks.
-constexpr int kSlotWordsF32 = 36;   // 144 B: a dense record, or 27 (node) / 36 (pair) partial sums
-constexpr int kSlotWordsF64 = 60;   // 240 B: a dense record, or 27 double partial sums
+// After a list, the lanes' partial sums go through the staging area, one 36-float slot per
+// lane (27 sums for a node, 21 or 36 for a pair); the stride keeps 16-byte accesses by
+// consecutive lanes on distinct banks.
+constexpr int kSlotWordsF32 = 36;
 
 // Staging of term records for the assembly kernels.  A batch holds kTPL records per lane:
 // record r = 32 t + l is lane l's t-th term, at stage + r * kRec (kRec words: a record plus
@@ -455,7 +457,7 @@ __device__ __forceinline__ void accumulate_row(DAcc *D, DAcc *B, const float *ro
 // NT (threads per block) is chosen by the autotuner among 64, 128 and 256; the work of a
 // warp, and so every sum, is the same for all three.
 template <class DAcc, int NT, int C>
-__global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *scenes, const Plan *plan,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_node(const Scene *scenes, const Plan *plan,
                                                                      const uint32_t *node_scene, uint32_t total_nodes,
                                                                      const uint32_t *n2t_offset, const uint32_t *n2t_val,
                                                                      const float *drec, const float *rrec,
@@ -464,10 +466,11 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
                                                                      float *sym_blocks, double *diag64, float *jtr,
                                                                      int *err) {
     constexpr bool kCentred = sizeof(DAcc) == 8;   // mixed precision also uses node-centred twists
-    constexpr int kSlot = kCentred ? kSlotWordsF64 : kSlotWordsF32;   // per-lane partial sums at the end
-    static_assert(27 * sizeof(DAcc) <= 4 * kSlot, "a slot holds one lane's 27 partial sums");
+    constexpr int kSlot = kSlotWordsF32;             // per-lane partial sums at the end (27 floats)
     constexpr int kRec = record_stride<C>();
-    constexpr int kTPL = terms_per_lane(NT, kRec);
+    // at most 2 records per lane and 64 registers: 32 warps per SM, which this latency-bound
+    // kernel needs more than deeper batches
+    constexpr int kTPL = terms_per_lane(NT, kRec) < 2 ? terms_per_lane(NT, kRec) : 2;
     __shared__ __align__(16) float stage[NT / 32][max_int(kTPL * 32 * kRec, 32 * kSlot)];
     const int lane = threadIdx.x & 31;
     float *slots = stage[threadIdx.x >> 5];
@@ -487,11 +490,11 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
         const float4 *dbase = reinterpret_cast<const float4 *>(drec + (size_t)DenseLayout<C>::kFloats * p.dense_begin);
         const float4 *rbase = reinterpret_cast<const float4 *>(rrec + (size_t)kRegRecord * sc.edge_base);
         const float3 cen = f3(c4.x, c4.y, c4.z);
-        DAcc D[21], B[6];
+        float D[21], B[6];
 #pragma unroll
-        for (int i = 0; i < 21; ++i) D[i] = DAcc(0);
+        for (int i = 0; i < 21; ++i) D[i] = 0.f;
 #pragma unroll
-        for (int i = 0; i < 6; ++i) B[i] = DAcc(0);
+        for (int i = 0; i < 6; ++i) B[i] = 0.f;
         for (uint32_t base = beg; base < end; base += 32 * kTPL) {
             // 1 dense, 2 regularisation edge, 3 node motion; feature terms have a zero Jacobian
             // (PreconditionerRhsBuilder.cu:214-219)
@@ -574,16 +577,15 @@ __global__ void __launch_bounds__(NT, 640 / NT) k_assemble_node(const Scene *sce
             __syncwarp();
         }
         // lane partial sums -> slots; lane e sums entry e over the lanes in lane order
-        DAcc *part = reinterpret_cast<DAcc *>(mine);
 #pragma unroll
-        for (int i = 0; i < 21; ++i) part[i] = D[i];
+        for (int i = 0; i < 21; ++i) mine[i] = D[i];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) part[21 + i] = B[i];
+        for (int i = 0; i < 6; ++i) mine[21 + i] = B[i];
         __syncwarp();
         DAcc acc = DAcc(0);
         if (lane < 27) {
 #pragma unroll 8
-            for (int l = 0; l < 32; ++l) acc += reinterpret_cast<const DAcc *>(slots + l * kSlot)[lane];
+            for (int l = 0; l < 32; ++l) acc += DAcc(slots[l * kSlot + lane]);
         }
         __syncwarp();
         if (lane < 21) {
@@ -1810,15 +1812,12 @@ static void launch_assemble_node(Workspace &w, cudaStream_t st) {
     else launch_assemble_node_c<DAcc, NT, 1>(w, st);
 }
 
-// 256 threads of the FP64 node kernel would need 60 KB of static shared memory, so that
-// shape is offered for the FP32 kernel only.
 template <class DAcc>
 static void launch_assemble_node_nt(Workspace &w, int nt, cudaStream_t st) {
     if (nt == 64) {
         launch_assemble_node<DAcc, 64>(w, st);
     } else if (nt == 256) {
-        if constexpr (sizeof(DAcc) == 4) launch_assemble_node<DAcc, 256>(w, st);
-        else launch_assemble_node<DAcc, 128>(w, st);
+        launch_assemble_node<DAcc, 256>(w, st);
     } else {
         launch_assemble_node<DAcc, 128>(w, st);
     }
