@@ -877,7 +877,8 @@ struct PcgArgs {
     double *group_partial;
     double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
     // per scene, kSceneSync words: [0] phase-A tickets, [1] phase-B / init tickets (arrivals of
-    // row groups), [32] alpha generation, [33] delta/beta generation (bumped when published)
+    // row groups, growing during a launch), [32] alpha generation, [33] delta/beta generation
+    // (bumped when published)
     uint32_t *scene_counter;
     uint32_t cap_blocks, cap_half, cap_items, total_nodes, num_scenes;
     int *err;
@@ -963,7 +964,11 @@ __device__ bool wait_scenes(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, 
     return ok;
 }
 
-__device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, int mode, int lane) {
+// `phase` counts the publications of the counter: phase A(it) is phase it of counter 0; init
+// is phase 0 and phase B(it) phase it + 1 of counter 1.  The tickets only grow during a
+// launch, so the arrival that brings them to (phase + 1) times the scene's group count is
+// the last one, and no reset sits between the publications.
+__device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, int mode, int phase, int lane) {
     if (g_begin >= g_end) return;
     __threadfence();   // every lane's vector and partial writes of the phase before the tickets
     __syncwarp();
@@ -983,11 +988,7 @@ __device__ void publish_range(const PcgArgs &A, uint32_t g_begin, uint32_t g_end
             if (lane == 0) {
                 const uint32_t n = (uint32_t)(s1 - s0);
                 const uint32_t ticket = atomicAdd(&A.scene_counter[kSceneSync * scene + ctr], n);
-                last = (ticket + n == (uint32_t)A.scenes[scene].num_chunks) ? 1 : 0;
-                if (last) {
-                    atomicExch(&A.scene_counter[kSceneSync * scene + ctr], 0u);
-                    __threadfence();
-                }
+                last = (ticket + n == (uint32_t)A.scenes[scene].num_chunks * (uint32_t)(phase + 1)) ? 1 : 0;
             }
             if (__shfl_sync(0xffffffffu, last, 0)) reduce_scene(A, scene, mode, lane);
         }
@@ -1371,7 +1372,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         const double part = node_dot_group(A, rv, sv, n.valid);
         if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
     }
-    publish_range(A, g_begin, g_end, 2, lane);
+    publish_range(A, g_begin, g_end, 2, 0, lane);
     if (!wait_scenes(A, g_begin, g_end, 1, 1u, lane)) return;
 
     for (int it = 0; it < A.pcg_iters; ++it) {
@@ -1379,7 +1380,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         float *sd_new = (it & 1) ? A.sd0 : A.sd1;
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
         stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
-        publish_range(A, g_begin, g_end, 0, lane);
+        publish_range(A, g_begin, g_end, 0, it, lane);
         if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
         for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
@@ -1406,7 +1407,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
             const double part = node_dot_group(A, rv, sv, n.valid);
             if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
         }
-        publish_range(A, g_begin, g_end, 1, lane);
+        publish_range(A, g_begin, g_end, 1, it + 1, lane);
         if (it + 1 < A.pcg_iters && !wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 2u, lane)) return;
     }
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
