@@ -1350,15 +1350,23 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
-    // this warp's contiguous range of row groups (balanced by slot count) and their rows
+    // phase A: this warp's contiguous range of row groups, balanced by stored blocks
     const uint32_t g_begin = min(A.warp_groups[gwarp], A.total_groups);
     const uint32_t g_end = max(g_begin, min(A.warp_groups[gwarp + 1], A.total_groups));
     const uint32_t r_begin = g_begin < A.total_groups ? A.group_row[g_begin] : A.total_nodes;
     const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
+    // init, phase B and the twist update work per row, so they take an equal number of groups
+    // per warp instead; every phase reads what others wrote only after a wait for all the groups
+    // of the scene, so the two partitions need not agree
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t b_begin = (uint32_t)((unsigned long long)A.total_groups * gwarp / nwarps);
+    const uint32_t b_end = (uint32_t)((unsigned long long)A.total_groups * (gwarp + 1) / nwarps);
+    const uint32_t br_begin = b_begin < A.total_groups ? A.group_row[b_begin] : A.total_nodes;
+    const uint32_t br_end = b_end < A.total_groups ? A.group_row[b_end] : A.total_nodes;
 
     // ---- init: r = b, s = M^-1 b, x = 0, d = 0, delta = <r, s> ----
-    for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
-        const NodeStep n = node_step(A, g, g_end, lane);
+    for (uint32_t g = b_begin; g < b_end; g += kGroupsPerStep) {
+        const NodeStep n = node_step(A, g, b_end, lane);
         float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (n.valid) {
             const float zero[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1372,7 +1380,7 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         const double part = node_dot_group(A, rv, sv, n.valid);
         if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
     }
-    publish_range(A, g_begin, g_end, 2, 0, lane);
+    publish_range(A, b_begin, b_end, 2, 0, lane);
     if (!wait_scenes(A, g_begin, g_end, 1, 1u, lane)) return;
 
     for (int it = 0; it < A.pcg_iters; ++it) {
@@ -1381,10 +1389,10 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         // ---- phase A: d = s + beta d, q = A d, <d, q> ----
         stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
         publish_range(A, g_begin, g_end, 0, it, lane);
-        if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
+        if (!wait_scenes(A, b_begin, b_end, 0, (uint32_t)it + 1u, lane)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
-        for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
-            const NodeStep n = node_step(A, g, g_end, lane);
+        for (uint32_t g = b_begin; g < b_end; g += kGroupsPerStep) {
+            const NodeStep n = node_step(A, g, b_end, lane);
             float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             if (n.valid) {
                 const float alpha = (float)__ldcg(A.scalars + 8ull * n.scene + 1);
@@ -1407,12 +1415,12 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
             const double part = node_dot_group(A, rv, sv, n.valid);
             if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
         }
-        publish_range(A, g_begin, g_end, 1, it + 1, lane);
+        publish_range(A, b_begin, b_end, 1, it + 1, lane);
         if (it + 1 < A.pcg_iters && !wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 2u, lane)) return;
     }
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
     //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
-    for (uint32_t row = r_begin + lane; row < r_end; row += 32) {
+    for (uint32_t row = br_begin + lane; row < br_end; row += 32) {
         float xv[6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) xv[c] = ldcg(A.x + 8ull * row + c);
