@@ -189,6 +189,17 @@ int ws_splat_maps(const float *verts, const float *attr_verts, const float *attr
                   int num_verts, int width, int height, float fx, float fy, float cx, float cy,
                   int footprint, uint32_t *index_map, float *vertex_map, float *normal_map,
                   void *stream);
+/* Measurement maps from a depth image in millimetres (device, `pitch` elements per row):
+ * createVertexConfidMapKernel (libs/star/img_proc/vertex_map.cu:13-33), the depth clip of
+ * filterAndScaleVertexKernel (libs/star/geometry/geometry_map/SurfelMapInitializer.cu:107-137,
+ * here on the depth in metres at full resolution) and createNormalRadiusMapKernel with eigen33
+ * (libs/star/img_proc/normal_map.cu:32-118, libs/star/math/eigen33.hpp).  Writes width*height
+ * float4 texels of each output: vertex_confid = (x, y, z, 1), or zeros outside the clip;
+ * normal_radius = (normal facing the camera, radius in mm), or zeros where fewer than half of
+ * the 7x7 window holds vertices. */
+int ws_measure_maps(const uint16_t *depth_mm, int width, int height, int pitch, float fx, float fy,
+                    float cx, float cy, float clip_near, float clip_far, float radius_scale,
+                    float *vertex_confid, float *normal_radius, void *stream);
 
 /* ---- Measurement hooks ---- */
 

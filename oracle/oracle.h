@@ -118,6 +118,15 @@ int orc_solve(const orc_problem *p, const orc_settings *s, float *out_dq, orc_de
 int orc_forward_warp(const float *node_dq, int n_nodes, const float *verts4, int n_verts,
                      const uint16_t *knn, const float *sw, const float *cw, float *out4, int threads);
 
+/* Measurement maps from a depth image in millimetres: createVertexConfidMapKernel
+ * (img_proc/vertex_map.cu:13-33), the clip of filterAndScaleVertexKernel
+ * (geometry_map/SurfelMapInitializer.cu:107-137, on the depth in metres) and
+ * createNormalRadiusMapKernel with eigen33 (img_proc/normal_map.cu:32-118, math/eigen33.hpp),
+ * in FP32 with the reference's host arithmetic (1 / sqrt for the inverse square roots).
+ * Outputs width*height float4 each. */
+int orc_measure_maps(const uint16_t *depth_mm, int width, int height, float fx, float fy, float cx, float cy,
+                     float clip_near, float clip_far, float radius_scale, float *vertex4, float *normal4);
+
 #ifdef __cplusplus
 }
 #endif

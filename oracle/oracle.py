@@ -307,6 +307,19 @@ def binblock_csr(n_nodes, sym_rows, sym_cols):
     return rp[: n_rp.value], col
 
 
+def measure_maps(depth_mm, fx, fy, cx, cy, clip_near=0.1, clip_far=3.0, radius_scale=1.0):
+    """orc_measure_maps: vertex and normal/radius maps, two (H, W, 4) float32 arrays."""
+    d = _c(depth_mm, np.uint16)
+    h, w = d.shape
+    vert = np.zeros((h, w, 4), np.float32)
+    nrm = np.zeros((h, w, 4), np.float32)
+    rc = lib().orc_measure_maps(_p(d), C.c_int(w), C.c_int(h), C.c_float(fx), C.c_float(fy), C.c_float(cx),
+                                C.c_float(cy), C.c_float(clip_near), C.c_float(clip_far), C.c_float(radius_scale),
+                                _p(vert), _p(nrm))
+    assert rc == 0
+    return vert, nrm
+
+
 def forward_warp(dq, verts, knn, sw, cw, threads=0):
     d = _c(dq, np.float32)
     v = _c(verts, np.float32)

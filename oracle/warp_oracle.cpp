@@ -1318,4 +1318,193 @@ int orc_forward_warp(const float *node_dq, int n_nodes, const float *verts4, int
     return 0;
 }
 
+/* ---- measurement maps (img_proc/vertex_map.cu, img_proc/normal_map.cu, math/eigen33.hpp) ---- */
+namespace meas {
+struct P3 {
+    float x, y, z;
+};
+static inline P3 p3(float x, float y, float z) { return P3{x, y, z}; }
+static inline P3 pcross(P3 a, P3 b) { return p3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline float pdot(P3 a, P3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline P3 pmul(P3 a, float s) { return p3(a.x * s, a.y * s, a.z * s); }
+static inline float inv_sqrt(float v) { return 1.0f / sqrtf(v); }   // eigen33.h host branch
+static const float kEps = 1.192092896e-07f;                          // numeric_limits.hpp:30-32
+static const float kMinPos = 1.175494351e-38f;                       // numeric_limits.hpp:35-37
+
+static inline bool is_zero(P3 v) {   // vector_ops.hpp:123-126
+    return fabsf(v.x) < 1e-3f && fabsf(v.y) < 1e-3f && fabsf(v.z) < 1e-3f;
+}
+// eigen33::compute_root2 (eigen33.hpp:6-17)
+static void root2(float b, float c, P3 &r) {
+    r.x = 0.0f;
+    float d = b * b - 4.f * c;
+    if (d < 0.f) d = 0.f;
+    const float sd = sqrtf(d);
+    r.z = 0.5f * (b + sd);
+    r.y = 0.5f * (b - sd);
+}
+// eigen33::compute_root3 (eigen33.hpp:50-98)
+static void root3(float c0, float c1, float c2, P3 &r) {
+    if (fabsf(c0) < kEps) {
+        root2(c2, c1, r);
+        return;
+    }
+    const float inv3 = 1.f / 3.f, sq3 = sqrtf(3.f);
+    const float c2o3 = c2 * inv3;
+    float ao3 = (c1 - c2 * c2o3) * inv3;
+    if (ao3 > 0.f) ao3 = 0.f;
+    const float hb = 0.5f * (c0 + c2o3 * (2.f * c2o3 * c2o3 - c1));
+    float q = hb * hb + ao3 * ao3 * ao3;
+    if (q > 0.f) q = 0.f;
+    const float rho = sqrtf(-ao3);
+    const float th = atan2f(sqrtf(-q), hb) * inv3;
+    const float ct = cosf(th), st = sinf(th);
+    r.x = c2o3 + 2.f * rho * ct;
+    r.y = c2o3 - rho * (ct + sq3 * st);
+    r.z = c2o3 - rho * (ct - sq3 * st);
+    if (r.x >= r.y) std::swap(r.x, r.y);
+    if (r.y >= r.z) {
+        std::swap(r.y, r.z);
+        if (r.x >= r.y) std::swap(r.x, r.y);
+    }
+    if (r.x <= 0.0f) root2(c2, c1, r);
+}
+// eigen33::unit_orthogonal (eigen33.hpp:19-48)
+static P3 unit_orth(P3 s) {
+    const float pe = kEps * kEps;
+    const bool xs = s.x * s.x <= pe * s.z * s.z, ys = s.y * s.y <= pe * s.z * s.z;
+    if (!xs || !ys) {
+        const float inv = inv_sqrt(s.x * s.x + s.y * s.y);
+        return p3(-s.y * inv, s.x * inv, 0.0f);
+    }
+    const float inv = inv_sqrt(s.z * s.z + s.y * s.y);
+    return p3(0.0f, -s.z * inv, s.y * inv);
+}
+// the longest of the cross products of the rows of (M - lambda I), normalised
+static P3 best_cross(const P3 rows[3], float lambda, float &len) {
+    P3 a = rows[0], b = rows[1], c = rows[2];
+    a.x -= lambda;
+    b.y -= lambda;
+    c.z -= lambda;
+    const P3 v0 = pcross(a, b), v1 = pcross(a, c), v2 = pcross(b, c);
+    const float l0 = pdot(v0, v0), l1 = pdot(v1, v1), l2 = pdot(v2, v2);
+    if (l0 >= l1 && l0 >= l2) { len = l0; return pmul(v0, inv_sqrt(l0)); }
+    if (l1 >= l0 && l1 >= l2) { len = l1; return pmul(v1, inv_sqrt(l1)); }
+    len = l2;
+    return pmul(v2, inv_sqrt(l2));
+}
+// eigen33::compute (eigen33.hpp:100-320), returning evecs[0]
+static P3 min_eigenvector(float m[6]) {
+    const float scale1 = std::max(std::max(std::max(fabsf(m[0]), fabsf(m[1])), std::max(fabsf(m[2]), fabsf(m[3]))),
+                                  std::max(fabsf(m[4]), fabsf(m[5])));
+    const float scale = scale1 <= kMinPos ? 1.f : scale1;
+    for (int i = 0; i < 6; ++i) m[i] /= scale;
+    const float a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5];   // [a b c; b d e; c e f]
+    const float c0 = a * d * f + 2.f * b * c * e - a * e * e - d * c * c - f * b * b;
+    const float c1 = a * d - b * b + a * f - c * c + d * f - e * e;
+    const float c2 = a + d + f;
+    P3 ev;
+    root3(c0, c1, c2, ev);
+    const P3 rows[3] = {p3(a, b, c), p3(b, d, e), p3(c, e, f)};
+    float len;
+    if (ev.z - ev.x <= kEps) return p3(1.f, 0.f, 0.f);
+    if (ev.y - ev.x <= kEps) {
+        const P3 e2 = best_cross(rows, ev.z, len);
+        const P3 e1 = unit_orth(e2);
+        return pcross(e1, e2);
+    }
+    if (ev.z - ev.y <= kEps) return best_cross(rows, ev.x, len);
+    P3 vec[3];
+    float mmax[3];
+    vec[2] = best_cross(rows, ev.z, mmax[2]);
+    int lo = 2, hi = 2;
+    vec[1] = best_cross(rows, ev.y, mmax[1]);
+    if (mmax[1] <= mmax[lo]) lo = 1;
+    if (mmax[1] > mmax[hi]) hi = 1;
+    vec[0] = best_cross(rows, ev.x, mmax[0]);
+    {   // the reference tests the length of the third cross product here, whichever was longest
+        P3 rb = rows[1], rc = rows[2];
+        rb.y -= ev.x;
+        rc.z -= ev.x;
+        const P3 w = pcross(rb, rc);
+        const float l3 = pdot(w, w);
+        if (l3 <= mmax[lo]) lo = 0;
+        if (l3 > mmax[hi]) hi = 0;
+    }
+    const int mid = 3 - lo - hi;
+    P3 t = pcross(vec[(lo + 1) % 3], vec[(lo + 2) % 3]);
+    vec[lo] = pmul(t, inv_sqrt(pdot(t, t)));
+    t = pcross(vec[(mid + 1) % 3], vec[(mid + 2) % 3]);
+    vec[mid] = pmul(t, inv_sqrt(pdot(t, t)));
+    return vec[0];
+}
+}  // namespace meas
+
+int orc_measure_maps(const uint16_t *depth_mm, int width, int height, float fx, float fy, float cx, float cy,
+                     float clip_near, float clip_far, float radius_scale, float *vertex4, float *normal4) {
+    using namespace meas;
+    if (!depth_mm || !vertex4 || !normal4 || width <= 0 || height <= 0) return -1;
+    const float ifx = 1.0f / fx, ify = 1.0f / fy;
+    std::vector<P3> vert((size_t)width * height);
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            const size_t i = (size_t)y * width + x;
+            const float z = float(depth_mm[i]) / (1000.f);
+            const bool kept = !(z > clip_far || z < clip_near);
+            vert[i] = kept ? p3((float(x) - cx) * ifx * z, (float(y) - cy) * ify * z, z) : p3(0.f, 0.f, 0.f);
+            vertex4[4 * i] = vert[i].x;
+            vertex4[4 * i + 1] = vert[i].y;
+            vertex4[4 * i + 2] = vert[i].z;
+            vertex4[4 * i + 3] = kept ? 1.f : 0.f;
+        }
+    auto at = [&](int x, int y) -> P3 {   // border texels read as zero
+        if (x < 0 || y < 0 || x >= width || y >= height) return p3(0.f, 0.f, 0.f);
+        return vert[(size_t)y * width + x];
+    };
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            float *out = normal4 + 4 * ((size_t)y * width + x);
+            out[0] = out[1] = out[2] = out[3] = 0.f;
+            const P3 c = at(x, y);
+            if (is_zero(c)) continue;
+            P3 cen = p3(0.f, 0.f, 0.f);
+            int count = 0;
+            for (int cy2 = y - 3; cy2 <= y + 3; ++cy2)
+                for (int cx2 = x - 3; cx2 <= x + 3; ++cx2) {
+                    const P3 p = at(cx2, cy2);
+                    if (!is_zero(p)) {
+                        cen.x += p.x;
+                        cen.y += p.y;
+                        cen.z += p.z;
+                        ++count;
+                    }
+                }
+            if (count <= 24) continue;
+            cen = pmul(cen, 1.0f / count);
+            float cov[6] = {0, 0, 0, 0, 0, 0};
+            for (int cy2 = y - 3; cy2 < y + 3; ++cy2)      // the reference's loops end one short
+                for (int cx2 = x - 3; cx2 < x + 3; ++cx2) {
+                    const P3 p = at(cx2, cy2);
+                    if (!is_zero(p)) {
+                        const P3 dd = p3(p.x - cen.x, p.y - cen.y, p.z - cen.z);
+                        cov[0] += dd.x * dd.x;
+                        cov[1] += dd.x * dd.y;
+                        cov[2] += dd.x * dd.z;
+                        cov[3] += dd.y * dd.y;
+                        cov[4] += dd.y * dd.z;
+                        cov[5] += dd.z * dd.z;
+                    }
+                }
+            P3 n = min_eigenvector(cov);
+            if (pdot(n, c) >= 0.0f) n = pmul(n, -1.f);
+            const float radius = c.z * (1000 * 1.414f / 570.0f) * radius_scale;   // compute_radius, normal_map.cu:10-23
+            const float nz = fabsf(n.z);
+            out[0] = n.x;
+            out[1] = n.y;
+            out[2] = n.z;
+            out[3] = nz > 0.5f ? radius / nz : 2.0f * radius;
+        }
+    return 0;
+}
+
 }  // extern "C"

@@ -31,7 +31,7 @@ EXPORTED = [
     "ws_default_penalties", "ws_create", "ws_destroy", "ws_set_inputs", "ws_set_batch", "ws_solve",
     "ws_solve_graph", "ws_sync_status", "ws_get_solution", "ws_get_counts", "ws_get_dense_terms",
     "ws_get_node2term", "ws_get_node_pairs", "ws_get_system", "ws_get_dense_jacobian", "ws_init_nodes",
-    "ws_build_node_graph", "ws_skinning", "ws_forward_warp", "ws_splat_maps", "ws_version",
+    "ws_build_node_graph", "ws_skinning", "ws_forward_warp", "ws_splat_maps", "ws_measure_maps", "ws_version",
     "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
     "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
     "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
@@ -149,6 +149,7 @@ def load() -> C.CDLL:
         "ws_build_node_graph": (i, [vp, i, i, f, vp, vp, vp, vp]),
         "ws_skinning": (i, [vp, i, vp, i, f, vp, vp, vp, vp]),
         "ws_forward_warp": (i, [vp, i, vp, vp, i, vp, vp, vp, vp, vp, vp]),
+        "ws_measure_maps": (i, [vp, i, i, i, f, f, f, f, f, f, f, vp, vp, vp]),
         "ws_splat_maps": (i, [vp, vp, vp, i, i, i, f, f, f, f, i, vp, vp, vp, vp]),
         "ws_splat_maps_noalloc": (i, [vp, vp, vp, i, i, i, f, f, f, f, i, vp, vp, vp, vp]),
         "ws_version": (i, []),

@@ -18,7 +18,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libwarpsolve.so"
-SOURCES = ["ws_api.cu", "ws_index.cu", "ws_solve.cu", "ws_graph.cu", "ws_server.cu"]
+SOURCES = ["ws_api.cu", "ws_index.cu", "ws_solve.cu", "ws_graph.cu", "ws_server.cu", "ws_measure.cu"]
+# The measurement maps keep every multiply and add separately rounded, as the host restatement
+# of their eigen solver does: its branches test quantities against the FP32 epsilon.
+FILE_FLAGS = {"ws_measure.cu": ["--fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-pthread",
          "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
@@ -46,7 +49,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         src = CSRC / s
         obj = BUILD / (s + ".o")
         if force or _stale(obj, src):
-            jobs.append([cc, *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)])
+            jobs.append([cc, *ARCH, *FLAGS, *FILE_FLAGS.get(s, []), "-c", str(src), "-o", str(obj)])
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

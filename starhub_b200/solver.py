@@ -375,6 +375,17 @@ class GpuGeometry:
                                        _ptr(ov), _ptr(on), self._stream()), "ws_forward_warp")
         return ov.cpu().numpy(), (on.cpu().numpy() if on is not None else None)
 
+    def measure_maps(self, depth_mm, cam, clip_near=0.1, clip_far=3.0, radius_scale=1.0):
+        """Vertex and normal/radius maps of a depth image in millimetres (ws_measure_maps);
+        returns two (height, width, 4) float32 arrays."""
+        d = _dev(np.ascontiguousarray(depth_mm).view(np.int16), self.device)
+        vert = torch.empty((cam.height, cam.width, 4), dtype=torch.float32, device=self.device)
+        nrm = torch.empty_like(vert)
+        check(self.lib.ws_measure_maps(_ptr(d), cam.width, cam.height, cam.width, cam.fx, cam.fy, cam.cx, cam.cy,
+                                       clip_near, clip_far, radius_scale, _ptr(vert), _ptr(nrm), self._stream()),
+              "ws_measure_maps")
+        return vert.cpu().numpy(), nrm.cpu().numpy()
+
     def splat(self, verts, cam, footprint):
         v = _dev(verts, self.device, torch.float32)
         idx = torch.empty((cam.height, cam.width), dtype=torch.int32, device=self.device)
