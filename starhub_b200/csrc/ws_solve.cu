@@ -1467,18 +1467,40 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 // Standalone y = A x over the assembled symmetric store of the last Gauss-Newton iteration
 // (x, y: 8 floats per node).  Pass 1 (k_spmv) writes the diagonal and upper part of every
 // row and the transposed contributions; pass 2 (k_spmv_lower) adds each row's contributions.
-// Pass 1 keeps no staging buffers: a warp's blocks are contiguous, so lane l loads item l's
-// block straight into registers (nine 16-byte loads) together with x of the item's column,
-// and the item records are loaded a chunk ahead.  Only the ring of the rows' x and the
-// lanes' products for the row sums sit in shared memory (3 KB per warp), so registers, not
-// shared memory, set the number of warps per SM.  Warp v takes half of PCG range v / 2 (by
-// row groups), so the ranges are the PCG's, at twice the warps.
+// Pass 1 streams a warp's contiguous blocks through one 4.6 KB shared-memory buffer: the
+// chunk's blocks arrive with cp.async (every copy instruction moves 512 contiguous bytes),
+// each lane moves its item's block into registers, and the buffer at once takes the next
+// chunk's copies, which then overlap the current chunk's arithmetic.  x of the items'
+// columns is loaded a chunk ahead into registers, the item records two chunks ahead.  With
+// 7 KB of shared memory per warp, registers set the number of warps per SM.  Warp v takes
+// half of PCG range v / 2 (by row groups), so the ranges are the PCG's, at twice the warps.
 constexpr int kSpmvRing = 64;
 constexpr int kSpmvBlocksPerSm = 6;   // twice the PCG's 3 blocks per SM: one wave
+__device__ __forceinline__ void spmv_issue_blocks(const PcgArgs &A, uint32_t u, uint32_t u_end, float *buf, int lane) {
+    const uint32_t nparts = u < u_end ? 9u * min(32u, u_end - u) : 0u;
+    const float *src = A.sym_blocks + 36ull * u;
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const uint32_t part = 32u * p + lane;
+        if (part < nparts) cp_async16(buf + 4 * part, src + 4ull * part);
+    }
+    cp_async_commit();
+}
+__device__ __forceinline__ void spmv_load_x(const PcgArgs &A, const float *x, uint4 it, float4 &x0, float2 &x1) {
+    x0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    x1 = make_float2(0.f, 0.f);
+    if (it.z != kInvalidIndex) {
+        const uint32_t col = min(it.x, A.total_nodes - 1);
+        x0 = __ldg(reinterpret_cast<const float4 *>(x + 8ull * col));
+        x1 = __ldg(reinterpret_cast<const float2 *>(x + 8ull * col + 4));
+    }
+}
 __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs A, const float *x, float *y) {
+    __shared__ __align__(16) float buf_all[kPcgThreads / 32][32 * 36];          // the chunk's blocks
     __shared__ __align__(16) float ring_all[kPcgThreads / 32][kSpmvRing * 8];   // x of recent rows, by row
     __shared__ __align__(16) float prod_all[kPcgThreads / 32][32 * 8];          // each lane's B x_col
     const int lane = threadIdx.x & 31;
+    float *buf = buf_all[threadIdx.x >> 5];
     float *ring = ring_all[threadIdx.x >> 5];
     float *prod = prod_all[threadIdx.x >> 5];
     const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1489,37 +1511,40 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     if (g0 >= g1) return;
     const uint32_t r0 = A.group_row[g0], r1 = g1 < A.total_groups ? A.group_row[g1] : A.total_nodes;
     const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
-    uint4 nxt = load_item(A.item_info, u0 + lane, u1);
+    uint4 cur = load_item(A.item_info, u0 + lane, u1);
+    uint4 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
+    float4 xa;
+    float2 xb;
+    spmv_load_x(A, x, cur, xa, xb);
+    spmv_issue_blocks(A, u0, u1, buf, lane);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
     for (uint32_t u = u0; u < u1; u += 32) {
-        const uint4 cur = nxt;
-        nxt = load_item(A.item_info, u + 32 + lane, u1);
+        const uint4 after = load_item(A.item_info, u + 64 + lane, u1);
         const bool valid = cur.z != kInvalidIndex;
         const uint32_t xrow = valid ? min(cur.z, A.total_nodes - 1) : kInvalidIndex;
         const bool diag = cur.y == kInvalidIndex;
-        float4 b[9];
-        float xc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (valid) {
-            const float4 *src = reinterpret_cast<const float4 *>(A.sym_blocks + 36ull * (u + lane));
-#pragma unroll
-            for (int q = 0; q < 9; ++q) b[q] = __ldcs(src + q);
-            const uint32_t col = min(cur.x, A.total_nodes - 1);
-            const float4 x0 = __ldg(reinterpret_cast<const float4 *>(x + 8ull * col));
-            const float2 x1 = __ldg(reinterpret_cast<const float2 *>(x + 8ull * col + 4));
-            xc[0] = x0.x; xc[1] = x0.y; xc[2] = x0.z; xc[3] = x0.w; xc[4] = x1.x; xc[5] = x1.y;
-            if (diag) {   // a row's first item: publish x of the row for its later items
-                float4 *rr = reinterpret_cast<float4 *>(ring + 8 * (xrow & (kSpmvRing - 1)));
-                rr[0] = x0;
-                rr[1] = make_float4(x1.x, x1.y, 0.f, 0.f);
-            }
+        const float xc[6] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y};
+        if (valid && diag) {   // a row's first item: publish x of the row for its later items
+            float4 *rr = reinterpret_cast<float4 *>(ring + 8 * (xrow & (kSpmvRing - 1)));
+            rr[0] = xa;
+            rr[1] = make_float4(xb.x, xb.y, 0.f, 0.f);
         }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncwarp();
+        float4 b[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) b[q] = reinterpret_cast<const float4 *>(buf + 36 * lane)[q];
+        __syncwarp();
+        // the buffer is free: the next chunk's blocks and x arrive while this one is computed
+        spmv_issue_blocks(A, u + 32, u1, buf, lane);
+        spmv_load_x(A, x, nxt, xa, xb);
+        float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
             const float4 v0 = reinterpret_cast<const float4 *>(ring + 8 * (xrow & (kSpmvRing - 1)))[0];
             const float2 v1 = reinterpret_cast<const float2 *>(ring + 8 * (xrow & (kSpmvRing - 1)) + 4)[0];
             const float vr[6] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y};
-            float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
                 const float e4[4] = {b[q].x, b[q].y, b[q].z, b[q].w};
@@ -1579,7 +1604,10 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         for (int i = 0; i < 6; ++i) carry[i] = __shfl_sync(0xffffffffu, sum[i], last);
         carry_row = cont ? __shfl_sync(0xffffffffu, xrow, last) : kInvalidIndex;
         __syncwarp();
+        cur = nxt;
+        nxt = after;
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");   // the last (empty) copy group
 }
 
 __global__ void __launch_bounds__(256) k_spmv_lower(PcgArgs A, float *y) {
