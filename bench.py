@@ -18,6 +18,7 @@ on the host cores for the same workload and metric.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -49,6 +50,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--spmv-replicas", type=int, default=6,
                    help="replicate the scene batch this many times for the >1 GB SpMV measurement; 1 skips it")
+    p.add_argument("--node-growth-surfels", type=int, default=1_000_000,
+                   help="surfels of the node-growth measurement (torus, R = 6 mm); 0 skips it")
     p.add_argument("--serving-executors", type=int, default=2, help="solver workspaces of the serving run")
     p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the serving run (32 frame streams, 1k-16k nodes); 0 skips it")
@@ -190,6 +193,64 @@ def measure_spmv(solver, n_nodes, stored, stream, dev, launches=20, warmup=3):
     return {"nodes": n_nodes, "stored_blocks": int(stored), "algorithmic_bytes": int(bytes_), "ms_per_launch": ms,
             "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak, "peak_kind": kind,
             "exceeds_l2": bool(bytes_ > 126e6), "timing": "CUDA graph of back-to-back launches"}
+
+
+def measure_node_growth(geo, n_surfels, dev, stream, oracle_timing, repeats=3):
+    """Node construction from surfels (ws_init_nodes: voxel subsample + greedy overlap check on
+    the device) and the K = 8 node graph of the result (ws_build_node_graph), on a torus of
+    `n_surfels` with R = 6 mm.  ws_init_nodes synchronises, so it is timed on the host around the
+    call (device allocations and the copy of the nodes to the host included); the node graph
+    with CUDA events.  The oracle's times on the same input are added when asked."""
+    import torch
+    from starhub_b200 import scenes
+    radius = 0.006
+    rng = np.random.default_rng(31)
+    p, _ = scenes.sample_torus(rng, n_surfels, 0.3, 0.1)
+    p = p @ scenes.rot_x(30.0).T + np.array([0, 0, 1.0])
+    surfels = scenes.pack4(p, 1.0)
+    s_dev = torch.from_numpy(surfels).to(dev)
+    nodes = geo.init_nodes(s_dev, radius)
+    init_ms = []
+    for _ in range(repeats):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        nodes = geo.init_nodes(s_dev, radius)
+        init_ms.append((time.perf_counter() - t0) * 1e3)
+    nd = torch.from_numpy(nodes).to(dev)
+    n = int(nd.shape[0])
+    knn = torch.empty((n, 8), dtype=torch.int16, device=dev)
+    w = torch.empty((n, 8), dtype=torch.float32, device=dev)
+    edges = torch.empty((n * 8, 3), dtype=torch.int16, device=dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    graph_ms = []
+    for it in range(repeats + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = geo.lib.ws_build_node_graph(ctypes.c_void_p(nd.data_ptr()), n, 8, ctypes.c_float(radius),
+                                         ctypes.c_void_p(knn.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                                         ctypes.c_void_p(edges.data_ptr()), sp)
+        e1.record(stream)
+        e1.synchronize()
+        if st != 0:
+            raise RuntimeError(f"ws_build_node_graph failed: {st}")
+        if it:
+            graph_ms.append(e0.elapsed_time(e1))
+    out = {"surfels": n_surfels, "node_radius_m": radius, "nodes": n,
+           "init_nodes_ms": float(np.median(init_ms)), "node_graph_k8_ms": float(np.median(graph_ms))}
+    if oracle_timing:
+        sys.path.insert(0, str(Path(__file__).resolve().parent / "oracle"))
+        import oracle as orc
+        og = orc.OracleGeometry()
+        out["candidates"] = int(og.voxel_subsample(surfels, np.float32(0.7) * np.float32(radius)).shape[0])
+        t0 = time.perf_counter()
+        o = og.init_nodes(surfels, radius)
+        out["oracle_init_nodes_ms"] = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        og.node_graph(o, 8, radius)
+        out["oracle_node_graph_k8_ms"] = (time.perf_counter() - t0) * 1e3
+        out["oracle_threads"] = {"init_nodes": 1, "node_graph": os.cpu_count() or 1}
+        out["nodes_equal_oracle"] = bool(np.array_equal(o, nodes))
+    return out
 
 
 def cpu_solve_rate(sample, threads, precision):
@@ -415,6 +476,13 @@ def main():
         del big
         torch.cuda.empty_cache()
 
+    # ---- node construction and node graph (rank 0) ----
+    growth_out = None
+    if rank == 0 and args.node_growth_surfels > 0:
+        growth_out = measure_node_growth(geo, args.node_growth_surfels, dev, stream,
+                                         oracle_timing=world == 1 and not args.no_cpu_baseline)
+        torch.cuda.empty_cache()
+
     # ---- roofline of the dominant kernel ----
     peak, peak_kind = measured_peak_hbm()
     n_tot = tot_nodes
@@ -507,6 +575,7 @@ def main():
             "cpu_baseline": cpu,
             "serving": serving_out,
             "spmv": spmv_out,
+            "node_growth": growth_out,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": sampler.summary(),

@@ -162,13 +162,29 @@ int ws_get_dense_jacobian(ws_solver *solver, int scene, float *residual, float *
 /* ---- Node graph, skinning and warp (bit-exact to the reference's integer outputs) ---- */
 
 /* NodeGraph::InitializeNodeGraphFromVertex (libs/star/geometry/node_graph/NodeGraph.cu:460-498):
- * voxel subsample on the GPU (VoxelSubsamplerSorting.cu:8-96), greedy host dedup
- * (NodeGraph.cu:652-704), two anchor nodes prepended.  `surfels` is a device float4 array;
- * `nodes_host` receives float4 nodes.  Synchronises `stream`. */
+ * voxel subsample (VoxelSubsamplerSorting.cu:8-96) and the greedy overlap check of
+ * AppendNodeFromVertexHost (NodeGraph.cu:652-704), both on the GPU, two anchor nodes prepended.
+ * `surfels` is a device float4 array; `nodes_host` receives float4 nodes.  *num_nodes is set
+ * also when the count exceeds `capacity` (WS_ERR_CAPACITY); a NaN candidate gives
+ * WS_ERR_INVALID_ARGUMENT.  Synchronises `stream`. */
 int ws_init_nodes(const float *surfels, int num_surfels, float node_radius, float *nodes_host,
                   int capacity, int *num_nodes, void *stream);
+/* NodeGraph::NaiveExpandNodeGraphFromVertexUnsupported (NodeGraph.cu:500-532) with
+ * AppendNodeFromVertexHost (NodeGraph.cu:652-704) and updateAppendNodeInitialTime
+ * (NodeGraph.cu:316-337), on the GPU: the unsupported vertices (device float4, w ignored) are
+ * subsampled on a 0.7 R voxel grid, the candidates that no earlier kept candidate overlaps
+ * (0.85 R) are kept, and they are appended (w = 1) after the first *num_nodes nodes of
+ * `reference_nodes` and of `live_nodes` (device float4; `live_nodes` may be NULL).  `node_time`
+ * (device, may be NULL) gets `current_time` for the appended nodes.  On WS_OK *num_nodes is the
+ * new count.  WS_ERR_CAPACITY when it would exceed `capacity`: the arrays are unchanged and
+ * *num_nodes holds the count needed.  No vertices: WS_OK, nothing changes.  Synchronises `stream`. */
+int ws_expand_nodes(const float *vertices, int num_vertices, float node_radius, float *reference_nodes,
+                    float *live_nodes, unsigned *node_time, unsigned current_time, int capacity, int *num_nodes,
+                    void *stream);
 /* UpdateNodeDistanceKernel + BuildNodeGraphKernel + BuildNodeGraphPairKernel
- * (NodeGraph.cu:10-118): device in/out; k = 4 or 8; edges gets (i, knn[i][k], k). */
+ * (NodeGraph.cu:10-118): device in/out; k = 4 or 8; edges gets (i, knn[i][k], k).  The
+ * n x n half-distance table is not built: each node scans runs of 32 nodes and skips the runs
+ * whose bounding box cannot enter its heap (same results).  Asynchronous on `stream`. */
 int ws_build_node_graph(const float *nodes, int num_nodes, int k, float node_radius,
                         uint16_t *knn, float *spatial_w, uint16_t *edges, void *stream);
 /* SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94): device in/out. */

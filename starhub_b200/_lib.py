@@ -30,7 +30,7 @@ WS_NOALLOC_MAX_PIXELS = 1280 * 720
 EXPORTED = [
     "ws_default_penalties", "ws_create", "ws_destroy", "ws_set_inputs", "ws_set_batch", "ws_solve",
     "ws_solve_graph", "ws_sync_status", "ws_get_solution", "ws_get_counts", "ws_get_dense_terms",
-    "ws_get_node2term", "ws_get_node_pairs", "ws_get_system", "ws_get_dense_jacobian", "ws_init_nodes",
+    "ws_get_node2term", "ws_get_node_pairs", "ws_get_system", "ws_get_dense_jacobian", "ws_init_nodes", "ws_expand_nodes",
     "ws_build_node_graph", "ws_skinning", "ws_forward_warp", "ws_splat_maps", "ws_measure_maps", "ws_version",
     "ws_error_string", "ws_set_profiling", "ws_get_phase_times", "ws_graph_kernel_count",
     "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
@@ -129,6 +129,7 @@ def load() -> C.CDLL:
     lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | getattr(os, "RTLD_GLOBAL", 0))
     vp, i, f = C.c_void_p, C.c_int, C.c_float
     pi = C.POINTER(C.c_int)
+    u = C.c_uint
     sig = {
         "ws_default_penalties": (None, [C.POINTER(WsInputs)]),
         "ws_create": (i, [C.POINTER(WsConfig), C.POINTER(vp)]),
@@ -146,6 +147,7 @@ def load() -> C.CDLL:
         "ws_get_system": (i, [vp, i, vp, vp, vp, i, pi, vp, vp, vp]),
         "ws_get_dense_jacobian": (i, [vp, i, vp, vp, i, pi]),
         "ws_init_nodes": (i, [vp, i, f, vp, i, pi, vp]),
+        "ws_expand_nodes": (i, [vp, i, f, vp, vp, vp, u, i, pi, vp]),
         "ws_build_node_graph": (i, [vp, i, i, f, vp, vp, vp, vp]),
         "ws_skinning": (i, [vp, i, vp, i, f, vp, vp, vp, vp]),
         "ws_forward_warp": (i, [vp, i, vp, vp, i, vp, vp, vp, vp, vp, vp]),

@@ -1,4 +1,4 @@
-// Node graph construction, skinning, forward warp and the solver-map splat.
+// Node graph construction and growth, skinning, forward warp and the solver-map splat.
 //
 // Integer outputs (node candidates, node and surfel k-NN ids) follow the
 // reference bit for bit: the same float expressions with the fused
@@ -10,6 +10,7 @@
 #include <mutex>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -100,7 +101,10 @@ __global__ void k_voxel_marks(const uint32_t *keys, uint32_t n, uint32_t *marks)
 }
 
 // samplingPointsKernel (VoxelSubsamplerSorting.cu:60-96): per voxel the point nearest the
-// voxel centre, first wins on ties.
+// voxel centre, first wins on ties.  The centre is a rounded float3 computed before the loop
+// over the voxel's points, as the source writes it; the intrinsics keep nvcc from fusing its
+// product into the subtraction, which moves squared distances by about 1e-10 m^2 and flips
+// near-ties between points (about 2 voxels in 89k on a 1M-point torus).
 __global__ void k_voxel_sample(const uint32_t *keys, const uint32_t *perm, const uint32_t *head_off, uint32_t n,
                                const float4 *pts, float voxel, float4 *out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -112,32 +116,219 @@ __global__ void k_voxel_sample(const uint32_t *keys, const uint32_t *perm, const
         int x = enc % 1024;
         int y = (enc - z * 1024 * 1024) / 1024;
         x -= 512; y -= 512; z -= 512;
-        const float cx = float(x + 0.5) * voxel, cy = float(y + 0.5) * voxel, cz = float(z + 0.5) * voxel;
+        const float cx = __fmul_rn(float(x + 0.5), voxel), cy = __fmul_rn(float(y + 0.5), voxel),
+                    cz = __fmul_rn(float(z + 0.5), voxel);
         float best = 1e5f;
         uint32_t bi = i;
         for (uint32_t k = i; k < e; ++k) {
             const float4 p = pts[perm[k]];
-            const float dd = sq3_fused(p.x - cx, p.y - cy, p.z - cz);
+            const float dd = sq3_fused(__fsub_rn(p.x, cx), __fsub_rn(p.y, cy), __fsub_rn(p.z, cz));
             if (dd < best) { best = dd; bi = k; }
         }
         out[head_off[i]] = pts[perm[bi]];
     }
 }
 
+// ---- Overlap check of the node candidates on the device ----
+//
+// AppendNodeFromVertexHost (libs/star/geometry/node_graph/NodeGraph.cu:652-704) walks the
+// candidates in order and keeps one when no candidate kept before it lies within 0.85 R
+// (squared distance <= (0.85 R)^2, summed as ((dx*dx + dy*dy) + dz*dz) + dw*dw with dw = 0).
+// That is the lexicographically first maximal independent set of the graph that joins
+// candidates within 0.85 R, and it comes out of rounds: a candidate is rejected once one of
+// its earlier neighbours is kept, and kept once all of them are rejected.  Every decision is
+// final and equals the sequential loop's (by induction on the index), and each round decides
+// at least the lowest undecided candidate, so at most nv rounds run.
+
+// Dedup grid: cells of 1.125 x the overlap radius.  Two candidates that pass the distance test
+// differ by at most r (1 + 2^-22) per axis, i.e. 0.889 cells; the scaled coordinates are
+// clamped to +-2^18 cells, where a float resolves 1/32 of a cell, so their rounding adds at most
+// 1/32 and such candidates lie in the same or adjacent cells.  Cell coordinates wrap at 1024
+// per axis, which only adds far candidates that the distance test turns away.
+constexpr float kDedupCellScale = 1.125f;
+
+__device__ __forceinline__ int dedup_cell(float v, float inv_cell) {
+    return __float2int_rd(fminf(fmaxf(__fmul_rn(v, inv_cell), -262144.f), 262144.f));
+}
+
+__device__ __forceinline__ uint32_t dedup_key(int x, int y, int z) {
+    return (uint32_t)(x & 1023) | ((uint32_t)(y & 1023) << 10) | ((uint32_t)(z & 1023) << 20);
+}
+
+__global__ void k_dedup_keys(const float4 *cand, uint32_t nv, float inv_cell, uint32_t *keys, uint32_t *ids, int *err) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+        const float4 p = cand[i];
+        if (isnan(p.x) || isnan(p.y) || isnan(p.z)) atomicOr(err, 1);
+        keys[i] = dedup_key(dedup_cell(p.x, inv_cell), dedup_cell(p.y, inv_cell), dedup_cell(p.z, inv_cell));
+        ids[i] = i;
+    }
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *a, uint32_t n, uint32_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Earlier candidates that overlap candidate i, found in the 3 x 3 rows of three cells around
+// it (a row is one key range unless its x wraps).  kFill = false counts them into `cnt`;
+// kFill = true writes their indices from offset `cnt[i]` of `nbr`.
+template <bool kFill>
+__global__ void k_dedup_neighbours(const float4 *cand, const uint32_t *cell_keys, const uint32_t *cell_ids, uint32_t nv,
+                                   float inv_cell, float thr, uint32_t *cnt, uint32_t *nbr) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+        const float4 p = cand[i];
+        const int cx = dedup_cell(p.x, inv_cell), cy = dedup_cell(p.y, inv_cell), cz = dedup_cell(p.z, inv_cell);
+        const int x0 = (cx - 1) & 1023, x1 = (cx + 1) & 1023;
+        uint32_t c = 0, out = kFill ? cnt[i] : 0u;
+        for (int dz = -1; dz <= 1; ++dz) {
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t lo_key[2], hi_key[2];
+                int ranges = 1;
+                if (x0 < x1) {
+                    lo_key[0] = dedup_key(x0, cy + dy, cz + dz);
+                    hi_key[0] = dedup_key(x1, cy + dy, cz + dz);
+                } else {
+                    lo_key[0] = dedup_key(x0, cy + dy, cz + dz);
+                    hi_key[0] = dedup_key(1023, cy + dy, cz + dz);
+                    lo_key[1] = dedup_key(0, cy + dy, cz + dz);
+                    hi_key[1] = dedup_key(x1, cy + dy, cz + dz);
+                    ranges = 2;
+                }
+                for (int q = 0; q < ranges; ++q) {
+                    for (uint32_t b = lower_bound_u32(cell_keys, nv, lo_key[q]); b < nv && __ldg(cell_keys + b) <= hi_key[q];
+                         ++b) {
+                        const uint32_t j = __ldg(cell_ids + b);
+                        if (j >= i) continue;
+                        const float4 o = cand[j];
+                        const float ex = o.x - p.x, ey = o.y - p.y, ez = o.z - p.z;
+                        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
+                        if (d2 <= thr) {
+                            if (kFill) nbr[out++] = j; else ++c;
+                        }
+                    }
+                }
+            }
+        }
+        if (!kFill) cnt[i] = c;
+    }
+}
+
+// The rounds, in one block of 1024 threads.  Decisions (0 open, 1 kept, 2 rejected) live in
+// shared memory when nv bytes fit, else in `decision`; they are read volatile, so a decision
+// taken earlier in the same round is used at once.  Thread t walks candidates t, t + 1024, ...
+// from the first one it has not yet settled.  On return `decision` holds every decision;
+// `err` is set only if nv + 1 rounds left a candidate open, which the argument above excludes.
+constexpr int kDedupThreads = 1024;
+constexpr uint32_t kDedupSharedMax = 160 * 1024;
+
+__global__ void __launch_bounds__(kDedupThreads) k_dedup_greedy(const uint32_t *nbr_ptr, const uint32_t *nbr, uint32_t nv,
+                                                                uint8_t *decision, int in_shared, int *err) {
+    extern __shared__ uint8_t s_decision[];
+    volatile uint8_t *dec = in_shared ? s_decision : decision;
+    for (uint32_t i = threadIdx.x; i < nv; i += kDedupThreads) dec[i] = 0;
+    __syncthreads();
+    uint32_t first = threadIdx.x;
+    bool done = false;
+    for (uint32_t round = 0; round <= nv && !done; ++round) {   // uniform: `done` comes from a block vote
+        int open = 0;
+        bool settled_prefix = true;
+        for (uint32_t i = first; i < nv; i += kDedupThreads) {
+            uint8_t d = dec[i];
+            if (d == 0) {
+                d = 1;
+                for (uint32_t k = __ldg(nbr_ptr + i), e = __ldg(nbr_ptr + i + 1); k < e; ++k) {
+                    const uint8_t t = dec[__ldg(nbr + k)];
+                    if (t == 1) { d = 2; break; }
+                    if (t == 0) d = 0;
+                }
+                if (d != 0) dec[i] = d;
+            }
+            if (d == 0) {
+                open = 1;
+                settled_prefix = false;
+            } else if (settled_prefix) {
+                first = i + kDedupThreads;
+            }
+        }
+        done = !__syncthreads_or(open);
+    }
+    if (!done && threadIdx.x == 0) atomicOr(err, 2);
+    if (in_shared)
+        for (uint32_t i = threadIdx.x; i < nv; i += kDedupThreads) decision[i] = s_decision[i];
+}
+
+__global__ void k_dedup_flags(const uint8_t *decision, uint32_t nv, uint32_t *flags) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+        flags[i] = decision[i] == 1 ? 1u : 0u;
+}
+
+// Kept candidates in candidate order, w = 1 (the host loop appends make_float4(x, y, z, 1)).
+__global__ void k_dedup_emit(const float4 *cand, const uint8_t *decision, const uint32_t *pos, uint32_t nv, float4 *out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+        if (decision[i] == 1) {
+            const float4 c = cand[i];
+            out[pos[i]] = make_float4(c.x, c.y, c.z, 1.0f);
+        }
+}
+
+__global__ void k_fill_u32(uint32_t *a, uint32_t n, uint32_t v) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+
+// Bounding boxes of runs of kGraphRun consecutive nodes (lo in boxes[0, runs), hi after).
+// NaN coordinates stay out of a box: fminf/fmaxf return the other operand.
+constexpr int kGraphRun = 32;
+
+__global__ void k_node_boxes(const float4 *nodes, int n, float4 *lo, float4 *hi) {
+    const int runs = (n + kGraphRun - 1) / kGraphRun;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < runs; r += gridDim.x * blockDim.x) {
+        float4 a = make_float4(INFINITY, INFINITY, INFINITY, 0.f), b = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        for (int k = r * kGraphRun, e = min(n, (r + 1) * kGraphRun); k < e; ++k) {
+            const float4 p = nodes[k];
+            a.x = fminf(a.x, p.x); a.y = fminf(a.y, p.y); a.z = fminf(a.z, p.z);
+            b.x = fmaxf(b.x, p.x); b.y = fmaxf(b.y, p.y); b.z = fmaxf(b.z, p.z);
+        }
+        lo[r] = a;
+        hi[r] = b;
+    }
+}
+
 // UpdateNodeDistanceKernel + BuildNodeGraphKernel (libs/star/geometry/node_graph/NodeGraph.cu:10-101):
 // half-precision squared distances, k nearest including the node itself, __expf weights normalized.
+//
+// The reference fills an n x n table of half distances and scans a row of it in column order.
+// Here each node scans the other nodes in the same order but skips a run of kGraphRun whose
+// box is no nearer than the heap's current maximum.  Such a run cannot change the heap: the
+// per-axis gap to the box is at most each member's |dx| (a difference rounded to nearest is
+// monotone in its operands), the squared sum and the rounding to half are monotone too, so
+// the same expression on the gaps bounds every member's half distance from below, and the
+// heap only takes a distance strictly below its maximum.  Every heap update of the full scan
+// happens in the same order, so ids, weights and their ties come out the same.
 template <int K>
-__global__ void k_node_graph(const float4 *nodes, int n, float r2, uint16_t *knn, float *w, uint16_t *edges) {
+__global__ void k_node_graph(const float4 *nodes, int n, float r2, const float4 *box_lo, const float4 *box_hi,
+                             uint16_t *knn, float *w, uint16_t *edges) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
         const float4 va = nodes[a];
         Heap<K> h;
         h.init(1e3f);
-        for (int b = 0; b < n; ++b) {
-            const float4 vb = nodes[b];
-            const float4 hi = (a >= b) ? va : vb, lo = (a >= b) ? vb : va;
-            const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
-            const float dist = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-            h.update((uint16_t)b, __half2float(__float2half_rn(dist)));
+        for (int r0 = 0, run = 0; r0 < n; r0 += kGraphRun, ++run) {
+            const float4 lo = box_lo[run], hi = box_hi[run];
+            const float gx = fmaxf(fmaxf(lo.x - va.x, va.x - hi.x), 0.f);
+            const float gy = fmaxf(fmaxf(lo.y - va.y, va.y - hi.y), 0.f);
+            const float gz = fmaxf(fmaxf(lo.z - va.z, va.z - hi.z), 0.f);
+            const float bound = __fmaf_rn(gz, gz, __fmaf_rn(gy, gy, __fmul_rn(gx, gx)));
+            if (__half2float(__float2half_rn(bound)) >= h.max_d) continue;
+            for (int b = r0, e = min(n, r0 + kGraphRun); b < e; ++b) {
+                const float4 vb = nodes[b];
+                const float4 hi_v = (a >= b) ? va : vb, lo_v = (a >= b) ? vb : va;
+                const float dx = hi_v.x - lo_v.x, dy = hi_v.y - lo_v.y, dz = hi_v.z - lo_v.z;
+                const float dist = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+                h.update((uint16_t)b, __half2float(__float2half_rn(dist)));
+            }
         }
         h.sort();
         float wv[K], sum = 0.f;
@@ -299,7 +490,114 @@ int noalloc_scratch(unsigned long long **out) {
     return WS_OK;
 }
 
+// Device temporaries of a node-growth call, from the stream-ordered pool of `st`: taken and
+// given back in stream order, so later calls reuse the pool's memory without a device-wide
+// synchronisation.
+struct DeviceBlocks {
+    explicit DeviceBlocks(cudaStream_t s) : st(s) {}
+    DeviceBlocks(const DeviceBlocks &) = delete;
+    DeviceBlocks &operator=(const DeviceBlocks &) = delete;
+    cudaStream_t st;
+    std::vector<void *> ptrs;
+    cudaError_t err = cudaSuccess;
+    template <class T>
+    T *get(size_t bytes) {
+        void *p = nullptr;
+        if (err == cudaSuccess) err = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (err != cudaSuccess) return nullptr;
+        ptrs.push_back(p);
+        return static_cast<T *>(p);
+    }
+    ~DeviceBlocks() {
+        for (void *p : ptrs) cudaFreeAsync(p, st);
+    }
+};
+
+// Node candidates of a point set and the overlap check, all on the device:
+// VoxelSubsamplerSorting::PerformSubsample (libs/star/geometry/sampling/VoxelSubsamplerSorting.cu:8-96)
+// on a 0.7 R grid, then the greedy check of AppendNodeFromVertexHost (NodeGraph.cu:652-704).
+// On WS_OK, (*nodes)[0 .. *kept) holds the kept candidates in candidate order (w = 1).
+// Synchronises `st` (the counts return to the host).
+int grow_nodes(const float4 *pts, uint32_t n, float node_radius, DeviceBlocks &mem, cudaStream_t st, float4 **nodes,
+               uint32_t *kept) {
+    const float voxel = 0.7f * node_radius;
+    // n + 1 entries: a spare value buffer later takes the scan of the kept flags and its total.
+    uint32_t *keys = mem.get<uint32_t>(4ull * (n + 1)), *vals = mem.get<uint32_t>(4ull * (n + 1));
+    uint32_t *keys2 = mem.get<uint32_t>(4ull * (n + 1)), *vals2 = mem.get<uint32_t>(4ull * (n + 1));
+    uint32_t *heads = mem.get<uint32_t>(4ull * (n + 1));
+    uint32_t *tmp = mem.get<uint32_t>(4ull * (n / ws::kScanTile + 4));
+    uint32_t *hist = mem.get<uint32_t>(4ull * 256 * ws::sort_max_tiles(n));
+    uint32_t *digit = mem.get<uint32_t>(4ull * 256);
+    float4 *cand = mem.get<float4>(16ull * n);
+    int *err = mem.get<int>(4);
+    if (mem.err != cudaSuccess) return WS_ERR_CUDA;
+    uint32_t nv = 0;
+    {
+        ws::k_voxel_key<<<ws::grid_of(n, 256), 256, 0, st>>>(pts, n, voxel, keys, vals);
+        const bool alt = ws::radix_sort<uint32_t>(keys, vals, keys2, vals2, nullptr, n, n, 30, hist, digit, st);
+        const uint32_t *sk = alt ? keys2 : keys, *sv = alt ? vals2 : vals;
+        ws::k_voxel_marks<<<ws::grid_of(n, 256), 256, 0, st>>>(sk, n, heads);
+        ws::exclusive_scan(heads, heads, nullptr, n, n, tmp, st);
+        ws::k_voxel_sample<<<ws::grid_of(n, 256), 256, 0, st>>>(sk, sv, heads, n, pts, voxel, cand);
+        if (cudaMemcpyAsync(&nv, heads + n, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return WS_ERR_CUDA;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return WS_ERR_CUDA;
+    }
+    *nodes = mem.get<float4>(16ull * nv);
+    if (mem.err != cudaSuccess) return WS_ERR_CUDA;
+    *kept = 0;
+    if (nv == 0) return WS_OK;
+    // The host loop's constants, in the same float arithmetic.
+    const float r = 0.85f * node_radius;
+    const float thr = r * r;
+    const float inv_cell = 1.0f / (ws::kDedupCellScale * r);
+    uint32_t *cnt = heads;   // free again: the candidates are written
+    uint32_t total = 0;
+    int flag = 0;
+    const uint32_t *ck = nullptr, *ci = nullptr;
+    uint32_t *spare_keys = nullptr, *spare_vals = nullptr;
+    {
+        if (cudaMemsetAsync(err, 0, 4, st) != cudaSuccess) return WS_ERR_CUDA;
+        ws::k_dedup_keys<<<ws::grid_of(nv, 256), 256, 0, st>>>(cand, nv, inv_cell, keys, vals, err);
+        const bool alt = ws::radix_sort<uint32_t>(keys, vals, keys2, vals2, nullptr, nv, nv, 30, hist, digit, st);
+        ck = alt ? keys2 : keys;
+        ci = alt ? vals2 : vals;
+        spare_keys = alt ? keys : keys2;
+        spare_vals = alt ? vals : vals2;
+        ws::k_dedup_neighbours<false><<<ws::grid_of(nv, 128), 128, 0, st>>>(cand, ck, ci, nv, inv_cell, thr, cnt, nullptr);
+        ws::exclusive_scan(cnt, cnt, nullptr, nv, nv, tmp, st);
+        if (cudaMemcpyAsync(&total, cnt + nv, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(&flag, err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return WS_ERR_CUDA;
+        // AppendNodeFromVertexHost stops on a NaN candidate (LOG(FATAL)).
+        if (flag & 1) return WS_ERR_INVALID_ARGUMENT;
+    }
+    uint32_t *nbr = mem.get<uint32_t>(4ull * total);
+    if (mem.err != cudaSuccess) return WS_ERR_CUDA;
+    ws::k_dedup_neighbours<true><<<ws::grid_of(nv, 128), 128, 0, st>>>(cand, ck, ci, nv, inv_cell, thr, cnt, nbr);
+    uint8_t *decision = reinterpret_cast<uint8_t *>(spare_keys);
+    const int in_shared = nv <= ws::kDedupSharedMax ? 1 : 0;
+    if (cudaFuncSetAttribute(ws::k_dedup_greedy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ws::kDedupSharedMax) != cudaSuccess)
+        return WS_ERR_CUDA;
+    ws::k_dedup_greedy<<<1, ws::kDedupThreads, in_shared ? nv : 0, st>>>(cnt, nbr, nv, decision, in_shared, err);
+    uint32_t *pos = spare_vals;
+    ws::k_dedup_flags<<<ws::grid_of(nv, 256), 256, 0, st>>>(decision, nv, pos);
+    ws::exclusive_scan(pos, pos, nullptr, nv, nv, tmp, st);
+    ws::k_dedup_emit<<<ws::grid_of(nv, 256), 256, 0, st>>>(cand, decision, pos, nv, *nodes);
+    if (cudaGetLastError() != cudaSuccess) return WS_ERR_CUDA;
+    uint32_t count = 0;
+    if (cudaMemcpyAsync(&count, pos + nv, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&flag, err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return WS_ERR_CUDA;
+    if (flag & 2) return WS_ERR_CUDA;
+    *kept = count;
+    return WS_OK;
+}
+
 }  // namespace
+
 
 extern "C" {
 
@@ -308,63 +606,58 @@ int ws_init_nodes(const float *surfels, int n, float node_radius, float *nodes_h
     if (!surfels || n <= 0 || !nodes_host || !num_nodes || cap < 2 || !(node_radius > 0.f))
         return WS_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const float voxel = 0.7f * node_radius;
-    uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr, *heads = nullptr, *tmp = nullptr,
-             *hist = nullptr, *digit = nullptr;
-    float4 *cand = nullptr;
-    const uint32_t un = (uint32_t)n;
-    cudaError_t e = cudaSuccess;
-    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
-    A(cudaMalloc(&keys, 4ull * un));
-    A(cudaMalloc(&vals, 4ull * un));
-    A(cudaMalloc(&keys2, 4ull * un));
-    A(cudaMalloc(&vals2, 4ull * un));
-    A(cudaMalloc(&heads, 4ull * (un + 1)));
-    A(cudaMalloc(&tmp, 4ull * (un / ws::kScanTile + 4)));
-    A(cudaMalloc(&hist, 4ull * 256 * ws::sort_max_tiles(un)));
-    A(cudaMalloc(&digit, 4ull * 256));
-    A(cudaMalloc(&cand, 16ull * un));
-    std::vector<float4> hc;
-    uint32_t nv = 0;
-    if (e == cudaSuccess) {
-        const float4 *pts = reinterpret_cast<const float4 *>(surfels);
-        ws::k_voxel_key<<<ws::grid_of(n, 256), 256, 0, st>>>(pts, un, voxel, keys, vals);
-        const bool alt = ws::radix_sort<uint32_t>(keys, vals, keys2, vals2, nullptr, un, un, 30, hist, digit, st);
-        const uint32_t *sk = alt ? keys2 : keys, *sv = alt ? vals2 : vals;
-        ws::k_voxel_marks<<<ws::grid_of(n, 256), 256, 0, st>>>(sk, un, heads);
-        ws::exclusive_scan(heads, heads, nullptr, un, un, tmp, st);
-        ws::k_voxel_sample<<<ws::grid_of(n, 256), 256, 0, st>>>(sk, sv, heads, un, pts, voxel, cand);
-        A(cudaMemcpyAsync(&nv, heads + un, 4, cudaMemcpyDeviceToHost, st));
-        A(cudaStreamSynchronize(st));
-        hc.resize(nv);
-        if (nv) A(cudaMemcpy(hc.data(), cand, 16ull * nv, cudaMemcpyDeviceToHost));
-    }
-    for (void *p : {(void *)keys, (void *)vals, (void *)keys2, (void *)vals2, (void *)heads, (void *)tmp, (void *)hist,
-                    (void *)digit, (void *)cand})
-        if (p) cudaFree(p);
-    if (e != cudaSuccess) return WS_ERR_CUDA;
-    // NodeGraph::AppendNodeFromVertexHost (NodeGraph.cu:652-704): greedy in candidate order.
-    const float r = 0.85f * node_radius;
-    const float thr = r * r;
-    std::vector<float4> acc;
-    for (uint32_t i = 0; i < nv; ++i) {
-        const float4 p = make_float4(hc[i].x, hc[i].y, hc[i].z, 1.0f);
-        if (std::isnan(p.x) || std::isnan(p.y) || std::isnan(p.z)) return WS_ERR_INVALID_ARGUMENT;
-        bool is_node = true;
-        for (const float4 &q : acc) {
-            const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z, dw = q.w - p.w;
-            const float d2 = ((dx * dx + dy * dy) + dz * dz) + dw * dw;
-            if (d2 <= thr) { is_node = false; break; }
-        }
-        if (is_node) acc.push_back(p);
-    }
-    const int total = (int)acc.size() + 2;
-    *num_nodes = total;
+    DeviceBlocks mem(st);
+    float4 *nodes = nullptr;
+    uint32_t kept = 0;
+    const int rc = grow_nodes(reinterpret_cast<const float4 *>(surfels), (uint32_t)n, node_radius, mem, st, &nodes, &kept);
+    if (rc != WS_OK) return rc;
+    // InitializeNodeGraphFromVertex (NodeGraph.cu:479-486): two anchors at the origin come first.
+    const float anchors[8] = {0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    const long long total = (long long)kept + 2;
+    *num_nodes = (int)std::min<long long>(total, INT_MAX);
     if (total > cap) return WS_ERR_CAPACITY;
-    for (int a = 0; a < 2; ++a) {
-        nodes_host[4 * a] = 0.f; nodes_host[4 * a + 1] = 0.f; nodes_host[4 * a + 2] = 0.f; nodes_host[4 * a + 3] = 1.f;
+    std::memcpy(nodes_host, anchors, sizeof(anchors));
+    if (kept && cudaMemcpyAsync(nodes_host + 8, nodes, 16ull * kept, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return WS_ERR_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
+int ws_expand_nodes(const float *vertices, int num_vertices, float node_radius, float *reference_nodes,
+                    float *live_nodes, unsigned *node_time, unsigned current_time, int cap, int *num_nodes,
+                    void *stream) {
+    if (!num_nodes || !reference_nodes || num_vertices < 0 || !(node_radius > 0.f) || *num_nodes < 0 ||
+        cap < *num_nodes)
+        return WS_ERR_INVALID_ARGUMENT;
+    // NaiveExpandNodeGraphFromVertexUnsupported (NodeGraph.cu:500-510): nothing to add.
+    if (num_vertices == 0) return WS_OK;
+    if (!vertices) return WS_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DeviceBlocks mem(st);
+    float4 *nodes = nullptr;
+    uint32_t kept = 0;
+    const int rc =
+        grow_nodes(reinterpret_cast<const float4 *>(vertices), (uint32_t)num_vertices, node_radius, mem, st, &nodes, &kept);
+    if (rc != WS_OK) return rc;
+    const long long before = *num_nodes, total = before + kept;
+    if (total > cap) {
+        *num_nodes = (int)std::min<long long>(total, INT_MAX);
+        return WS_ERR_CAPACITY;
     }
-    std::memcpy(nodes_host + 8, acc.data(), acc.size() * sizeof(float4));
+    if (kept) {
+        const size_t bytes = 16ull * kept;
+        if (cudaMemcpyAsync(reference_nodes + 4 * before, nodes, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return WS_ERR_CUDA;
+        if (live_nodes && live_nodes != reference_nodes &&
+            cudaMemcpyAsync(live_nodes + 4 * before, nodes, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return WS_ERR_CUDA;
+        // updateAppendNodeInitialTime (NodeGraph.cu:316-337)
+        if (node_time) {
+            ws::k_fill_u32<<<ws::grid_of(kept, 256), 256, 0, st>>>(node_time + before, kept, current_time);
+            if (cudaGetLastError() != cudaSuccess) return WS_ERR_CUDA;
+        }
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return WS_ERR_CUDA;
+    *num_nodes = (int)total;
     return WS_OK;
 }
 
@@ -373,13 +666,21 @@ int ws_build_node_graph(const float *nodes, int n, int k, float node_radius, uin
     if (!nodes || n <= 0 || n > 65535 || !knn || !w || !edges || (k != 4 && k != 8)) return WS_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float r2 = node_radius * node_radius;
+    const int runs = (n + ws::kGraphRun - 1) / ws::kGraphRun;
+    // Run boxes from the stream-ordered pool: the call stays asynchronous.
+    float4 *boxes = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void **>(&boxes), 32ull * runs, st) != cudaSuccess) return WS_ERR_CUDA;
+    const float4 *nd = reinterpret_cast<const float4 *>(nodes);
+    ws::k_node_boxes<<<ws::grid_of(runs, 128), 128, 0, st>>>(nd, n, boxes, boxes + runs);
     const int threads = 64;
     const int grid = (n + threads - 1) / threads;
     if (k == 4)
-        ws::k_node_graph<4><<<grid, threads, 0, st>>>(reinterpret_cast<const float4 *>(nodes), n, r2, knn, w, edges);
+        ws::k_node_graph<4><<<grid, threads, 0, st>>>(nd, n, r2, boxes, boxes + runs, knn, w, edges);
     else
-        ws::k_node_graph<8><<<grid, threads, 0, st>>>(reinterpret_cast<const float4 *>(nodes), n, r2, knn, w, edges);
-    return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+        ws::k_node_graph<8><<<grid, threads, 0, st>>>(nd, n, r2, boxes, boxes + runs, knn, w, edges);
+    const cudaError_t launched = cudaGetLastError();
+    const cudaError_t freed = cudaFreeAsync(boxes, st);
+    return launched == cudaSuccess && freed == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }
 
 int ws_skinning(const float *nodes, int n_nodes, const float *verts, int n_verts, float node_radius, uint16_t *knn,

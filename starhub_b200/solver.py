@@ -322,7 +322,7 @@ def _wrap_device_floats(ptr: int, count: int, device: int) -> torch.Tensor:
 
 class GpuGeometry:
     """Node construction, node graph, skinning, forward warp and map splat on the GPU
-    (ws_init_nodes, ws_build_node_graph, ws_skinning, ws_forward_warp, ws_splat_maps)."""
+    (ws_init_nodes, ws_expand_nodes, ws_build_node_graph, ws_skinning, ws_forward_warp, ws_splat_maps)."""
 
     def __init__(self, device="cuda"):
         self.lib = _lib.load()
@@ -339,6 +339,19 @@ class GpuGeometry:
         check(self.lib.ws_init_nodes(_ptr(s), int(s.shape[0]), float(node_radius), out.ctypes.data, cap, C.byref(n),
                                      self._stream()), "ws_init_nodes")
         return out[: n.value].copy()
+
+    def expand_nodes(self, reference_nodes, live_nodes, num_nodes, vertices, node_radius, node_time=None,
+                     current_time=0):
+        """Appends nodes grown from `vertices` (NodeGraph::NaiveExpandNodeGraphFromVertexUnsupported,
+        NodeGraph.cu:500-532) to device arrays of capacity rows; returns the new node count."""
+        v = _dev(vertices, self.device, torch.float32)
+        n = C.c_int(int(num_nodes))
+        cap = int(reference_nodes.shape[0])
+        live = _ptr(live_nodes) if live_nodes is not None else None
+        times = _ptr(node_time) if node_time is not None else None
+        check(self.lib.ws_expand_nodes(_ptr(v), int(v.shape[0]), float(node_radius), _ptr(reference_nodes), live, times,
+                                       int(current_time), cap, C.byref(n), self._stream()), "ws_expand_nodes")
+        return n.value
 
     def node_graph(self, nodes, k, node_radius):
         nd = _dev(nodes, self.device, torch.float32)
