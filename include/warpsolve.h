@@ -124,6 +124,7 @@ int ws_get_solution(ws_solver *solver, int scene, const float **dev_node_se3, in
  * solve, for every scene of the batch at once.  x and y are device arrays of 8 floats per
  * node (6 used) in batch order: scene i's nodes follow those of scenes 0..i-1.  In
  * WS_PREC_MIXED the unknowns are node-centred twists (t' = t - c x w), as in the solve.
+ * The products meet in y through atomic adds, so y may differ in the last bits between calls.
  * Asynchronous on `stream`; WS_ERR_NOT_READY before the first solve. */
 int ws_spmv(ws_solver *solver, const float *x, float *y, void *stream);
 /* The same operator applied matrix-free from the term records of the last Gauss-Newton

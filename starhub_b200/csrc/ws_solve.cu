@@ -1465,9 +1465,11 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 }
 
 // Standalone y = A x over the assembled symmetric store of the last Gauss-Newton iteration
-// (x, y: 8 floats per node).  Pass 1 (k_spmv) writes the diagonal and upper part of every
-// row and the transposed contributions; pass 2 (k_spmv_lower) adds each row's contributions.
-// Pass 1 streams a warp's contiguous blocks through one 4.6 KB shared-memory buffer: the
+// (x, y: 8 floats per node).  y starts at zero; every row's diagonal-and-upper sum and every
+// transposed product B^T x_row of an upper item are added into y with vector atomics, which
+// resolve in L2 (y of the whole batch fits there), so DRAM sees the blocks, the item records,
+// x and y once each: no contribution buffer and no second pass.  Sums meet in no fixed order.
+// The kernel streams a warp's contiguous blocks through one 4.6 KB shared-memory buffer: the
 // chunk's blocks arrive with cp.async (every copy instruction moves 512 contiguous bytes),
 // each lane moves its item's block into registers, and the buffer at once takes the next
 // chunk's copies, which then overlap the current chunk's arithmetic.  x of the items'
@@ -1556,9 +1558,9 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
                 }
             }
             if (!diag) {
-                float4 *co = reinterpret_cast<float4 *>(A.contrib + 8ull * min(cur.y, A.cap_half - 1));
-                co[0] = make_float4(t[0], t[1], t[2], t[3]);
-                co[1] = make_float4(t[4], t[5], 0.f, 0.f);
+                float *yc = y + 8ull * min(cur.x, A.total_nodes - 1);
+                atomicAdd(reinterpret_cast<float4 *>(yc), make_float4(t[0], t[1], t[2], t[3]));
+                atomicAdd(reinterpret_cast<float2 *>(yc + 4), make_float2(t[4], t[5]));
             }
             reinterpret_cast<float4 *>(prod + 8 * lane)[0] = make_float4(a[0], a[1], a[2], a[3]);
             reinterpret_cast<float2 *>(prod + 8 * lane + 4)[0] = make_float2(a[4], a[5]);
@@ -1594,9 +1596,8 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
                 sum[5] += p1.y;
             }
             if (ends_row) {
-                float4 *yo = reinterpret_cast<float4 *>(y + 8ull * xrow);
-                yo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
-                yo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
+                atomicAdd(reinterpret_cast<float4 *>(y + 8ull * xrow), make_float4(sum[0], sum[1], sum[2], sum[3]));
+                atomicAdd(reinterpret_cast<float2 *>(y + 8ull * xrow + 4), make_float2(sum[4], sum[5]));
             }
         }
         const bool cont = __shfl_sync(0xffffffffu, owner && !ends_row ? 1 : 0, last) != 0;
@@ -1608,15 +1609,6 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         nxt = after;
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");   // the last (empty) copy group
-}
-
-__global__ void __launch_bounds__(256) k_spmv_lower(PcgArgs A, float *y) {
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < A.total_nodes; row += gridDim.x * blockDim.x) {
-        float v[6];
-        load6(y + 8ull * row, v);
-        add_lower(A, row, v);
-        store6(y + 8ull * row, v);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1954,8 +1946,9 @@ cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *u
 
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st) {
     const PcgArgs a = pcg_args(w, 0);
+    const cudaError_t e = cudaMemsetAsync(y, 0, 32ull * w.total_nodes, st);
+    if (e != cudaSuccess) return e;
     k_spmv<<<2 * pcg_launch_blocks(w), kPcgThreads, 0, st>>>(a, x, y);
-    k_spmv_lower<<<grid_for(w.total_nodes, 256, w.num_sms), 256, 0, st>>>(a, y);
     return cudaGetLastError();
 }
 
