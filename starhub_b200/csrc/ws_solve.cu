@@ -1469,15 +1469,19 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 // transposed product B^T x_row of an upper item are added into y with vector atomics, which
 // resolve in L2 (y of the whole batch fits there), so DRAM sees the blocks, the item records,
 // x and y once each: no contribution buffer and no second pass.  Sums meet in no fixed order.
-// The kernel streams a warp's contiguous blocks through one 4.6 KB shared-memory buffer: the
-// chunk's blocks arrive with cp.async (every copy instruction moves 512 contiguous bytes),
-// each lane moves its item's block into registers, and the buffer at once takes the next
-// chunk's copies, which then overlap the current chunk's arithmetic.  x of the items'
-// columns is loaded a chunk ahead into registers, the item records two chunks ahead.  With
-// 7 KB of shared memory per warp, registers set the number of warps per SM.  Warp v takes
-// half of PCG range v / 2 (by row groups), so the ranges are the PCG's, at twice the warps.
+// The kernel streams a warp's contiguous blocks through kSpmvBuffers shared-memory buffers of
+// 4.6 KB: a chunk's blocks arrive with cp.async (every copy instruction moves 512 contiguous
+// bytes), each lane moves its item's block into registers, and the buffer at once takes the
+// copies of the chunk kSpmvBuffers ahead, which overlap the arithmetic of the chunks between.
+// x of the items' columns is loaded a chunk ahead into registers, the item records two chunks
+// ahead.  Warp v takes part v % kSpmvSplit of PCG range v / kSpmvSplit (by row groups), so the
+// ranges are the PCG's, at kSpmvSplit times the warps.
 constexpr int kSpmvRing = 64;
-constexpr int kSpmvBlocksPerSm = 6;   // twice the PCG's 3 blocks per SM: one wave
+constexpr int kSpmvBuffers = 2;
+constexpr int kSpmvSplit = 1;
+constexpr int kSpmvBlocksPerSm = 3;   // kSpmvSplit x the PCG's 3 blocks per SM: one wave of 12 warps per SM
+constexpr int kSpmvWarpFloats = kSpmvBuffers * 32 * 36 + kSpmvRing * 8 + 32 * 8;
+constexpr size_t kSpmvSmemBytes = sizeof(float) * (kPcgThreads / 32) * kSpmvWarpFloats;
 __device__ __forceinline__ void spmv_issue_blocks(const PcgArgs &A, uint32_t u, uint32_t u_end, float *buf, int lane) {
     const uint32_t nparts = u < u_end ? 9u * min(32u, u_end - u) : 0u;
     const float *src = A.sym_blocks + 36ull * u;
@@ -1498,18 +1502,18 @@ __device__ __forceinline__ void spmv_load_x(const PcgArgs &A, const float *x, ui
     }
 }
 __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs A, const float *x, float *y) {
-    __shared__ __align__(16) float buf_all[kPcgThreads / 32][32 * 36];          // the chunk's blocks
-    __shared__ __align__(16) float ring_all[kPcgThreads / 32][kSpmvRing * 8];   // x of recent rows, by row
-    __shared__ __align__(16) float prod_all[kPcgThreads / 32][32 * 8];          // each lane's B x_col
+    // per warp: the chunk buffers, x of recent rows (by row), each lane's B x_col
+    extern __shared__ __align__(16) float spmv_smem[];
     const int lane = threadIdx.x & 31;
-    float *buf = buf_all[threadIdx.x >> 5];
-    float *ring = ring_all[threadIdx.x >> 5];
-    float *prod = prod_all[threadIdx.x >> 5];
+    float *bufs = spmv_smem + (threadIdx.x >> 5) * kSpmvWarpFloats;
+    float *ring = bufs + kSpmvBuffers * 32 * 36;
+    float *prod = ring + kSpmvRing * 8;
     const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t pg0 = min(A.warp_groups[v >> 1], A.total_groups);
-    const uint32_t pg1 = max(pg0, min(A.warp_groups[(v >> 1) + 1], A.total_groups));
-    const uint32_t mid = pg0 + (pg1 - pg0 + 1) / 2;
-    const uint32_t g0 = (v & 1) ? mid : pg0, g1 = (v & 1) ? pg1 : mid;
+    const uint32_t pv = v / kSpmvSplit, part = v % kSpmvSplit;
+    const uint32_t pg0 = min(A.warp_groups[pv], A.total_groups);
+    const uint32_t pg1 = max(pg0, min(A.warp_groups[pv + 1], A.total_groups));
+    const uint32_t g0 = pg0 + ((pg1 - pg0) * part + kSpmvSplit - 1) / kSpmvSplit;
+    const uint32_t g1 = pg0 + ((pg1 - pg0) * (part + 1) + kSpmvSplit - 1) / kSpmvSplit;
     if (g0 >= g1) return;
     const uint32_t r0 = A.group_row[g0], r1 = g1 < A.total_groups ? A.group_row[g1] : A.total_nodes;
     const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
@@ -1518,10 +1522,13 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     float4 xa;
     float2 xb;
     spmv_load_x(A, x, cur, xa, xb);
-    spmv_issue_blocks(A, u0, u1, buf, lane);
+#pragma unroll
+    for (int k = 0; k < kSpmvBuffers; ++k) spmv_issue_blocks(A, u0 + 32u * k, u1, bufs + k * 32 * 36, lane);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
-    for (uint32_t u = u0; u < u1; u += 32) {
+    uint32_t chunk = 0;
+    for (uint32_t u = u0; u < u1; u += 32, ++chunk) {
+        float *buf = bufs + (chunk % kSpmvBuffers) * 32 * 36;
         const uint4 after = load_item(A.item_info, u + 64 + lane, u1);
         const bool valid = cur.z != kInvalidIndex;
         const uint32_t xrow = valid ? min(cur.z, A.total_nodes - 1) : kInvalidIndex;
@@ -1532,14 +1539,17 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
             rr[0] = xa;
             rr[1] = make_float4(xb.x, xb.y, 0.f, 0.f);
         }
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        // every copy group commits in order: this chunk's is done when at most the
+        // kSpmvBuffers - 1 later ones are pending
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kSpmvBuffers - 1) : "memory");
         __syncwarp();
         float4 b[9];
 #pragma unroll
         for (int q = 0; q < 9; ++q) b[q] = reinterpret_cast<const float4 *>(buf + 36 * lane)[q];
         __syncwarp();
-        // the buffer is free: the next chunk's blocks and x arrive while this one is computed
-        spmv_issue_blocks(A, u + 32, u1, buf, lane);
+        // the buffer is free: the blocks kSpmvBuffers chunks ahead and the next x arrive while
+        // this chunk is computed
+        spmv_issue_blocks(A, u + 32u * kSpmvBuffers, u1, buf, lane);
         spmv_load_x(A, x, nxt, xa, xb);
         float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
@@ -1946,9 +1956,12 @@ cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *u
 
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st) {
     const PcgArgs a = pcg_args(w, 0);
+    const cudaError_t attr =
+        cudaFuncSetAttribute(k_spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpmvSmemBytes);
+    if (attr != cudaSuccess) return attr;
     const cudaError_t e = cudaMemsetAsync(y, 0, 32ull * w.total_nodes, st);
     if (e != cudaSuccess) return e;
-    k_spmv<<<2 * pcg_launch_blocks(w), kPcgThreads, 0, st>>>(a, x, y);
+    k_spmv<<<kSpmvSplit * pcg_launch_blocks(w), kPcgThreads, kSpmvSmemBytes, st>>>(a, x, y);
     return cudaGetLastError();
 }
 
