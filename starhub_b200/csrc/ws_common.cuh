@@ -19,6 +19,7 @@ constexpr int kVecStride = 8;        // floats per node in PCG vectors
 constexpr int kDenseRecord = 32;     // floats per dense-term record, largest layout (128 B)
 constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
+constexpr uint32_t kItemRowStart = 0x80000000u;   // item_col: the row's first (diagonal) item
 constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group (divides 32)
 
 // Dense-term record layouts, chosen per batch.  With the optical-flow term (some scene of the

@@ -401,7 +401,7 @@ __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, co
                         const uint32_t *half_row, const uint32_t *half_col, const uint32_t *row_first,
                         const uint32_t *row_cnt_lo, const uint32_t *rowptr, const uint32_t *node_scene,
                         uint32_t cap_blocks, uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx,
-                        uint4 *item_info, int *err) {
+                        uint4 *item_info, uint32_t *item_col, int *err) {
     const uint32_t n = counts[kCntHalf];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t col = sorted_col[k];
@@ -425,18 +425,21 @@ __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, co
         colidx[s_lo] = row;
         colidx[s_up] = half_col[h];
         item_info[h + row + 1u] = make_uint4(half_col[h], k, row, node_scene[row]);
+        item_col[h + row + 1u] = half_col[h];
     }
 }
 
 // Diagonal slot of every row, plus the packed (col, ref, row, scene) record of each slot of
 // the row that the PCG streams.
 __global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *item_ptr, const uint32_t *node_scene,
-                            uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx, uint4 *item_info, int *err) {
+                            uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx, uint4 *item_info,
+                            uint32_t *item_col, int *err) {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         const uint32_t s = rowptr[g];
         if (s < cap_blocks) colidx[s] = g;
         // the row's first item is its diagonal block
         item_info[item_ptr[g]] = make_uint4(g, kInvalidIndex, g, node_scene[g]);
+        item_col[item_ptr[g]] = g | kItemRowStart;
         if (g + 1 == total_nodes && rowptr[total_nodes] > cap_blocks) set_error(err, WS_ERR_CAPACITY);
     }
 }
@@ -544,9 +547,9 @@ void index_build(Workspace &w, cudaStream_t st) {
     k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,
                                                                     w.row_first, w.row_cnt_lo, w.rowptr, w.node_scene,
                                                                     w.cap_blocks, w.half_slot_up, w.half_slot_lo, w.colidx,
-                                                                    w.item_info, w.error_flag);
+                                                                    w.item_info, w.item_col, w.error_flag);
     k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.item_ptr, w.node_scene, N, w.cap_blocks,
-                                                             w.colidx, w.item_info, w.error_flag);
+                                                             w.colidx, w.item_info, w.item_col, w.error_flag);
     count_launch(w, 2);
     pcg_ranges(w, st);
 }

@@ -868,6 +868,7 @@ struct PcgArgs {
     const uint32_t *rowptr;        // block-CSR row pointers (lower slots follow the diagonal)
     const uint32_t *item_ptr;      // [nodes + 1] first item of every row in the symmetric store
     const uint4 *item_info;        // per item: column, CSR slot of the transposed use, row, scene
+    const uint32_t *item_col;      // per item: column | kItemRowStart on a row's diagonal item
     const uint32_t *warp_groups;   // [warps + 1] first row group of each warp
     const float *sym_blocks;       // per item: the 6x6 block, row-major
     const float *inv_diag, *jtr;
@@ -1473,8 +1474,8 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 // 4.6 KB: a chunk's blocks arrive with cp.async (every copy instruction moves 512 contiguous
 // bytes), each lane moves its item's block into registers, and the buffer at once takes the
 // copies of the chunk kSpmvBuffers ahead, which overlap the arithmetic of the chunks between.
-// x of the items' columns is loaded a chunk ahead into registers, the item records two chunks
-// ahead.  Warp v takes part v % kSpmvSplit of PCG range v / kSpmvSplit (by row groups), so the
+// x of the items' columns is loaded a chunk ahead into registers, the items' 4-byte column
+// words (item_col: the column, with the row's start marked) two chunks ahead.  Warp v takes part v % kSpmvSplit of PCG range v / kSpmvSplit (by row groups), so the
 // ranges are the PCG's, at kSpmvSplit times the warps.
 constexpr int kSpmvRing = 64;
 constexpr int kSpmvBuffers = 2;
@@ -1492,11 +1493,16 @@ __device__ __forceinline__ void spmv_issue_blocks(const PcgArgs &A, uint32_t u, 
     }
     cp_async_commit();
 }
-__device__ __forceinline__ void spmv_load_x(const PcgArgs &A, const float *x, uint4 it, float4 &x0, float2 &x1) {
+// Item word of the standalone SpMV: column | kItemRowStart on a row's first (diagonal) item,
+// kInvalidIndex past the end of the range.
+__device__ __forceinline__ uint32_t load_col(const uint32_t *cols, uint32_t u, uint32_t end) {
+    return u < end ? __ldg(cols + u) : kInvalidIndex;
+}
+__device__ __forceinline__ void spmv_load_x(const PcgArgs &A, const float *x, uint32_t word, float4 &x0, float2 &x1) {
     x0 = make_float4(0.f, 0.f, 0.f, 0.f);
     x1 = make_float2(0.f, 0.f);
-    if (it.z != kInvalidIndex) {
-        const uint32_t col = min(it.x, A.total_nodes - 1);
+    if (word != kInvalidIndex) {
+        const uint32_t col = min(word & ~kItemRowStart, A.total_nodes - 1);
         x0 = __ldg(reinterpret_cast<const float4 *>(x + 8ull * col));
         x1 = __ldg(reinterpret_cast<const float2 *>(x + 8ull * col + 4));
     }
@@ -1517,8 +1523,8 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     if (g0 >= g1) return;
     const uint32_t r0 = A.group_row[g0], r1 = g1 < A.total_groups ? A.group_row[g1] : A.total_nodes;
     const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
-    uint4 cur = load_item(A.item_info, u0 + lane, u1);
-    uint4 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
+    uint32_t cur = load_col(A.item_col, u0 + lane, u1);
+    uint32_t nxt = load_col(A.item_col, u0 + 32 + lane, u1);
     float4 xa;
     float2 xb;
     spmv_load_x(A, x, cur, xa, xb);
@@ -1526,13 +1532,19 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     for (int k = 0; k < kSpmvBuffers; ++k) spmv_issue_blocks(A, u0 + 32u * k, u1, bufs + k * 32 * 36, lane);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
+    // the row of the item before the chunk; the range starts with row r0's diagonal item, so
+    // an item's row is this plus the row starts up to and including it (unsigned wrap at r0 = 0)
+    uint32_t row_before = r0 - 1u;
     uint32_t chunk = 0;
     for (uint32_t u = u0; u < u1; u += 32, ++chunk) {
         float *buf = bufs + (chunk % kSpmvBuffers) * 32 * 36;
-        const uint4 after = load_item(A.item_info, u + 64 + lane, u1);
-        const bool valid = cur.z != kInvalidIndex;
-        const uint32_t xrow = valid ? min(cur.z, A.total_nodes - 1) : kInvalidIndex;
-        const bool diag = cur.y == kInvalidIndex;
+        const uint32_t after = load_col(A.item_col, u + 64 + lane, u1);
+        const bool valid = cur != kInvalidIndex;
+        const bool diag = valid && (cur & kItemRowStart) != 0;
+        const unsigned row_starts = __ballot_sync(0xffffffffu, diag);
+        const uint32_t row = row_before + (uint32_t)__popc(row_starts & (0xffffffffu >> (31 - lane)));
+        row_before += (uint32_t)__popc(row_starts);
+        const uint32_t xrow = valid ? min(row, A.total_nodes - 1) : kInvalidIndex;
         const float xc[6] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y};
         if (valid && diag) {   // a row's first item: publish x of the row for its later items
             float4 *rr = reinterpret_cast<float4 *>(ring + 8 * (xrow & (kSpmvRing - 1)));
@@ -1568,7 +1580,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
                 }
             }
             if (!diag) {
-                float *yc = y + 8ull * min(cur.x, A.total_nodes - 1);
+                float *yc = y + 8ull * min(cur & ~kItemRowStart, A.total_nodes - 1);
                 atomicAdd(reinterpret_cast<float4 *>(yc), make_float4(t[0], t[1], t[2], t[3]));
                 atomicAdd(reinterpret_cast<float2 *>(yc + 4), make_float2(t[4], t[5]));
             }
@@ -1577,15 +1589,15 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         }
         __syncwarp();
         // row segments of this chunk, summed in item order by the lane that ends them
-        const uint32_t next_first = __shfl_sync(0xffffffffu, nxt.z, 0);
-        const uint32_t row_up = __shfl_up_sync(0xffffffffu, xrow, 1);
-        const uint32_t row_dn = __shfl_down_sync(0xffffffffu, xrow, 1);
-        const uint32_t following = (lane == 31) ? next_first : row_dn;
-        const bool starts = valid && (lane == 0 || row_up != xrow);
+        // an item ends its row when the next item starts another row or the range ends
+        const uint32_t next_first = __shfl_sync(0xffffffffu, nxt, 0);
+        const uint32_t word_dn = __shfl_down_sync(0xffffffffu, cur, 1);
+        const uint32_t following = (lane == 31) ? next_first : word_dn;
+        const bool starts = valid && (lane == 0 || diag);
         const unsigned start_mask = __ballot_sync(0xffffffffu, starts);
         const unsigned valid_mask = __ballot_sync(0xffffffffu, valid);
         const int last = 31 - __clz(valid_mask);
-        const bool ends_row = valid && following != xrow;
+        const bool ends_row = valid && (following == kInvalidIndex || (following & kItemRowStart) != 0);
         const bool owner = valid && (ends_row || lane == last);
         float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (owner) {
@@ -1902,6 +1914,7 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.rowptr = w.rowptr;
     a.item_ptr = w.item_ptr;
     a.item_info = w.item_info;
+    a.item_col = w.item_col;
     a.contrib = w.contrib;
     a.warp_groups = w.pcg_warp_groups;
     a.sym_blocks = w.sym_blocks;

@@ -94,6 +94,9 @@ struct Workspace {
     uint32_t cap_items = 0;                                  // cap_nodes + cap_half
     uint32_t *item_ptr = nullptr;                            // [cap_nodes + 1]
     uint4 *item_info = nullptr;                              // [cap_items]
+    // Per item, 4 bytes for the standalone SpMV: the column, with kItemRowStart set on a row's
+    // first (diagonal) item; rows follow from counting those marks.
+    uint32_t *item_col = nullptr;                            // [cap_items]
     float *sym_blocks = nullptr;                             // [cap_items * 36]
     float *contrib = nullptr;                                // [cap_half * 8]
     uint32_t *pcg_warp_groups = nullptr;                     // [pcg_grid * warps per block + 1]
