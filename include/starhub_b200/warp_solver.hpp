@@ -8,7 +8,11 @@
 //   * star::b200::OptimizationProcessorWarpSolver mirrors the processor entry
 //     (examples/mono_star/opt/OptimizationProcessorWarpSolver.h:18-30):
 //     ProcessFrame (frame 0 is a no-op, OptimizationProcessorWarpSolver.cu:35-36)
-//     and SolvedSE3.
+//     and SolvedSE3;
+//   * star::b200::NodeGraph mirrors the node construction and growth of
+//     star::NodeGraph (libs/star/geometry/node_graph/NodeGraph.h:23-60):
+//     InitializeNodeGraphFromVertex, NaiveExpandNodeGraphFromVertexUnsupported,
+//     BuildNodeGraphFromScratch and the accessors of the node arrays.
 // Maps arrive as cudaTextureObject_t like in Measure4Solver / Render4Solver
 // (libs/star/opt/solver_types.h:21-37); TextureMap resolves a texture object to
 // the pitch-linear device array the C ABI reads (pitch-2D resources are used in
@@ -17,6 +21,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -164,6 +169,111 @@ private:
     WarpSolver solver_;
     int gn_, pcg_;
     bool solved_ = false;
+};
+
+// star::NodeGraph's node construction and growth over ws_init_nodes, ws_expand_nodes and
+// ws_build_node_graph.  The node arrays are device memory owned here and sized for max_nodes,
+// like the reference's preallocation; GetNodeKnn returns k ids per node, edges are (i, knn, k).
+class NodeGraph {
+public:
+    NodeGraph(float node_radius, int max_nodes, int knn = 4) : radius_(node_radius), cap_(max_nodes), k_(knn) {
+        if (!(node_radius > 0.f) || max_nodes < 2 || max_nodes > 65535 || (knn != 4 && knn != 8))
+            throw Error(WS_ERR_INVALID_ARGUMENT, "NodeGraph");
+        try {
+            alloc(&ref_, 16ull * cap_);
+            alloc(&live_, 16ull * cap_);
+            alloc(&time_, 4ull * cap_);
+            alloc(&knn_, 2ull * k_ * cap_);
+            alloc(&weight_, 4ull * k_ * cap_);
+            alloc(&edges_, 6ull * k_ * cap_);
+        } catch (...) {
+            release();
+            throw;
+        }
+    }
+    ~NodeGraph() { release(); }
+    NodeGraph(const NodeGraph &) = delete;
+    NodeGraph &operator=(const NodeGraph &) = delete;
+
+    // InitializeNodeGraphFromVertex (NodeGraph.cu:460-498): nodes from `vertex` (device float4),
+    // two anchors first, reference = live coordinates, initial time `current_time`, then the graph.
+    void InitializeNodeGraphFromVertex(const float4 *vertex, unsigned num_vertex, unsigned current_time, bool use_ref,
+                                       cudaStream_t stream = 0) {
+        std::vector<float4> host((size_t)cap_);
+        int n = 0;
+        check(ws_init_nodes(reinterpret_cast<const float *>(vertex), (int)num_vertex, radius_,
+                            reinterpret_cast<float *>(host.data()), cap_, &n, stream),
+              "InitializeNodeGraphFromVertex");
+        const std::vector<unsigned> times((size_t)n, current_time);
+        check(cudaMemcpyAsync(ref_, host.data(), 16ull * n, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
+                      cudaMemcpyAsync(live_, host.data(), 16ull * n, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
+                      cudaMemcpyAsync(time_, times.data(), 4ull * n, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
+                      cudaStreamSynchronize(stream) == cudaSuccess
+                  ? WS_OK
+                  : WS_ERR_CUDA,
+              "InitializeNodeGraphFromVertex");
+        prev_size_ = 0;
+        size_ = (unsigned)n;
+        BuildNodeGraphFromScratch(use_ref, stream);
+    }
+
+    // NaiveExpandNodeGraphFromVertexUnsupported (NodeGraph.cu:500-532): appends the greedy
+    // nodes of `vertex_unsupported` (device float4) to both coordinate arrays with initial time
+    // `current_time`.  The graph is rebuilt by a later BuildNodeGraphFromScratch, as there.
+    void NaiveExpandNodeGraphFromVertexUnsupported(const float4 *vertex_unsupported, unsigned num_vertex,
+                                                   unsigned current_time, cudaStream_t stream) {
+        int n = (int)size_;
+        check(ws_expand_nodes(reinterpret_cast<const float *>(vertex_unsupported), (int)num_vertex, radius_,
+                              reinterpret_cast<float *>(ref_), reinterpret_cast<float *>(live_), time_, current_time,
+                              cap_, &n, stream),
+              "NaiveExpandNodeGraphFromVertexUnsupported");
+        prev_size_ = size_;
+        size_ = (unsigned)n;
+    }
+
+    // BuildNodeGraphFromScratch (NodeGraph.cu:357-365): k-NN graph of the reference (use_ref)
+    // or live coordinates.
+    void BuildNodeGraphFromScratch(bool use_ref, cudaStream_t stream) {
+        if (size_ == 0) return;
+        check(ws_build_node_graph(reinterpret_cast<const float *>(use_ref ? ref_ : live_), (int)size_, k_, radius_,
+                                  knn_, weight_, edges_, stream),
+              "BuildNodeGraphFromScratch");
+    }
+
+    const float4 *GetReferenceNodeCoordinate() const { return ref_; }
+    const float4 *GetLiveNodeCoordinate() const { return live_; }
+    const uint16_t *GetNodeKnn() const { return knn_; }
+    const float *GetNodeKnnSpatialWeight() const { return weight_; }
+    const uint16_t *GetNodeGraph() const { return edges_; }
+    const unsigned *GetNodeInitialTime() const { return time_; }
+    unsigned GetNodeSize() const { return size_; }
+    unsigned GetPrevNodeSize() const { return prev_size_; }
+    float GetNodeRadiusSquare() const { return radius_ * radius_; }
+
+private:
+    template <class T>
+    static void alloc(T **p, size_t bytes) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) throw Error(WS_ERR_CUDA, "NodeGraph allocation");
+        *p = static_cast<T *>(q);
+    }
+    void release() {
+        void *ptrs[] = {ref_, live_, time_, knn_, weight_, edges_};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        ref_ = live_ = nullptr;
+        time_ = nullptr;
+        knn_ = edges_ = nullptr;
+        weight_ = nullptr;
+    }
+
+    float radius_;
+    int cap_, k_;
+    unsigned size_ = 0, prev_size_ = 0;
+    float4 *ref_ = nullptr, *live_ = nullptr;
+    unsigned *time_ = nullptr;
+    uint16_t *knn_ = nullptr, *edges_ = nullptr;
+    float *weight_ = nullptr;
 };
 
 }  // namespace b200

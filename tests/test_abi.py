@@ -58,3 +58,32 @@ def test_default_penalties_match_reference(lib):
     # PenaltyConstants::setDefaultValue (examples/mono_star/opt/PenaltyConstants.cu:8-15)
     assert (round(s.lambda_depth, 6), s.lambda_optical_flow, s.lambda_reg, s.lambda_node_translation,
             s.lambda_feature) == (0.1, 0.0, 1.0, 0.0, 1.0)
+
+
+def test_cpp_facade_builds_and_links(lib, tmp_path):
+    """The header-only C++ facade (include/starhub_b200/warp_solver.hpp) compiles and links
+    against the library: every entry point its classes call is exported."""
+    import shutil
+    import subprocess
+    cuda = Path("/usr/local/cuda")
+    if shutil.which("g++") is None or not (cuda / "include" / "cuda_runtime.h").exists():
+        pytest.skip("g++ or the CUDA headers are missing")
+    src = tmp_path / "facade.cpp"
+    src.write_text(
+        '#include "starhub_b200/warp_solver.hpp"\n'
+        "using namespace star::b200;\n"
+        "int use(const float4 *v, unsigned n, cudaStream_t st) {\n"
+        "  NodeGraph g(0.025f, 4096, 8);\n"
+        "  g.InitializeNodeGraphFromVertex(v, n, 0, true, st);\n"
+        "  g.NaiveExpandNodeGraphFromVertexUnsupported(v, n, 1, st);\n"
+        "  g.BuildNodeGraphFromScratch(false, st);\n"
+        "  OptimizationProcessorWarpSolver p(4096, 640 * 480, 4096 * 8);\n"
+        "  return (int)g.GetNodeSize() + (p.SolvedSE3() != nullptr);\n"
+        "}\n"
+        "int main(int argc, char **) { return argc > 100 ? use(nullptr, 0, 0) : 0; }\n")
+    lib_dir = ROOT / "starhub_b200"
+    cmd = ["g++", "-std=c++17", "-Wall", "-Wextra", "-I", str(ROOT / "include"), "-I", str(cuda / "include"),
+           str(src), "-o", str(tmp_path / "facade"), "-L", str(lib_dir), "-lwarpsolve", "-L", str(cuda / "lib64"),
+           "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
