@@ -113,3 +113,98 @@ def test_node_graph_ties(ws, orc, order, k):
     np.testing.assert_array_equal(gk, ok)
     np.testing.assert_array_equal(ge, oe)
     np.testing.assert_allclose(gw, ow, rtol=2e-5, atol=1e-7)
+
+
+FACADE_PROGRAM = r"""
+#include <cstdio>
+#include <vector>
+#include "starhub_b200/warp_solver.hpp"
+
+static std::vector<float4> read_points(const char *path) {
+    std::vector<float4> v;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return v;
+    float4 p;
+    while (std::fread(&p, sizeof(p), 1, f) == 1) v.push_back(p);
+    std::fclose(f);
+    return v;
+}
+
+int main(int argc, char **argv) {
+    if (argc != 4) return 2;
+    const std::vector<float4> first = read_points(argv[1]), more = read_points(argv[2]);
+    float4 *d_first = nullptr, *d_more = nullptr;
+    cudaMalloc(&d_first, 16 * first.size());
+    cudaMalloc(&d_more, 16 * more.size());
+    cudaMemcpy(d_first, first.data(), 16 * first.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_more, more.data(), 16 * more.size(), cudaMemcpyHostToDevice);
+    star::b200::NodeGraph graph(0.01f, 32768, 4);   // 8,936 + 8,947 nodes
+    graph.InitializeNodeGraphFromVertex(d_first, (unsigned)first.size(), 3, true, 0);
+    const unsigned n0 = graph.GetNodeSize();
+    graph.NaiveExpandNodeGraphFromVertexUnsupported(d_more, (unsigned)more.size(), 5, 0);
+    graph.BuildNodeGraphFromScratch(true, 0);
+    const unsigned n = graph.GetNodeSize();
+    std::vector<float4> nodes(n);
+    std::vector<uint16_t> knn(4ull * n);
+    std::vector<unsigned> times(n);
+    cudaMemcpy(nodes.data(), graph.GetReferenceNodeCoordinate(), 16ull * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(knn.data(), graph.GetNodeKnn(), 8ull * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(times.data(), graph.GetNodeInitialTime(), 4ull * n, cudaMemcpyDeviceToHost);
+    FILE *f = std::fopen(argv[3], "wb");
+    std::fwrite(&n0, 4, 1, f);
+    std::fwrite(&n, 4, 1, f);
+    std::fwrite(nodes.data(), 16, n, f);
+    std::fwrite(knn.data(), 2, 4ull * n, f);
+    std::fwrite(times.data(), 4, n, f);
+    std::fclose(f);
+    cudaFree(d_first);
+    cudaFree(d_more);
+    return graph.GetPrevNodeSize() == n0 ? 0 : 3;
+}
+"""
+
+
+def test_cpp_facade_node_graph_matches_the_c_abi(ws, orc, tmp_path):
+    """star::b200::NodeGraph (the C++ facade) gives the nodes, graph and initial times of the
+    C ABI calls it wraps, which the oracle checks above."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+    from starhub_b200.solver import GpuGeometry
+    root = Path(__file__).resolve().parents[1]
+    cuda = Path("/usr/local/cuda")
+    if shutil.which("g++") is None:
+        pytest.skip("g++ missing")
+    s = torus_surfels(200_000, 41)
+    first, more = s[:100_000], s[100_000:]
+    (tmp_path / "first.bin").write_bytes(first.tobytes())
+    (tmp_path / "more.bin").write_bytes(more.tobytes())
+    (tmp_path / "prog.cpp").write_text(FACADE_PROGRAM)
+    lib_dir = root / "starhub_b200"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(root / "include"), "-I", str(cuda / "include"),
+                        str(tmp_path / "prog.cpp"), "-o", str(tmp_path / "prog"), "-L", str(lib_dir), "-lwarpsolve",
+                        f"-Wl,-rpath,{lib_dir}", "-L", str(cuda / "lib64"), "-lcudart"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(tmp_path / "prog"), str(tmp_path / "first.bin"), str(tmp_path / "more.bin"),
+                        str(tmp_path / "out.bin")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    raw = (tmp_path / "out.bin").read_bytes()
+    n0, n = np.frombuffer(raw[:8], np.uint32)
+    off = 8
+    nodes = np.frombuffer(raw[off:off + 16 * n], np.float32).reshape(n, 4); off += 16 * n
+    knn = np.frombuffer(raw[off:off + 8 * n], np.uint16).reshape(n, 4); off += 8 * n
+    times = np.frombuffer(raw[off:off + 4 * n], np.uint32)
+
+    geo = GpuGeometry()
+    base = geo.init_nodes(first, 0.01)
+    assert n0 == len(base)
+    dev = torch.device("cuda")
+    ref = torch.zeros((32768, 4), dtype=torch.float32, device=dev)
+    ref[: len(base)] = torch.from_numpy(base).to(dev)
+    total = geo.expand_nodes(ref, None, len(base), more, 0.01)
+    assert n == total
+    want = ref[:total].cpu().numpy()
+    np.testing.assert_array_equal(nodes, want)
+    wk, _, _ = geo.node_graph(want, 4, 0.01)
+    np.testing.assert_array_equal(knn, wk)
+    assert (times[:n0] == 3).all() and (times[n0:] == 5).all()
