@@ -127,6 +127,11 @@ int ws_get_solution(ws_solver *solver, int scene, const float **dev_node_se3, in
  * The products meet in y through atomic adds, so y may differ in the last bits between calls.
  * Asynchronous on `stream`; WS_ERR_NOT_READY before the first solve. */
 int ws_spmv(ws_solver *solver, const float *x, float *y, void *stream);
+/* Failure-detection self-test, no reference counterpart (the reference has no bounded waits):
+ * one warp runs the PCG's scene wait on a generation counter that nothing advances.  Returns
+ * WS_ERR_TIMEOUT after about two seconds of requested sleep when the bound works (the device
+ * stays usable), WS_ERR_CUDA if a CUDA call fails.  Synchronises `stream`. */
+int ws_selftest_wait_timeout(void *stream);
 /* The same operator applied matrix-free from the term records of the last Gauss-Newton
  * iteration (J x per term, then J^T (J x) gathered per node over the node->term lists, plus
  * the diagonal regulariser), without the assembled blocks.  No reference counterpart (the

@@ -557,6 +557,12 @@ int ws_spmv(ws_solver *h, const float *x, float *y, void *stream) {
     return ws::gn_spmv(w, x, y, (cudaStream_t)stream) == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }
 
+int ws_selftest_wait_timeout(void *stream) {
+    int status = 0;
+    if (ws::pcg_wait_selftest(&status, (cudaStream_t)stream) != cudaSuccess) return WS_ERR_CUDA;
+    return status == 0 ? WS_OK : status;
+}
+
 int ws_spmv_matrix_free(ws_solver *h, const float *x, float *y, void *stream) {
     if (!h || !x || !y) return WS_ERR_INVALID_ARGUMENT;
     ws::Workspace &w = h->w;

@@ -965,6 +965,38 @@ __device__ bool wait_scenes(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, 
     return ok;
 }
 
+// Failure-detection self-test: one warp runs wait_scenes on one scene whose generation
+// nothing advances.  With the bound in place it gives up after about two seconds of requested
+// sleep and leaves WS_ERR_TIMEOUT in `err`; the launch then ends like any other.
+__global__ void k_wait_selftest(PcgArgs A) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) wait_scenes(A, 0u, 1u, 0, 1u, lane);
+}
+
+cudaError_t pcg_wait_selftest(int *status, cudaStream_t st) {
+    // scene_counter: one scene's kSceneSync words, all zero; group_scene: group 0 -> scene 0; err
+    uint32_t *words = nullptr;
+    const size_t n_words = kSceneSync + 1 + 1;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&words), 4 * n_words, st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(words, 0, 4 * n_words, st);
+    PcgArgs a{};
+    a.scene_counter = words;
+    a.group_scene = words + kSceneSync;
+    a.err = reinterpret_cast<int *>(words + kSceneSync + 1);
+    int flag = 0;
+    if (e == cudaSuccess) {
+        k_wait_selftest<<<1, 32, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, a.err, 4, cudaMemcpyDeviceToHost, st);
+    const cudaError_t f = cudaFreeAsync(words, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = f;
+    *status = flag;
+    return e;
+}
+
 // `phase` counts the publications of the counter: phase A(it) is phase it of counter 0; init
 // is phase 0 and phase B(it) phase it + 1 of counter 1.  The tickets only grow during a
 // launch, so the arrival that brings them to (phase + 1) times the scene's group count is

@@ -166,3 +166,21 @@ def test_wide_pair_keys_give_the_narrow_results(ws, tiny_scene):
     np.testing.assert_array_equal(batch[-1], solo_b)
     np.testing.assert_array_equal(batch[0], solo_t)
     np.testing.assert_array_equal(batch[63], solo_t)
+
+
+def test_pcg_wait_gives_up_and_the_device_stays_usable(ws, tiny_scene):
+    """The PCG's scene wait is bounded: on a generation counter that nothing advances it
+    returns WS_ERR_TIMEOUT (about two seconds of requested sleep), no GPU fault, and a solve
+    on the same device afterwards succeeds and equals one before it."""
+    import time
+    from starhub_b200 import _lib
+    from starhub_b200.solver import DeviceScene
+    ds = DeviceScene.from_scene(tiny_scene)
+    (before,) = _solve([ds])
+    t0 = time.perf_counter()
+    status = _lib.load().ws_selftest_wait_timeout(None)
+    elapsed = time.perf_counter() - t0
+    assert status == _lib.WS_ERR_TIMEOUT
+    assert 0.05 < elapsed < 60.0
+    (after,) = _solve([ds])
+    np.testing.assert_array_equal(after, before)
