@@ -217,18 +217,19 @@ __global__ void k_dedup_neighbours(const float4 *cand, const uint32_t *cell_keys
     }
 }
 
-// The rounds, in one block of 1024 threads.  Decisions (0 open, 1 kept, 2 rejected) live in
-// shared memory when nv bytes fit, else in `decision`; they are read volatile, so a decision
-// taken earlier in the same round is used at once.  Thread t walks candidates t, t + 1024, ...
-// from the first one it has not yet settled.  On return `decision` holds every decision;
-// `err` is set only if nv + 1 rounds left a candidate open, which the argument above excludes.
+// The rounds for small candidate sets (at most kDedupOneBlockMax), in one block of 1024
+// threads.  Decisions (0 open, 1 kept, 2 rejected) live in shared memory, one byte per
+// candidate, and are read volatile, so a decision taken earlier in the same round is used at
+// once.  Thread t walks candidates t, t + 1024, ... from the first one it has not yet settled.
+// On return `decision` holds every decision; `err` is set only if nv + 1 rounds left a
+// candidate open, which the argument above excludes.
 constexpr int kDedupThreads = 1024;
-constexpr uint32_t kDedupSharedMax = 160 * 1024;
+constexpr uint32_t kDedupOneBlockMax = 16384;
 
 __global__ void __launch_bounds__(kDedupThreads) k_dedup_greedy(const uint32_t *nbr_ptr, const uint32_t *nbr, uint32_t nv,
-                                                                uint8_t *decision, int in_shared, int *err) {
+                                                                uint8_t *decision, int *err) {
     extern __shared__ uint8_t s_decision[];
-    volatile uint8_t *dec = in_shared ? s_decision : decision;
+    volatile uint8_t *dec = s_decision;
     for (uint32_t i = threadIdx.x; i < nv; i += kDedupThreads) dec[i] = 0;
     __syncthreads();
     uint32_t first = threadIdx.x;
@@ -257,8 +258,87 @@ __global__ void __launch_bounds__(kDedupThreads) k_dedup_greedy(const uint32_t *
         done = !__syncthreads_or(open);
     }
     if (!done && threadIdx.x == 0) atomicOr(err, 2);
-    if (in_shared)
-        for (uint32_t i = threadIdx.x; i < nv; i += kDedupThreads) decision[i] = s_decision[i];
+    for (uint32_t i = threadIdx.x; i < nv; i += kDedupThreads) decision[i] = s_decision[i];
+}
+
+// The same rounds over the whole GPU, for large candidate sets.  One launch whose blocks are
+// all resident (a cooperative launch); thread t takes candidates t, t + T, ... (T threads in
+// all); decisions in global memory (zeroed before the launch), read volatile; a barrier of our
+// own between rounds.  sync[0] counts a barrier's arrivals, sync[1] is its generation, and
+// sync[2 + r % 2] says whether round r left a candidate open: every write to it comes before
+// round r's barrier, so all threads read the same value after it, and the barrier's last
+// arrival clears the other word for round r + 1 (its readers, in round r - 1, have all arrived).
+// A barrier wait sleeps with backoff and gives up after about two seconds of requested sleep,
+// or at once when another block has: `err` gets 4 and the blocks leave.
+constexpr int kDedupGridThreads = 512;
+constexpr unsigned long long kDedupBarrierTimeoutNs = 2000000000ull;
+
+__device__ bool dedup_grid_barrier(unsigned *sync, unsigned clear_word, int *err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned *gen = sync + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
+            atomicExch(sync + clear_word, 0u);
+            atomicExch(sync, 0u);
+            __threadfence();
+            atomicAdd(sync + 1, 1u);
+        } else {
+            unsigned long long waited_ns = 0;
+            unsigned sleep_ns = 32;
+            while (*gen == g) {
+                if (waited_ns > kDedupBarrierTimeoutNs || (*reinterpret_cast<volatile int *>(err) & 4) != 0) {
+                    atomicOr(err, 4);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(sleep_ns);
+                waited_ns += sleep_ns;
+                sleep_ns = min(sleep_ns * 2u, 256u);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__global__ void __launch_bounds__(kDedupGridThreads) k_dedup_greedy_grid(const uint32_t *nbr_ptr, const uint32_t *nbr,
+                                                                        uint32_t nv, uint8_t *decision, unsigned *sync,
+                                                                        int *err) {
+    volatile uint8_t *dec = decision;
+    const uint32_t threads = gridDim.x * blockDim.x;
+    uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t round = 0; round <= nv; ++round) {   // uniform: the exit reads a word written before the barrier
+        int open = 0;
+        bool settled_prefix = true;
+        for (uint32_t i = first; i < nv; i += threads) {
+            uint8_t d = dec[i];
+            if (d == 0) {
+                d = 1;
+                for (uint32_t k = __ldg(nbr_ptr + i), e = __ldg(nbr_ptr + i + 1); k < e; ++k) {
+                    const uint8_t t = dec[__ldg(nbr + k)];
+                    if (t == 1) { d = 2; break; }
+                    if (t == 0) d = 0;
+                }
+                if (d != 0) dec[i] = d;
+            }
+            if (d == 0) {
+                open = 1;
+                settled_prefix = false;
+            } else if (settled_prefix) {
+                first = i + threads;
+            }
+        }
+        volatile unsigned *flag = sync + 2 + (round & 1);
+        if (open) *flag = 1u;
+        if (!dedup_grid_barrier(sync, 2 + ((round + 1) & 1), err)) return;
+        if (*flag == 0u) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, 2);
 }
 
 __global__ void k_dedup_flags(const uint8_t *decision, uint32_t nv, uint32_t *flags) {
@@ -576,11 +656,29 @@ int grow_nodes(const float4 *pts, uint32_t n, float node_radius, DeviceBlocks &m
     if (mem.err != cudaSuccess) return WS_ERR_CUDA;
     ws::k_dedup_neighbours<true><<<ws::grid_of(nv, 128), 128, 0, st>>>(cand, ck, ci, nv, inv_cell, thr, cnt, nbr);
     uint8_t *decision = reinterpret_cast<uint8_t *>(spare_keys);
-    const int in_shared = nv <= ws::kDedupSharedMax ? 1 : 0;
-    if (cudaFuncSetAttribute(ws::k_dedup_greedy, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ws::kDedupSharedMax) != cudaSuccess)
-        return WS_ERR_CUDA;
-    ws::k_dedup_greedy<<<1, ws::kDedupThreads, in_shared ? nv : 0, st>>>(cnt, nbr, nv, decision, in_shared, err);
+    if (nv <= ws::kDedupOneBlockMax) {   // 16 KB of shared memory at most
+        ws::k_dedup_greedy<<<1, ws::kDedupThreads, nv, st>>>(cnt, nbr, nv, decision, err);
+    } else {
+        unsigned *sync = mem.get<unsigned>(16);
+        int dev = 0, sms = 0, per_sm = 0, coop = 0;
+        if (mem.err != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ws::k_dedup_greedy_grid, ws::kDedupGridThreads, 0) !=
+                cudaSuccess ||
+            per_sm < 1)
+            return WS_ERR_CUDA;
+        const long long want = ((long long)nv + ws::kDedupGridThreads - 1) / ws::kDedupGridThreads;
+        const int grid = (int)std::min<long long>(want, (long long)per_sm * sms);
+        if (cudaMemsetAsync(decision, 0, nv, st) != cudaSuccess || cudaMemsetAsync(sync, 0, 16, st) != cudaSuccess)
+            return WS_ERR_CUDA;
+        const uint32_t *nbr_ptr = cnt;
+        uint32_t nv_arg = nv;
+        void *args[] = {(void *)&nbr_ptr, (void *)&nbr, (void *)&nv_arg, (void *)&decision, (void *)&sync, (void *)&err};
+        if (cudaLaunchCooperativeKernel((const void *)ws::k_dedup_greedy_grid, dim3(grid), dim3(ws::kDedupGridThreads),
+                                        args, 0, st) != cudaSuccess)
+            return WS_ERR_CUDA;
+    }
     uint32_t *pos = spare_vals;
     ws::k_dedup_flags<<<ws::grid_of(nv, 256), 256, 0, st>>>(decision, nv, pos);
     ws::exclusive_scan(pos, pos, nullptr, nv, nv, tmp, st);
@@ -591,6 +689,7 @@ int grow_nodes(const float4 *pts, uint32_t n, float node_radius, DeviceBlocks &m
         cudaMemcpyAsync(&flag, err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return WS_ERR_CUDA;
+    if (flag & 4) return WS_ERR_TIMEOUT;
     if (flag & 2) return WS_ERR_CUDA;
     *kept = count;
     return WS_OK;

@@ -1,9 +1,9 @@
 """Node-graph growth on the GPU, bit-exact to the oracle.
 
 * ws_init_nodes: voxel subsample plus the greedy overlap check of
-  AppendNodeFromVertexHost (NodeGraph.cu:652-704), run on the device in rounds; scenes with
-  up to 200k candidates, so that the decisions live in shared memory in one case and in
-  global memory in the other.
+  AppendNodeFromVertexHost (NodeGraph.cu:652-704), run on the device in rounds; scenes from
+  a few thousand candidates (one block, decisions in shared memory) to 200k (a cooperative
+  launch over all SMs with a grid barrier between rounds).
 * ws_expand_nodes: NaiveExpandNodeGraphFromVertexUnsupported (NodeGraph.cu:500-532) appends
   the greedy nodes of the unsupported vertices, sets their initial time, and leaves the
   arrays alone when they are full.
@@ -15,7 +15,7 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-DEDUP_SHARED_MAX = 160 * 1024
+DEDUP_ONE_BLOCK_MAX = 16384
 
 
 def torus_surfels(n, seed):
@@ -26,13 +26,14 @@ def torus_surfels(n, seed):
     return scenes.pack4(p, 1.0)
 
 
-@pytest.mark.parametrize("n,radius,decisions", [(1_000_000, 0.006, "shared"), (2_500_000, 0.004, "global")])
-def test_init_nodes_many_candidates_bit_exact(ws, orc, n, radius, decisions):
+@pytest.mark.parametrize("n,radius,rounds_on", [(100_000, 0.025, "one block"), (1_000_000, 0.006, "grid"),
+                                                (2_500_000, 0.004, "grid")])
+def test_init_nodes_many_candidates_bit_exact(ws, orc, n, radius, rounds_on):
     from starhub_b200.solver import GpuGeometry
     s = torus_surfels(n, 31)
     og = orc.OracleGeometry()
     candidates = og.voxel_subsample(s, np.float32(0.7) * np.float32(radius)).shape[0]
-    assert (candidates > DEDUP_SHARED_MAX) == (decisions == "global")
+    assert (candidates > DEDUP_ONE_BLOCK_MAX) == (rounds_on == "grid")
     g = GpuGeometry().init_nodes(s, radius)
     o = og.init_nodes(s, radius)
     assert g.shape == o.shape
