@@ -676,8 +676,10 @@ int grow_nodes(const float4 *pts, uint32_t n, float node_radius, DeviceBlocks &m
         uint32_t nv_arg = nv;
         void *args[] = {(void *)&nbr_ptr, (void *)&nbr, (void *)&nv_arg, (void *)&decision, (void *)&sync, (void *)&err};
         if (cudaLaunchCooperativeKernel((const void *)ws::k_dedup_greedy_grid, dim3(grid), dim3(ws::kDedupGridThreads),
-                                        args, 0, st) != cudaSuccess)
+                                        args, 0, st) != cudaSuccess) {
+            cudaGetLastError();   // a refused launch leaves no sticky error for later checks
             return WS_ERR_CUDA;
+        }
     }
     uint32_t *pos = spare_vals;
     ws::k_dedup_flags<<<ws::grid_of(nv, 256), 256, 0, st>>>(decision, nv, pos);
