@@ -53,14 +53,14 @@ def parse():
     p.add_argument("--node-growth-surfels", type=int, default=1_000_000,
                    help="surfels of the node-growth measurement (torus, R = 6 mm); 0 skips it")
     p.add_argument("--serving-executors", type=int, default=2, help="solver workspaces of the serving run")
-    p.add_argument("--serving-requests", type=int, default=2000,
+    p.add_argument("--serving-requests", type=int, default=10000,
                    help="requests of the serving run (32 frame streams, 1k-16k nodes); 0 skips it")
     return p.parse_args()
 
 
 def scene_node_targets(n, seed):
-    rng = np.random.default_rng(1_000_003 * 2 + seed)
-    return np.exp(rng.uniform(np.log(500), np.log(8000), n)).astype(int)
+    from starhub_b200 import scenes
+    return scenes.batch_node_targets(n, seed)
 
 
 def rank_seed(seed, rank):
@@ -86,11 +86,8 @@ def job_throughput(world, scenes_per_rank, steps, max_ms):
 
 def build_scenes(n, seed, geometry, rank=0):
     from starhub_b200 import scenes
-    out = []
-    for i, target in enumerate(scene_node_targets(n, rank_seed(seed, rank))):
-        spec = scenes.spec_for_nodes(int(target), scenes.config_spec(2))
-        out.append(scenes.make_scene(spec, geometry, seed=1_000_003 * 2 + 1000 * rank + i))
-    return out
+    return [scenes.batch_scene(t, geometry, i, replica=rank)
+            for i, t in enumerate(scene_node_targets(n, rank_seed(seed, rank)))]
 
 
 class ClockSampler:
@@ -147,15 +144,20 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def load_traffic():
-    """DRAM bytes per launch of the timed kernel from the committed ncu summary, if present."""
+def load_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum + dram__bytes_write.sum) from the
+    committed ncu summary, when that capture ran this workload; ncu cannot run inside the bench,
+    so the figure is static and the line says where it came from."""
     p = ROOT / "profiles" / "traffic.json"
-    if p.exists():
-        try:
-            return json.loads(p.read_text())
-        except Exception:
-            return {}
-    return {}
+    try:
+        entry = json.loads(p.read_text()).get(kernel)
+    except Exception:
+        entry = None
+    if not entry:
+        return None, "no ncu capture of this kernel committed"
+    if entry.get("workload") != workload:
+        return None, f"the committed ncu capture ({entry.get('source')}) ran another workload"
+    return int(entry["dram_bytes_per_launch"]), f"static ncu summary {entry.get('source')} of this workload"
 
 
 def measure_spmv(solver, n_nodes, stored, stream, dev, launches=20, warmup=3):
@@ -253,6 +255,27 @@ def measure_node_growth(geo, n_surfels, dev, stream, oracle_timing, repeats=3):
     return out
 
 
+def measure_accuracy(batch, host_scenes):
+    """Relative twist error and warped-position error (m) of the batch's solutions against the
+    FP64 oracle for the smallest, median and largest scene."""
+    from starhub_b200 import scenes
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    orc.build()
+    order = np.argsort([sc.num_nodes for sc in host_scenes], kind="stable")
+    picks = [int(order[0]), int(order[len(order) // 2]), int(order[-1])]
+    rows = []
+    for i in picks:
+        sc = host_scenes[i]
+        dq = batch.SolvedNodeSE3(i).cpu().numpy().copy()
+        ref = orc.solve(sc, gn_iters=GN_ITERS, pcg_iters=PCG_ITERS, threads=os.cpu_count() or 1)
+        rows.append({"scene": i, "nodes": sc.num_nodes, "twist": scenes.twist_error(dq, ref, sc.nodes),
+                     "position_m": scenes.position_error(sc, dq, ref)})
+    return {"against": "FP64 oracle on the same inputs", "scenes": rows,
+            "max_twist": max(r["twist"] for r in rows), "max_position_m": max(r["position_m"] for r in rows),
+            "bar": {"twist": 1e-4, "position_m": 1e-5}}
+
+
 def cpu_solve_rate(sample, threads, precision):
     """Solves/s of the CPU restatement over `sample` scenes (index build + GN loop)."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -265,8 +288,30 @@ def cpu_solve_rate(sample, threads, precision):
     return len(sample) / dt, dt
 
 
+def workload_config(args):
+    """The `config` object of the JSON line, identical in both arms."""
+    from starhub_b200 import scenes
+    k = scenes.config_spec(2).graph_k
+    return {"workload": f"{args.scenes} uneven torus scenes per GPU per step, nodes log-uniform [500, 8000], "
+                        f"surfels 130 x nodes, 640x480 maps, {k}-NN node graph, {GN_ITERS} GN x {PCG_ITERS} PCG",
+            "scenes": args.scenes, "graph_k": k, "gn_iters": GN_ITERS, "pcg_iters": PCG_ITERS,
+            "scene_seed": args.seed,
+            "l2": f"inputs larger than L2 ({args.scenes * 640 * 480 * 68 / 1e9:.2f} GB of maps per step)"}
+
+
+def stratified_picks(targets, count):
+    """`count` scenes of the set whose node counts follow the set's distribution: the scenes at
+    evenly spaced quantiles of the node-count order."""
+    order = np.argsort(targets, kind="stable")
+    pos = ((np.arange(count) + 0.5) * len(targets) / count).astype(int)
+    return [int(order[min(p, len(targets) - 1)]) for p in pos]
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the CPU restatement of the reference solver on the host cores."""
+    """--impl reference: the CPU restatement of the reference solver (FP32, the reference's
+    arithmetic) on the host cores, on the same scenes as the GPU arm.  A step solves one
+    scene; the timed steps take the scenes at evenly spaced quantiles of the set's node
+    counts, so their mean size is the set's."""
     if rank != 0:
         return
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -275,26 +320,27 @@ def run_reference(args, rank, world):
     from starhub_b200 import scenes
     geo = orc.OracleGeometry()
     targets = scene_node_targets(args.scenes, args.seed)
-    # a bounded sample of the same scene family: one scene per step, cycling through the set
     per_step = 1
-    picks = [int(i) for i in np.linspace(0, len(targets) - 1, max(1, min(len(targets), args.steps + args.warmup)))]
+    timed = stratified_picks(targets, min(args.steps, len(targets)))
+    warm = [int(i) for i in np.argsort(targets, kind="stable")[: max(1, args.warmup)]]
     built = {}
 
     def scene(i):
         if i not in built:
-            spec = scenes.spec_for_nodes(int(targets[i]), scenes.config_spec(2))
-            built[i] = scenes.make_scene(spec, geo, seed=1_000_003 * 2 + i)
+            built[i] = scenes.batch_scene(int(targets[i]), geo, i)
         return built[i]
 
     threads = os.cpu_count() or 1
     for w in range(args.warmup):
-        orc.solve(scene(picks[w % len(picks)]), precision=orc.ORC_PREC_FP32_REFERENCE, threads=threads)
+        orc.solve(scene(warm[w % len(warm)]), precision=orc.ORC_PREC_FP32_REFERENCE, gn_iters=GN_ITERS,
+                  pcg_iters=PCG_ITERS, threads=threads)
     times = []
     nodes = 0
     for k in range(args.steps):
-        sc = scene(picks[(args.warmup + k) % len(picks)])
+        sc = scene(timed[k % len(timed)])
         t0 = time.perf_counter()
-        orc.solve(sc, precision=orc.ORC_PREC_FP32_REFERENCE, threads=threads)
+        orc.solve(sc, precision=orc.ORC_PREC_FP32_REFERENCE, gn_iters=GN_ITERS, pcg_iters=PCG_ITERS,
+                  threads=threads)
         times.append(time.perf_counter() - t0)
         nodes += sc.num_nodes
     total = float(np.sum(times))
@@ -303,12 +349,15 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "uneven torus scenes, nodes log-uniform [500, 8000], 640x480, 5 GN x 20 PCG",
-                   "scenes_per_step": per_step, "mean_nodes": nodes / args.steps},
+        "config": workload_config(args),
+        "sample": {"scenes_per_step": per_step, "mean_nodes": nodes / args.steps,
+                   "workload_mean_target_nodes": float(np.mean(targets)),
+                   "scenes": sorted({timed[k % len(timed)] for k in range(args.steps)})},
         "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} scenes of the benchmark family, one per step, FP32 restatement "
-                                   f"(index build + GN loop), OpenMP over all host threads"},
+                         "sample": f"{args.steps} of the {args.scenes} benchmark scenes at evenly spaced quantiles of "
+                                   f"their node counts, one per step, FP32 restatement of the reference arithmetic "
+                                   f"(index build + {GN_ITERS} GN x {PCG_ITERS} PCG), OpenMP over all host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -376,8 +425,12 @@ def main():
     total_ms = max_over_ranks(t_all0.elapsed_time(t_all1), world, dev)
     value = job_throughput(world, len(ds), args.steps, total_ms)
 
-    # ---- accuracy of the timed configuration: a sample of scenes vs the FP64 oracle (rank 0) ----
-    # (checked in the test suite; the bench records the twist error of one scene per run)
+    # ---- accuracy of the timed configuration (rank 0, after the timed region): the smallest,
+    #      median and largest scenes of the batch, as solved by the timed graph replay, against the
+    #      FP64 oracle on the same inputs ----
+    accuracy = None
+    if rank == 0:
+        accuracy = measure_accuracy(batch, host_scenes)
 
     # ---- phase breakdown of one batched solve (CUDA events inside the library) ----
     batch.set_profiling(True)
@@ -507,7 +560,7 @@ def main():
     dom = max(("pcg", "eval", "assemble_node", "assemble_pair"), key=lambda k: phase_ms[k])
     bytes_, ms_, kname = per_launch[dom]
     achieved = bytes_ / (ms_ / 1e3) / 1e9
-    traffic = load_traffic().get(kname)
+    traffic, traffic_source = load_traffic(kname, workload_config(args)["workload"])
 
     # ---- CPU baseline on a bounded sample (rank 0, N = 1 only) ----
     cpu = None
@@ -555,12 +608,14 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 uneven torus scenes per GPU per step, nodes log-uniform [500, 8000], "
-                                   "surfels 130 x nodes, 640x480, 5 GN x 20 PCG, batched in one CUDA graph",
-                       "scenes": len(ds), "total_nodes": tot_nodes, "dense_terms": nd_tot, "block_nnz": nnzb, "stored_blocks": stored,
-                       "precision": "fp32 bulk, fp64 pcg reductions + 6x6 cholesky",
-                       "autotuned": {k: tuning[k] for k in ("node_threads", "pair_threads", "pcg_blocks_per_sm")},
-                       "l2": f"inputs larger than L2 ({tot_pix * 68 / 1e9:.2f} GB of maps per step)"},
+            "config": workload_config(args),
+            "workload_detail": {"total_nodes": tot_nodes, "dense_terms": nd_tot, "block_nnz": nnzb,
+                                "stored_blocks": stored,
+                                "precision": "fp32 bulk, fp64 pcg reductions + 6x6 cholesky",
+                                "timing": "one CUDA-graph replay of the batched solve per step",
+                                "autotuned": {k: tuning[k] for k in ("node_threads", "pair_threads",
+                                                                     "pcg_blocks_per_sm")}},
+            "accuracy": accuracy,
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "lone_solve_p50": float(np.percentile(lone_ms, 50)),
                            "lone_solve_p99": float(np.percentile(lone_ms, 99))},
@@ -571,6 +626,7 @@ def main():
             "phase_launches": {k: int(v) for k, v in phase_launch.items()},
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "traffic_source": traffic_source,
                          "algorithmic_bytes_per_launch": bytes_, "ms_per_launch": ms_},
             "cpu_baseline": cpu,
             "serving": serving_out,

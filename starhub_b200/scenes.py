@@ -26,6 +26,11 @@ from typing import Optional
 import numpy as np
 
 NODE_RADIUS = 0.025
+# Node-graph neighbours per node, self included.  The benchmark configurations build an
+# 8-NN graph; the reference ties the graph's K to the skinning K of 4
+# (libs/star/geometry/constants.h:6-7), which is the mode its own node graph produces.
+BASELINE_GRAPH_K = 8
+REFERENCE_GRAPH_K = 4
 
 
 @dataclass
@@ -68,6 +73,8 @@ class Scene:
     lambda_feature: float = 1.0
     gn_iters: int = 5
     pcg_iters: int = 20
+    node_motion_pred: Optional[np.ndarray] = None   # (N, 4) float32: predicted translation, confidence
+    feature_knn: Optional[np.ndarray] = None        # (F, 4) uint16: node ids of each feature term
 
     @property
     def num_nodes(self) -> int:
@@ -299,7 +306,7 @@ class SceneSpec:
     width: int = 640
     height: int = 480
     focal: float = 570.0
-    graph_k: int = 4
+    graph_k: int = BASELINE_GRAPH_K
     max_rot_deg: float = 5.0
     max_trans: float = 0.01
     depth_noise: float = 0.001
@@ -315,12 +322,14 @@ class SceneSpec:
 
 def config_spec(config: int, **overrides) -> SceneSpec:
     """The benchmark configurations (0: plain torus, 1: large union with flow,
-    2: batched torus family, 3: precision stress, 4: serving)."""
+    2: batched torus family, 3: precision stress, 4: serving).  Configurations 0, 2, 3 and 4
+    use the 8-NN node graph; configuration 1 names no graph size and keeps the reference's
+    K = 4.  `graph_k=REFERENCE_GRAPH_K` gives the reference's own graph for any of them."""
     if config == 0:
         s = SceneSpec()
     elif config == 1:
         s = SceneSpec(kind="union", n_surfels=1_200_000, width=1280, height=720, focal=920.0, flow=True,
-                      lambda_of=0.1, gn_iters=10, pcg_iters=30)
+                      lambda_of=0.1, gn_iters=10, pcg_iters=30, graph_k=REFERENCE_GRAPH_K)
     elif config == 2:
         s = SceneSpec()
     elif config == 3:
@@ -343,6 +352,19 @@ def spec_for_nodes(target_nodes: int, base: SceneSpec = None, surfels_per_node: 
     out.scale = scale
     out.n_surfels = int(surfels_per_node * target_nodes)
     return out
+
+
+def batch_node_targets(n: int, seed: int) -> np.ndarray:
+    """Node counts of the batched configuration's scenes: log-uniform in [500, 8000]."""
+    rng = np.random.default_rng(1_000_003 * 2 + seed)
+    return np.exp(rng.uniform(np.log(500), np.log(8000), n)).astype(int)
+
+
+def batch_scene(target_nodes: int, geometry, index: int, replica: int = 0) -> Scene:
+    """Scene `index` of the batched configuration (config 2): the config-0 torus scaled to
+    about `target_nodes` nodes, 130 surfels per node, 640x480 maps, 8-NN node graph."""
+    spec = spec_for_nodes(int(target_nodes), config_spec(2))
+    return make_scene(spec, geometry, seed=1_000_003 * 2 + 1000 * replica + index)
 
 
 def sample_surface(spec: SceneSpec, rng):

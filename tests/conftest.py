@@ -24,9 +24,20 @@ def orc():
 
 @pytest.fixture(scope="session")
 def small_scene(orc):
-    """Config-0 torus at reduced resolution: 320x240, 60k surfels, about 1.5k nodes."""
+    """Config-0 torus at reduced resolution: 320x240, 60k surfels, about 1.5k nodes, with the
+    reference's own 4-NN node graph."""
     from starhub_b200 import scenes
-    spec = scenes.config_spec(0, n_surfels=60_000, width=320, height=240, focal=285.0)
+    spec = scenes.config_spec(0, n_surfels=60_000, width=320, height=240, focal=285.0,
+                              graph_k=scenes.REFERENCE_GRAPH_K)
+    return scenes.make_scene(spec, orc.OracleGeometry(), seed=11)
+
+
+@pytest.fixture(scope="session")
+def small_scene_k8(orc):
+    """The same reduced config-0 torus with the 8-NN node graph of the benchmark configurations."""
+    from starhub_b200 import scenes
+    spec = scenes.config_spec(0, n_surfels=60_000, width=320, height=240, focal=285.0,
+                              graph_k=scenes.BASELINE_GRAPH_K)
     return scenes.make_scene(spec, orc.OracleGeometry(), seed=11)
 
 
@@ -34,7 +45,8 @@ def small_scene(orc):
 def tiny_scene(orc):
     """Small torus for fast CPU checks: 160x120, 12k surfels, scaled torus."""
     from starhub_b200 import scenes
-    spec = scenes.config_spec(0, n_surfels=12_000, width=160, height=120, focal=142.5, scale=0.5)
+    spec = scenes.config_spec(0, n_surfels=12_000, width=160, height=120, focal=142.5, scale=0.5,
+                              graph_k=scenes.REFERENCE_GRAPH_K)
     return scenes.make_scene(spec, orc.OracleGeometry(), seed=5)
 
 

@@ -68,3 +68,35 @@ def test_batch_index_matches_solo(ws, orc, batch_scenes):
         m = orc.nodepair2term(oknn, sc.edges, sc.num_nodes)
         np.testing.assert_array_equal(p["rows"], m["half_rows"])
         np.testing.assert_array_equal(p["term_index"], m["term_index"][: m["half_end"][-1]])
+
+
+def test_benchmark_batch_meets_the_bar(ws, orc):
+    """The benchmarked configuration: scenes of the 64-scene batch family (8-NN graph, 640x480,
+    130 surfels per node, 5 Gauss-Newton x 20 PCG) at its smallest, median and largest node
+    counts, solved together through the CUDA-graph replay of the batched solver, each within
+    1e-4 relative twist error and 1e-5 m warped-position error of the FP64 oracle."""
+    import torch
+    from starhub_b200 import scenes
+    from starhub_b200.scenes import position_error, twist_error
+    from starhub_b200.solver import DeviceScene, GpuGeometry, WarpSolver
+    targets = scenes.batch_node_targets(64, 2)
+    order = np.argsort(targets, kind="stable")
+    picks = [int(order[0]), int(order[32]), int(order[-1])]
+    geo = GpuGeometry()
+    host = [scenes.batch_scene(int(targets[i]), geo, i) for i in picks]
+    assert all(sc.graph_k == 8 for sc in host)
+    assert host[-1].num_nodes > 6000
+    ds = [DeviceScene.from_scene(sc) for sc in host]
+    b = WarpSolver(max_nodes=sum(d.num_nodes for d in ds), max_pixels=sum(d.num_pixels for d in ds),
+                   max_edges=sum(d.num_edges for d in ds), max_scenes=len(ds))
+    b.SetBatchInputs(ds)
+    st = torch.cuda.Stream()
+    for _ in range(2):                      # capture, then a replay
+        b.SolveStreamed(5, 20, stream=st, graph=True)
+    b.Sync()
+    for i, sc in enumerate(host):
+        dq = b.SolvedNodeSE3(i).cpu().numpy().copy()
+        ref = orc.solve(sc, gn_iters=5, pcg_iters=20)
+        te, pe = twist_error(dq, ref, sc.nodes), position_error(sc, dq, ref)
+        assert te <= 1e-4, f"scene {picks[i]} ({sc.num_nodes} nodes): twist error {te}"
+        assert pe <= 1e-5, f"scene {picks[i]} ({sc.num_nodes} nodes): position error {pe}"

@@ -14,6 +14,13 @@ TWIST_TOL = 1e-4       # relative twist error vs the FP64 oracle (mixed precisio
 POS_TOL = 1e-5         # metres, warped surfel positions vs the FP64 oracle
 
 
+@pytest.fixture(params=[4, 8], ids=["k4", "k8"])
+def parity_scene(request, small_scene, small_scene_k8):
+    """The reduced config-0 torus with the reference's 4-NN node graph and with the
+    benchmark configurations' 8-NN graph."""
+    return small_scene if request.param == 4 else small_scene_k8
+
+
 def solve_gpu(ws, scene, gn, pcg, precision=0, graph=False):
     import torch
     from starhub_b200.solver import DeviceScene, WarpSolver
@@ -26,8 +33,8 @@ def solve_gpu(ws, scene, gn, pcg, precision=0, graph=False):
     return s, ds, s.SolvedNodeSE3(0).cpu().numpy().copy()
 
 
-def test_index_bit_exact(ws, orc, small_scene):
-    sc = small_scene
+def test_index_bit_exact(ws, orc, parity_scene):
+    sc = parity_scene
     s, ds, _ = solve_gpu(ws, sc, 1, 1)
     # dense terms (compaction)
     pix, knn, sw, cw = s.dense_terms()
@@ -65,12 +72,12 @@ def to_local(step, centres):
     return out
 
 
-def test_first_iteration_terms_and_system(ws, orc, small_scene):
+def test_first_iteration_terms_and_system(ws, orc, parity_scene):
     """First Gauss-Newton iteration, stage by stage.  The mixed-precision device path solves
     for node-centred twists (centre = current warped node, here the node itself), so the
     blocks and the step are compared with the oracle's node-centred mixed mode and with
     the FP64 oracle's step mapped into node-centred coordinates."""
-    sc = small_scene
+    sc = parity_scene
     s, ds, _ = solve_gpu(ws, sc, 1, 20)
     _, info = orc.solve(sc, gn_iters=1, pcg_iters=20, debug=True, precision=orc.ORC_PREC_MIXED)
     _, info64 = orc.solve(sc, gn_iters=1, pcg_iters=20, debug=True)
@@ -103,9 +110,9 @@ def test_first_iteration_terms_and_system(ws, orc, small_scene):
     np.testing.assert_allclose(sysm["step"], ref, atol=1e-4 * np.abs(ref).max(), rtol=0)
 
 
-def test_full_solve_mixed_precision(ws, orc, small_scene):
+def test_full_solve_mixed_precision(ws, orc, parity_scene):
     from starhub_b200.scenes import position_error, twist_error
-    sc = small_scene
+    sc = parity_scene
     _, _, dq = solve_gpu(ws, sc, sc.gn_iters, sc.pcg_iters)
     ref = orc.solve(sc)
     assert np.isfinite(dq).all()
@@ -115,13 +122,13 @@ def test_full_solve_mixed_precision(ws, orc, small_scene):
     assert pe <= POS_TOL, f"position error {pe}"
 
 
-def test_full_solve_fp32_mode(ws, orc, small_scene):
+def test_full_solve_fp32_mode(ws, orc, parity_scene):
     """WS_PREC_FP32 reproduces the reference's arithmetic: FP32 everywhere with twists about
     the world origin.  The ~1 m lever arm makes the 6x6 blocks ill-conditioned, so its
     distance to the FP64 solve is a few 1e-3 in twist (the oracle's FP32 restatement shows
     the same); the tolerance below bounds that, not the accurate mixed path."""
     from starhub_b200.scenes import position_error, twist_error
-    sc = small_scene
+    sc = parity_scene
     _, _, dq = solve_gpu(ws, sc, sc.gn_iters, sc.pcg_iters, precision=1)
     ref64 = orc.solve(sc)
     assert np.isfinite(dq).all()
