@@ -78,12 +78,31 @@ def test_cpp_facade_builds_and_links(lib, tmp_path):
         "  g.NaiveExpandNodeGraphFromVertexUnsupported(v, n, 1, st);\n"
         "  g.BuildNodeGraphFromScratch(false, st);\n"
         "  OptimizationProcessorWarpSolver p(4096, 640 * 480, 4096 * 8);\n"
-        "  return (int)g.GetNodeSize() + (p.SolvedSE3() != nullptr);\n"
+        "  return (int)g.GetNodeSize() + (int)p.SolvedSE3().Size();\n"
         "}\n"
         "int main(int argc, char **) { return argc > 100 ? use(nullptr, 0, 0) : 0; }\n")
     lib_dir = ROOT / "starhub_b200"
     cmd = ["g++", "-std=c++17", "-Wall", "-Wextra", "-I", str(ROOT / "include"), "-I", str(cuda / "include"),
            str(src), "-o", str(tmp_path / "facade"), "-L", str(lib_dir), "-lwarpsolve", "-L", str(cuda / "lib64"),
            "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_app_call_site_compiles_against_the_facade(lib, tmp_path):
+    """tests/facade_app_callsite.cpp holds the pipeline's solver call site as
+    examples/mono_star/app.cu:45-150 writes it (processor constructed from the process-wide
+    configuration, ProcessFrame with the seven input structs, the frame index and the stream,
+    SolvedSE3() taken as GArrayView<DualQuaternion>), with `star::b200` for `star`.  It compiles
+    and links against the facade and the library."""
+    import shutil
+    import subprocess
+    cuda = Path("/usr/local/cuda")
+    if shutil.which("g++") is None or not (cuda / "include" / "cuda_runtime.h").exists():
+        pytest.skip("g++ or the CUDA headers are missing")
+    lib_dir = ROOT / "starhub_b200"
+    cmd = ["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"), "-I",
+           str(cuda / "include"), str(ROOT / "tests" / "facade_app_callsite.cpp"), "-o", str(tmp_path / "app"),
+           "-L", str(lib_dir), "-lwarpsolve", "-L", str(cuda / "lib64"), "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
