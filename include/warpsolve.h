@@ -132,6 +132,14 @@ int ws_spmv(ws_solver *solver, const float *x, float *y, void *stream);
  * WS_ERR_TIMEOUT after about two seconds of requested sleep when the bound works (the device
  * stays usable), WS_ERR_CUDA if a CUDA call fails.  Synchronises `stream`. */
 int ws_selftest_wait_timeout(void *stream);
+/* Failure-detection self-test of the grid barrier that node construction and growth use
+ * between the rounds of their overlap check (ws_init_nodes, ws_expand_nodes on more than 16k
+ * candidates); no reference counterpart (the reference runs that check on the host).  Two
+ * blocks are launched and only one arrives at the barrier, which nothing completes.  Returns
+ * WS_ERR_TIMEOUT after about two seconds of requested sleep when the bound works (the device
+ * stays usable), WS_OK if the wait ended otherwise, WS_ERR_CUDA if a CUDA call fails.
+ * Synchronises `stream`. */
+int ws_selftest_grid_barrier_timeout(void *stream);
 /* The same operator applied matrix-free from the term records of the last Gauss-Newton
  * iteration (J x per term, then J^T (J x) gathered per node over the node->term lists, plus
  * the diagonal regulariser), without the assembled blocks.  No reference counterpart (the

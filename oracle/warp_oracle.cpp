@@ -1059,7 +1059,8 @@ int orc_voxel_subsample(const float *pts4, int n, float voxel, float *out4, int 
         const int vx = (int)std::floor(pts4[4 * i] / voxel);
         const int vy = (int)std::floor(pts4[4 * i + 1] / voxel);
         const int vz = (int)std::floor(pts4[4 * i + 2] / voxel);
-        keys[i] = (vx + 512) + (vy + 512) * 1024 + (vz + 512) * 1024 * 1024;
+        // encodeVoxel in 32-bit two's complement (the reference's int arithmetic wraps the same way)
+        keys[i] = (int)((unsigned)(vx + 512) + (unsigned)(vy + 512) * 1024u + (unsigned)(vz + 512) * 1048576u);
     }
     const auto perm = stable_order(keys);
     int count = 0;

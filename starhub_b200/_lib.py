@@ -36,7 +36,7 @@ EXPORTED = [
     "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
     "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
     "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv", "ws_spmv_matrix_free", "ws_autotune",
-    "ws_selftest_wait_timeout",
+    "ws_selftest_wait_timeout", "ws_selftest_grid_barrier_timeout",
     "ws_set_tuning",
 ]
 
@@ -175,6 +175,7 @@ def load() -> C.CDLL:
         "ws_spmv": (i, [vp, vp, vp, vp]),
         "ws_spmv_matrix_free": (i, [vp, vp, vp, vp]),
         "ws_selftest_wait_timeout": (i, [vp]),
+        "ws_selftest_grid_barrier_timeout": (i, [vp]),
         "ws_autotune": (i, [vp, i, vp, C.POINTER(WsTuning)]),
         "ws_set_tuning": (i, [vp, C.POINTER(WsTuning)]),
     }

@@ -563,6 +563,12 @@ int ws_selftest_wait_timeout(void *stream) {
     return status == 0 ? WS_OK : status;
 }
 
+int ws_selftest_grid_barrier_timeout(void *stream) {
+    int flags = 0;
+    if (ws::grid_barrier_selftest(&flags, (cudaStream_t)stream) != cudaSuccess) return WS_ERR_CUDA;
+    return (flags & 4) ? WS_ERR_TIMEOUT : WS_OK;
+}
+
 int ws_spmv_matrix_free(ws_solver *h, const float *x, float *y, void *stream) {
     if (!h || !x || !y) return WS_ERR_INVALID_ARGUMENT;
     ws::Workspace &w = h->w;

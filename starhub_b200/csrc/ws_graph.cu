@@ -85,12 +85,17 @@ struct Heap {
 };
 
 // createVoxelKeyKernel (libs/star/geometry/sampling/VoxelSubsamplerSorting.cu:8-21) with
-// encodeVoxel (libs/star/common/encode_utils.h:138-141).
+// encodeVoxel (libs/star/common/encode_utils.h:138-141).  The reference sorts the encoded keys
+// as signed ints; a voxel below -512 in z gives a negative key, which sorts first.  The keys here
+// go through an unsigned radix sort, so they carry the sign bit flipped (kVoxelKeyBias), which
+// orders them as signed ints; the sampler flips it back before decoding.
+constexpr uint32_t kVoxelKeyBias = 0x80000000u;
 __global__ void k_voxel_key(const float4 *pts, uint32_t n, float voxel, uint32_t *keys, uint32_t *vals) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 p = pts[i];
         const int vx = __float2int_rd(p.x / voxel), vy = __float2int_rd(p.y / voxel), vz = __float2int_rd(p.z / voxel);
-        keys[i] = (uint32_t)((vx + 512) + (vy + 512) * 1024 + (vz + 512) * 1024 * 1024);
+        const int enc = (int)((unsigned)(vx + 512) + (unsigned)(vy + 512) * 1024u + (unsigned)(vz + 512) * 1048576u);
+        keys[i] = (uint32_t)enc ^ kVoxelKeyBias;
         vals[i] = i;
     }
 }
@@ -111,7 +116,7 @@ __global__ void k_voxel_sample(const uint32_t *keys, const uint32_t *perm, const
         if (i != 0 && keys[i] == keys[i - 1]) continue;   // not the first point of its voxel
         uint32_t e = i + 1;
         while (e < n && keys[e] == keys[i]) ++e;
-        const int enc = (int)keys[i];
+        const int enc = (int)(keys[i] ^ kVoxelKeyBias);
         int z = enc / (1024 * 1024);
         int x = enc % 1024;
         int y = (enc - z * 1024 * 1024) / 1024;
@@ -339,6 +344,32 @@ __global__ void __launch_bounds__(kDedupGridThreads) k_dedup_greedy_grid(const u
         if (*flag == 0u) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, 2);
+}
+
+// Failure-detection self-test of the barrier above: two blocks launched, only block 0 arrives,
+// so the generation never advances and block 0 must give up after about two seconds of
+// requested sleep with bit 2 of err set, and return.
+__global__ void k_barrier_selftest(unsigned *sync, int *err) {
+    if (blockIdx.x == 0) dedup_grid_barrier(sync, 2, err);
+}
+
+cudaError_t grid_barrier_selftest(int *flags, cudaStream_t st) {
+    unsigned *words = nullptr;   // sync[0..3], err
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&words), 5 * sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(words, 0, 5 * sizeof(unsigned), st);
+    int *err = reinterpret_cast<int *>(words + 4);
+    int flag = 0;
+    if (e == cudaSuccess) {
+        k_barrier_selftest<<<2, 32, 0, st>>>(words, err);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    const cudaError_t f = cudaFreeAsync(words, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = f;
+    *flags = flag;
+    return e;
 }
 
 __global__ void k_dedup_flags(const uint8_t *decision, uint32_t nv, uint32_t *flags) {

@@ -159,6 +159,7 @@ void pcg_ranges(Workspace &w, cudaStream_t st);
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st);
 // Runs the PCG's bounded scene wait on a generation nothing advances; *status gets the flag it left.
 cudaError_t pcg_wait_selftest(int *status, cudaStream_t st);
+cudaError_t grid_barrier_selftest(int *flags, cudaStream_t st);
 cudaError_t gn_spmv_matrix_free(Workspace &w, const float *x, float *y, float *ux_dense, float *ux_reg,
                                 cudaStream_t st);
 int pcg_warps_per_block();

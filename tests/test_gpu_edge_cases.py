@@ -184,3 +184,32 @@ def test_pcg_wait_gives_up_and_the_device_stays_usable(ws, tiny_scene):
     assert 0.05 < elapsed < 60.0
     (after,) = _solve([ds])
     np.testing.assert_array_equal(after, before)
+
+
+def test_node_growth_barrier_gives_up_and_the_device_stays_usable(ws):
+    """The grid barrier between the rounds of the device overlap check is bounded: with one of
+    two blocks arriving it returns WS_ERR_TIMEOUT (about two seconds of requested sleep), no
+    GPU fault, and node construction afterwards still equals the oracle's."""
+    import time
+    from starhub_b200 import _lib
+    from starhub_b200.solver import GpuGeometry
+    t0 = time.perf_counter()
+    status = _lib.load().ws_selftest_grid_barrier_timeout(None)
+    elapsed = time.perf_counter() - t0
+    assert status == _lib.WS_ERR_TIMEOUT
+    assert 0.05 < elapsed < 60.0
+    rng = np.random.default_rng(9)
+    from starhub_b200 import scenes
+    p, _ = scenes.sample_torus(rng, 50_000, 0.3, 0.1)
+    s = scenes.pack4(p + np.array([0, 0, 1.0]), 1.0)
+    sys_path_oracle()
+    import oracle as orc
+    np.testing.assert_array_equal(GpuGeometry().init_nodes(s, 0.025), orc.OracleGeometry().init_nodes(s, 0.025))
+
+
+def sys_path_oracle():
+    import sys
+    from pathlib import Path
+    p = str(Path(__file__).resolve().parents[1] / "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)

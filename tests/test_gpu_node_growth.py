@@ -40,6 +40,24 @@ def test_init_nodes_many_candidates_bit_exact(ws, orc, n, radius, rounds_on):
     np.testing.assert_array_equal(g, o)
 
 
+def test_init_nodes_keys_below_the_encoded_range_sort_as_signed(ws, orc):
+    """encodeVoxel (libs/star/common/encode_utils.h:138-141) assumes voxel coordinates in
+    (-512, 512); below -512 in z the key is negative, and the reference's sort of int keys puts
+    those voxels first.  A torus straddling z = -512 voxels (R = 6 mm: voxel 4.2 mm, z about
+    -2.2 m) gives keys of both signs; the device order must be the oracle's signed order."""
+    from starhub_b200.solver import GpuGeometry
+    s = torus_surfels(60_000, 17)
+    s[:, 2] -= np.float32(3.2)                        # z in about [-2.33, -2.07] m
+    radius = 0.006
+    voxel = np.float32(0.7) * np.float32(radius)
+    vz = np.floor(s[:, 2] / voxel).astype(np.int64)
+    assert (vz < -512).any() and (vz >= -512).any()
+    g = GpuGeometry().init_nodes(s, radius)
+    o = orc.OracleGeometry().init_nodes(s, radius)
+    assert g.shape == o.shape
+    np.testing.assert_array_equal(g, o)
+
+
 def test_init_nodes_nan_surfel_is_rejected(ws):
     from starhub_b200._lib import WarpSolveError
     from starhub_b200.solver import GpuGeometry

@@ -248,3 +248,13 @@ def test_node_centred_first_step_is_a_change_of_variables(orc, small_scene):
     xo = b["step"].astype(np.float64).copy()
     xo[:, 3:] += np.cross(c, xo[:, :3])
     np.testing.assert_allclose(xo, a["step"], atol=1e-5 * np.abs(a["step"]).max(), rtol=0)
+
+
+def test_voxel_keys_sort_as_signed_ints(orc):
+    """The reference sorts encodeVoxel's int keys (VoxelSubsamplerSorting.cu:8-21 with cub's
+    signed order): a voxel below -512 in z has a negative key and comes first, before a voxel
+    whose key is positive, whatever the input order."""
+    voxel = np.float32(0.01)
+    pts = np.array([[0.0, 0.0, 1.0, 1.0], [0.0, 0.0, -6.0, 1.0]], np.float32)   # vz = 100, vz = -600
+    out = orc.OracleGeometry().voxel_subsample(pts, voxel)
+    np.testing.assert_array_equal(out[:, 2], np.array([-6.0, 1.0], np.float32))
