@@ -174,9 +174,15 @@ def problem_from_scene(scene, keep):
     p.edges = _p(arrs["edges"])
     p.node_cw = _p(arrs["ncw"])
     p.node_radius_square = float(np.float32(scene.node_radius) * np.float32(scene.node_radius))
-    p.node_motion_pred = None
-    p.num_features = 0
-    p.feature_knn = None
+    pred = getattr(scene, "node_motion_pred", None)
+    feat = getattr(scene, "feature_knn", None)
+    if pred is not None:
+        keep["pred"] = _c(pred, np.float32)
+    if feat is not None:
+        keep["feat"] = _c(feat, np.uint16)
+    p.node_motion_pred = _p(keep["pred"]) if pred is not None else None
+    p.num_features = 0 if feat is None else int(feat.shape[0])
+    p.feature_knn = _p(keep["feat"]) if feat is not None else None
     p.init_dq = None
     return p
 

@@ -109,6 +109,9 @@ class DeviceScene:
             lambda_depth=scene.lambda_depth, lambda_of=scene.lambda_of,
             lambda_reg=scene.lambda_reg if lambda_reg is None else lambda_reg,
             lambda_node=scene.lambda_node, lambda_feature=scene.lambda_feature,
+            node_motion_pred=_dev(getattr(scene, "node_motion_pred", None), device, torch.float32),
+            feature_knn=(None if getattr(scene, "feature_knn", None) is None
+                         else _dev(np.ascontiguousarray(scene.feature_knn).view(np.int16), device, torch.int16)),
         )
 
     def to_inputs(self) -> WsInputs:
@@ -278,7 +281,8 @@ class WarpSolver:
 
     def node2term(self, scene=0):
         sc = self._scenes[scene]
-        cap = 4 * sc.num_pixels + 2 * sc.num_edges + sc.num_nodes + 64
+        nf = 0 if sc.feature_knn is None else int(sc.feature_knn.shape[0])
+        cap = 4 * sc.num_pixels + 2 * sc.num_edges + sc.num_nodes + 4 * nf + 64
         off = np.zeros(sc.num_nodes + 1, np.uint32); ti = np.zeros(cap, np.uint32)
         n = C.c_int()
         check(self._lib.ws_get_node2term(self._h, scene, off.ctypes.data, ti.ctypes.data, cap, C.byref(n)),
@@ -287,7 +291,8 @@ class WarpSolver:
 
     def node_pairs(self, scene=0):
         sc = self._scenes[scene]
-        cap = 6 * sc.num_pixels + sc.num_edges + 64
+        nf = 0 if sc.feature_knn is None else int(sc.feature_knn.shape[0])
+        cap = 6 * sc.num_pixels + sc.num_edges + 6 * nf + 64
         rows, cols, b, e = (np.zeros(cap, np.uint32) for _ in range(4))
         ti = np.zeros(cap, np.uint32)
         n, nt = C.c_int(), C.c_int()
