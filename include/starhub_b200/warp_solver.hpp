@@ -25,6 +25,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -443,21 +444,49 @@ private:
     bool solved_ = false;
 };
 
+// Skinner::PerformSkinning* inputs (libs/star/geometry/node_graph/skinner_types.h:10-33): the
+// surfel side writes its knn and weights, the node side is read.
+struct Geometry4Skinner {
+    GArrayView<float4> reference_vertex_confid;
+    GArrayView<float4> reference_normal_radius;
+    GArrayView<float4> live_vertex_confid;
+    GArrayView<float4> live_normal_radius;
+    ushortX<d_surfel_knn_size> *surfel_knn = nullptr;
+    floatX<d_surfel_knn_size> *surfel_knn_spatial_weight = nullptr;
+    floatX<d_surfel_knn_size> *surfel_knn_connect_weight = nullptr;
+};
+struct NodeGraph4Skinner {
+    GArrayView<float4> reference_node_coords;
+    GArrayView<float4> live_node_coords;
+    GArrayView<uint2> node_status;
+    float node_radius_square = 0.f;
+};
+
 // star::NodeGraph's node construction and growth over ws_init_nodes, ws_expand_nodes and
-// ws_build_node_graph.  The node arrays are device memory owned here and sized for max_nodes,
-// like the reference's preallocation; GetNodeKnn returns k ids per node, edges are (i, knn, k).
+// ws_build_node_graph_ex, with the node status and NodeGraph::ReAnchor.  The node arrays are device
+// memory owned here and sized for max_nodes, like the reference's preallocation; GetNodeKnn returns
+// k ids per node, edges are (i, knn, k).  `normalize_weights` chooses the node-graph weights: the
+// reference's geometry library is compiled without USE_INTERPOLATE_WEIGHT_NORMALIZATION, so its
+// weights are the raw exponentials (false, the default); true divides them by their sum.
 class NodeGraph {
 public:
-    NodeGraph(float node_radius, int max_nodes, int knn = 4) : radius_(node_radius), cap_(max_nodes), k_(knn) {
+    using Ptr = std::shared_ptr<NodeGraph>;
+    using ConstPtr = std::shared_ptr<NodeGraph const>;
+
+    NodeGraph(float node_radius, int max_nodes, int knn = 4, bool normalize_weights = false)
+        : radius_(node_radius), cap_(max_nodes), k_(knn), normalize_(normalize_weights) {
         if (!(node_radius > 0.f) || max_nodes < 2 || max_nodes > 65535 || (knn != 4 && knn != 8))
             throw Error(WS_ERR_INVALID_ARGUMENT, "NodeGraph");
         try {
             alloc(&ref_, 16ull * cap_);
             alloc(&live_, 16ull * cap_);
             alloc(&time_, 4ull * cap_);
+            alloc(&status_, 8ull * cap_);
             alloc(&knn_, 2ull * k_ * cap_);
             alloc(&weight_, 4ull * k_ * cap_);
+            alloc(&connect_, 4ull * k_ * cap_);
             alloc(&edges_, 6ull * k_ * cap_);
+            check(cudaMemset(status_, 0, 8ull * cap_) == cudaSuccess ? WS_OK : WS_ERR_CUDA, "NodeGraph");
         } catch (...) {
             release();
             throw;
@@ -468,7 +497,8 @@ public:
     NodeGraph &operator=(const NodeGraph &) = delete;
 
     // InitializeNodeGraphFromVertex (NodeGraph.cu:460-498): nodes from `vertex` (device float4),
-    // two anchors first, reference = live coordinates, initial time `current_time`, then the graph.
+    // two anchors first, reference = live coordinates, initial time `current_time`, status cleared,
+    // then the graph.
     void InitializeNodeGraphFromVertex(const float4 *vertex, unsigned num_vertex, unsigned current_time, bool use_ref,
                                        cudaStream_t stream = 0) {
         std::vector<float4> host((size_t)cap_);
@@ -480,6 +510,7 @@ public:
         check(cudaMemcpyAsync(ref_, host.data(), 16ull * n, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
                       cudaMemcpyAsync(live_, host.data(), 16ull * n, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
                       cudaMemcpyAsync(time_, times.data(), 4ull * n, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
+                      cudaMemsetAsync(status_, 0, 8ull * n, stream) == cudaSuccess &&
                       cudaStreamSynchronize(stream) == cudaSuccess
                   ? WS_OK
                   : WS_ERR_CUDA,
@@ -491,7 +522,7 @@ public:
 
     // NaiveExpandNodeGraphFromVertexUnsupported (NodeGraph.cu:500-532): appends the greedy
     // nodes of `vertex_unsupported` (device float4) to both coordinate arrays with initial time
-    // `current_time`.  The graph is rebuilt by a later BuildNodeGraphFromScratch, as there.
+    // `current_time` and a cleared status.  The graph is rebuilt by a later BuildNodeGraphFromScratch.
     void NaiveExpandNodeGraphFromVertexUnsupported(const float4 *vertex_unsupported, unsigned num_vertex,
                                                    unsigned current_time, cudaStream_t stream) {
         int n = (int)size_;
@@ -499,25 +530,80 @@ public:
                               reinterpret_cast<float *>(ref_), reinterpret_cast<float *>(live_), time_, current_time,
                               cap_, &n, stream),
               "NaiveExpandNodeGraphFromVertexUnsupported");
+        if ((unsigned)n > size_)
+            check(cudaMemsetAsync(status_ + size_, 0, 8ull * ((unsigned)n - size_), stream) == cudaSuccess
+                      ? WS_OK
+                      : WS_ERR_CUDA,
+                  "NaiveExpandNodeGraphFromVertexUnsupported");
         prev_size_ = size_;
         size_ = (unsigned)n;
     }
 
     // BuildNodeGraphFromScratch (NodeGraph.cu:357-365): k-NN graph of the reference (use_ref)
-    // or live coordinates.
+    // or live coordinates; deleted nodes (status .y == WS_DELETED_NODE_STATUS) are left out.
     void BuildNodeGraphFromScratch(bool use_ref, cudaStream_t stream) {
         if (size_ == 0) return;
-        check(ws_build_node_graph(reinterpret_cast<const float *>(use_ref ? ref_ : live_), (int)size_, k_, radius_,
-                                  knn_, weight_, edges_, stream),
+        check(ws_build_node_graph_ex(reinterpret_cast<const float *>(use_ref ? ref_ : live_),
+                                     reinterpret_cast<const uint32_t *>(status_), (int)size_, k_, radius_,
+                                     normalize_ ? 1 : 0, knn_, weight_, edges_, stream),
               "BuildNodeGraphFromScratch");
+    }
+
+    // ResetNodeGraphConnection (NodeGraph.cu:296-303): every connect weight to 1.
+    void ResetNodeGraphConnection(cudaStream_t stream) {
+        std::vector<float> ones((size_t)k_ * size_, 1.f);
+        if (!ones.empty())
+            check(cudaMemcpyAsync(connect_, ones.data(), 4ull * ones.size(), cudaMemcpyHostToDevice, stream) ==
+                              cudaSuccess &&
+                          cudaStreamSynchronize(stream) == cudaSuccess
+                      ? WS_OK
+                      : WS_ERR_CUDA,
+                  "ResetNodeGraphConnection");
+    }
+
+    // NodeGraph::ReAnchor (NodeGraph.cu:574-650): `tar` takes `src`'s graph (knn, weights, connect
+    // weights, edges), node status and initial times, its reference coordinates become `src`'s
+    // live coordinates, and it takes `src`'s node counts.  The reference also copies its n x n
+    // half-distance table, which this node graph does not keep (the graph is built without it).
+    static void ReAnchor(ConstPtr src_node_graph, Ptr tar_node_graph, cudaStream_t stream) {
+        const NodeGraph &s = *src_node_graph;
+        NodeGraph &t = *tar_node_graph;
+        if (s.k_ != t.k_ || t.cap_ < (int)s.size_) throw Error(WS_ERR_CAPACITY, "ReAnchor");
+        const size_t n = s.size_, k = (size_t)s.k_;
+        const bool ok =
+            cudaMemcpyAsync(t.knn_, s.knn_, 2 * k * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaMemcpyAsync(t.weight_, s.weight_, 4 * k * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaMemcpyAsync(t.connect_, s.connect_, 4 * k * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaMemcpyAsync(t.edges_, s.edges_, 6 * k * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaMemcpyAsync(t.status_, s.status_, 8 * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaMemcpyAsync(t.time_, s.time_, 4 * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaMemcpyAsync(t.ref_, s.live_, 16 * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+            cudaStreamSynchronize(stream) == cudaSuccess;
+        check(ok ? WS_OK : WS_ERR_CUDA, "ReAnchor");
+        t.size_ = s.size_;
+        t.prev_size_ = s.prev_size_;
+    }
+
+    // NodeGraph::GenerateNodeGraph4Skinner (NodeGraph.cu:534-545).
+    NodeGraph4Skinner GenerateNodeGraph4Skinner() const {
+        NodeGraph4Skinner out;
+        out.reference_node_coords = GArrayView<float4>(ref_, size_);
+        out.live_node_coords = GArrayView<float4>(live_, size_);
+        out.node_status = GArrayView<uint2>(status_, size_);
+        out.node_radius_square = radius_ * radius_;
+        return out;
     }
 
     const float4 *GetReferenceNodeCoordinate() const { return ref_; }
     const float4 *GetLiveNodeCoordinate() const { return live_; }
+    float4 *LiveNodeCoordinate() { return live_; }
     const uint16_t *GetNodeKnn() const { return knn_; }
     const float *GetNodeKnnSpatialWeight() const { return weight_; }
+    const float *GetNodeKnnConnectWeight() const { return connect_; }
     const uint16_t *GetNodeGraph() const { return edges_; }
     const unsigned *GetNodeInitialTime() const { return time_; }
+    uint2 *GetNodeStatus() { return status_; }
+    const uint2 *GetNodeStatusReadOnly() const { return status_; }
     unsigned GetNodeSize() const { return size_; }
     unsigned GetPrevNodeSize() const { return prev_size_; }
     float GetNodeRadiusSquare() const { return radius_ * radius_; }
@@ -530,22 +616,68 @@ private:
         *p = static_cast<T *>(q);
     }
     void release() {
-        void *ptrs[] = {ref_, live_, time_, knn_, weight_, edges_};
+        void *ptrs[] = {ref_, live_, time_, status_, knn_, weight_, connect_, edges_};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         ref_ = live_ = nullptr;
         time_ = nullptr;
+        status_ = nullptr;
         knn_ = edges_ = nullptr;
-        weight_ = nullptr;
+        weight_ = connect_ = nullptr;
     }
 
     float radius_;
     int cap_, k_;
+    bool normalize_;
     unsigned size_ = 0, prev_size_ = 0;
     float4 *ref_ = nullptr, *live_ = nullptr;
     unsigned *time_ = nullptr;
+    uint2 *status_ = nullptr;
     uint16_t *knn_ = nullptr, *edges_ = nullptr;
-    float *weight_ = nullptr;
+    float *weight_ = nullptr, *connect_ = nullptr;
+};
+
+// star::Skinner (libs/star/geometry/node_graph/Skinner.h:6-28) over ws_skinning_ex and
+// ws_skinning_incremental.  Templates over any structs with the members of Geometry4Skinner and
+// NodeGraph4Skinner (the reference's or the ones above).  `normalize_weights` as in NodeGraph.
+struct Skinner {
+    // PerformSkinningFromRef (Skinner.cu:336-352): reference surfels against reference nodes.
+    template <class G, class N>
+    static void PerformSkinningFromRef(G &geometry, N &node_graph, cudaStream_t stream = 0,
+                                       bool normalize_weights = false) {
+        skin(geometry.reference_vertex_confid, node_graph.reference_node_coords, geometry, node_graph, 0, 0,
+             normalize_weights, stream, "PerformSkinningFromRef");
+    }
+    // PerformSkinningFromLive (Skinner.cu:354-372): live surfels against live nodes.
+    template <class G, class N>
+    static void PerformSkinningFromLive(G &geometry, N &node_graph, cudaStream_t stream = 0,
+                                        bool normalize_weights = false) {
+        skin(geometry.live_vertex_confid, node_graph.live_node_coords, geometry, node_graph, 0, 0, normalize_weights,
+             stream, "PerformSkinningFromLive");
+    }
+    // PerformIncSkinnningFromLive (Skinner.cu:395-415): surfels from num_remaining_surfel on take
+    // the nodes from num_prev_node_size on into their current neighbours.
+    template <class G, class N>
+    static void PerformIncSkinnningFromLive(G &geometry, N &node_graph, const unsigned num_prev_node_size,
+                                            const unsigned num_remaining_surfel, cudaStream_t stream = 0,
+                                            bool normalize_weights = false) {
+        skin(geometry.live_vertex_confid, node_graph.live_node_coords, geometry, node_graph, num_prev_node_size,
+             num_remaining_surfel, normalize_weights, stream, "PerformIncSkinnningFromLive");
+    }
+
+private:
+    template <class V, class NV, class G, class N>
+    static void skin(const V &verts, const NV &nodes, G &geometry, N &node_graph, unsigned prev_nodes,
+                     unsigned remaining, bool normalize, cudaStream_t stream, const char *what) {
+        const int status = ws_skinning_incremental(
+            reinterpret_cast<const float *>(nodes.Ptr()), reinterpret_cast<const uint32_t *>(node_graph.node_status.Ptr()),
+            (int)node_graph.node_status.Size(), (int)prev_nodes, reinterpret_cast<const float *>(verts.Ptr()),
+            (int)verts.Size(), (int)remaining, std::sqrt(node_graph.node_radius_square), normalize ? 1 : 0,
+            reinterpret_cast<uint16_t *>(&geometry.surfel_knn[0]),
+            reinterpret_cast<float *>(&geometry.surfel_knn_spatial_weight[0]),
+            reinterpret_cast<float *>(&geometry.surfel_knn_connect_weight[0]), stream);
+        check(status, what);
+    }
 };
 
 }  // namespace b200

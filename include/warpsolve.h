@@ -201,9 +201,36 @@ int ws_expand_nodes(const float *vertices, int num_vertices, float node_radius, 
  * whose bounding box cannot enter its heap (same results).  Asynchronous on `stream`. */
 int ws_build_node_graph(const float *nodes, int num_nodes, int k, float node_radius,
                         uint16_t *knn, float *spatial_w, uint16_t *edges, void *stream);
-/* SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94): device in/out. */
+/* SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94): device in/out, weights divided
+ * by their sum (the mono_star configuration's USE_INTERPOLATE_WEIGHT_NORMALIZATION). */
 int ws_skinning(const float *nodes, int num_nodes, const float *verts, int num_verts,
                 float node_radius, uint16_t *knn, float *spatial_w, float *connect_w, void *stream);
+
+/* Node status: two uint32 per node, (compression, frozen time) as NodeGraph::m_node_status
+ * (libs/star/geometry/node_graph/NodeGraph.h:157); a node whose second word is
+ * WS_DELETED_NODE_STATUS (NodeGraph.h:18) is left out of the node graph and of skinning. */
+#define WS_DELETED_NODE_STATUS 0xFFFFFFFFu
+/* ws_build_node_graph with a node status (NULL = no node deleted; a pair with a deleted node has
+ * an infinite half distance, NodeGraph.cu:20-35) and a choice of weights: normalize_weights = 1
+ * divides each node's K weights by their sum (NodeGraph.cu:87-99 with
+ * USE_INTERPOLATE_WEIGHT_NORMALIZATION, examples/mono_star/common/global_configs.h:31-32), 0 keeps
+ * the raw __expf weights, which is what the reference's geometry library computes: it is compiled
+ * without that header. */
+int ws_build_node_graph_ex(const float *nodes, const uint32_t *node_status, int num_nodes, int k, float node_radius,
+                           int normalize_weights, uint16_t *knn, float *spatial_w, uint16_t *edges, void *stream);
+/* Skinner::PerformSkinningFromRef / PerformSkinningFromLive (Skinner.cu:336-372, kernel :10-94) with
+ * a node status (deleted nodes are skipped, Skinner.cu:39-48; NULL = none) and the choice of
+ * weights of ws_build_node_graph_ex.  Device in/out. */
+int ws_skinning_ex(const float *nodes, const uint32_t *node_status, int num_nodes, const float *verts, int num_verts,
+                   float node_radius, int normalize_weights, uint16_t *knn, float *spatial_w, float *connect_w,
+                   void *stream);
+/* Skinner::PerformIncSkinnningFromLive with IncSkinnerKernel (Skinner.cu:211-302, 395-415): after
+ * nodes num_prev_nodes .. num_nodes - 1 were appended, surfels num_remaining_surfels .. num_verts - 1
+ * are re-skinned from their current neighbours (`knn` on input, their distances recomputed) and the
+ * appended nodes only; earlier surfels are left as they are.  Device in/out. */
+int ws_skinning_incremental(const float *nodes, const uint32_t *node_status, int num_nodes, int num_prev_nodes,
+                            const float *verts, int num_verts, int num_remaining_surfels, float node_radius,
+                            int normalize_weights, uint16_t *knn, float *spatial_w, float *connect_w, void *stream);
 /* ForwardWarpVertexAndNodeKernel (libs/star/geometry/surfel/SurfelNodeDeformer.cu:13-79):
  * warps float4 vertices (and optional normals) by the normalized-DQ blend of `num_nodes` node DQs. */
 int ws_forward_warp(const float *node_se3, int num_nodes, const float *verts, const float *normals, int num_verts,
@@ -219,6 +246,32 @@ int ws_splat_maps(const float *verts, const float *attr_verts, const float *attr
                   int num_verts, int width, int height, float fx, float fy, float cx, float cy,
                   int footprint, uint32_t *index_map, float *vertex_map, float *normal_map,
                   void *stream);
+/* Solver maps as the reference's solver-map pass draws them (Render4Solver): Renderer::DrawSolverMaps
+ * and DrawSolverMapsWithRecentObservation (libs/star/geometry/render/RendererDraw.cu:105-175) with
+ * shaders/solver_map.vert:21-53 and solver_map.frag:10-17, on the GPU without a graphics stack.
+ * Surfels (device float4 arrays): vertex_confid (world xyz, confidence), normal_radius (world
+ * normal, radius) and color_time (x: colour bytes as float bits, z: last observed time; NULL = every
+ * surfel observed at current_time).  A surfel is drawn unless its camera-frame z is > max_depth or
+ * <= 0, or its confidence is below confidence_threshold while |time - current_time| >=
+ * time_threshold (-1: every unstable surfel is culled); it lands in pixel floor(f x / z + c + 0.5)
+ * and the `footprint` pixels around it (0 = the single pixel of a unit point), the nearest z wins and
+ * equal depths keep the lower surfel id.  Writes width*height texels of each non-NULL output:
+ * index (surfel id, 0xFFFFFFFF = none), vertex (xyz, 1), normal (xyz, 0), rgbd (colour / 127.5 - 1,
+ * 1 / z); empty texels are zero.  The depth compare is on the float camera z (the GL depth buffer
+ * quantises it). */
+typedef struct ws_render_params {
+    int width, height;
+    float fx, fy, cx, cy;
+    float world2camera[16];     /* row-major 4x4 */
+    float max_depth;            /* width_height_maxdepth_currtime.z */
+    float current_time;         /* width_height_maxdepth_currtime.w */
+    float confidence_threshold; /* confid_time_threshold.x (d_stable_surfel_confidence_threshold = 1) */
+    float time_threshold;       /* confid_time_threshold.y (d_rendering_recent_time_threshold = 3, or -1) */
+    int footprint;
+} ws_render_params;
+int ws_render_solver_maps(const float *vertex_confid, const float *normal_radius, const float *color_time,
+                          int num_surfels, const ws_render_params *params, uint32_t *index_map, float *vertex_map,
+                          float *normal_map, float *rgbd_map, void *stream);
 /* Measurement maps from a depth image in millimetres (device, `pitch` elements per row):
  * createVertexConfidMapKernel (libs/star/img_proc/vertex_map.cu:13-33), the depth clip of
  * filterAndScaleVertexKernel (libs/star/geometry/geometry_map/SurfelMapInitializer.cu:107-137,

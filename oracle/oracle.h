@@ -93,6 +93,15 @@ int orc_node_graph(const float *nodes4, int n, int k, float node_radius,
                    uint16_t *knn, float *spatial_w);
 int orc_skinning(const float *nodes4, int n_nodes, const float *verts4, int n_verts,
                  float node_radius, uint16_t *knn, float *spatial_w, float *connect_w, int threads);
+/* The same with node status (2 words per node, NULL = none deleted; .y == 0xFFFFFFFF is a deleted
+ * node, NodeGraph.h:18), weights divided by their sum or not, and for skinning the incremental form
+ * of IncSkinnerKernel (Skinner.cu:211-302: surfels first_vert.. keep their knn and take the nodes
+ * prev_nodes..). */
+int orc_node_graph_ex(const float *nodes4, const uint32_t *status, int n, int k, float node_radius, int normalize,
+                      uint16_t *knn, float *spatial_w);
+int orc_skinning_ex(const float *nodes4, const uint32_t *status, int n_nodes, int prev_nodes, const float *verts4,
+                    int first_vert, int n_verts, float node_radius, int normalize, uint16_t *knn, float *spatial_w,
+                    float *connect_w, int threads);
 
 /* Index build. */
 int orc_compact_pixels(int width, int height, const uint32_t *index_map, const float *flow,
@@ -126,6 +135,19 @@ int orc_forward_warp(const float *node_dq, int n_nodes, const float *verts4, int
  * Outputs width*height float4 each. */
 int orc_measure_maps(const uint16_t *depth_mm, int width, int height, float fx, float fy, float cx, float cy,
                      float clip_near, float clip_far, float radius_scale, float *vertex4, float *normal4);
+
+/* The solver-map pass (Renderer::DrawSolverMaps, RendererDraw.cu:105-175, with
+ * shaders/solver_map.vert:21-53 and solver_map.frag:10-17): per surfel the camera transform
+ * ((m0 x + m1 y) + m2 z) + m3, the culls (z > max depth or z <= 0 or the depth buffer's far plane;
+ * confidence < conf_threshold with |time - current| >= time_threshold), the pixel
+ * floor(f x / z + c + 0.5) and `footprint` pixels around it, nearest z first, equal z to the lower
+ * id.  world2camera is row-major 4x4; color_time may be NULL.  Outputs width*height texels each:
+ * index (0xFFFFFFFF = none), vertex (xyz, 1), normal (xyz, 0), rgbd (colour / 127.5 - 1, 1 / z). */
+int orc_render_solver_maps(const float *vertex_confid4, const float *normal_radius4, const float *color_time4,
+                           int n, int width, int height, float fx, float fy, float cx, float cy,
+                           const float *world2camera, float max_depth, float current_time,
+                           float conf_threshold, float time_threshold, int footprint, uint32_t *index_map,
+                           float *vertex4, float *normal4, float *rgbd4);
 
 #ifdef __cplusplus
 }

@@ -131,6 +131,40 @@ class OracleGeometry:
         edges[:, 2] = np.tile(np.arange(k, dtype=np.uint16), n)
         return knn, w, edges
 
+    def node_graph_ex(self, nodes, k, node_radius, status=None, normalize=True):
+        """orc_node_graph_ex: knn, weights and edges with node status and optional normalisation."""
+        nd = _c(nodes, np.float32)
+        n = nd.shape[0]
+        stt = _c(status, np.uint32) if status is not None else None
+        knn = np.zeros((n, k), np.uint16)
+        w = np.zeros((n, k), np.float32)
+        st = lib().orc_node_graph_ex(_p(nd), _p(stt), C.c_int(n), C.c_int(k), C.c_float(node_radius),
+                                     C.c_int(1 if normalize else 0), _p(knn), _p(w))
+        if st != 0:
+            raise RuntimeError(f"orc_node_graph_ex failed: {st}")
+        edges = np.zeros((n * k, 3), np.uint16)
+        edges[:, 0] = np.repeat(np.arange(n, dtype=np.uint16), k)
+        edges[:, 1] = knn.reshape(-1)
+        edges[:, 2] = np.tile(np.arange(k, dtype=np.uint16), n)
+        return knn, w, edges
+
+    def skinning_ex(self, nodes, verts, node_radius, status=None, normalize=True, prev_nodes=0, first_vert=0,
+                    knn=None):
+        """orc_skinning_ex: full skinning, or with prev_nodes > 0 the incremental form that starts surfels
+        first_vert.. from `knn` (their current neighbours) and takes the nodes prev_nodes.."""
+        nd = _c(nodes, np.float32)
+        v = _c(verts, np.float32)
+        stt = _c(status, np.uint32) if status is not None else None
+        out_knn = np.zeros((v.shape[0], 4), np.uint16) if knn is None else np.array(knn, np.uint16, copy=True)
+        sw = np.zeros((v.shape[0], 4), np.float32)
+        cw = np.zeros((v.shape[0], 4), np.float32)
+        st = lib().orc_skinning_ex(_p(nd), _p(stt), C.c_int(nd.shape[0]), C.c_int(prev_nodes), _p(v),
+                                   C.c_int(first_vert), C.c_int(v.shape[0]), C.c_float(node_radius),
+                                   C.c_int(1 if normalize else 0), _p(out_knn), _p(sw), _p(cw), C.c_int(self.threads))
+        if st != 0:
+            raise RuntimeError(f"orc_skinning_ex failed: {st}")
+        return out_knn, sw, cw
+
     def skinning(self, nodes, verts, node_radius):
         nd = _c(nodes, np.float32)
         v = _c(verts, np.float32)
@@ -311,6 +345,27 @@ def binblock_csr(n_nodes, sym_rows, sym_cols):
     if st != 0:
         raise RuntimeError(f"orc_binblock_csr failed: {st}")
     return rp[: n_rp.value], col
+
+
+def render_solver_maps(vertex_confid, normal_radius, color_time, cam, world2camera, max_depth, current_time,
+                       conf_threshold=1.0, time_threshold=3.0, footprint=0):
+    """orc_render_solver_maps: (index (H, W) uint32, vertex, normal, rgbd (H, W, 4) float32)."""
+    vc = _c(vertex_confid, np.float32)
+    nr = _c(normal_radius, np.float32)
+    ct = _c(color_time, np.float32) if color_time is not None else None
+    m = _c(np.asarray(world2camera, np.float32).reshape(16), np.float32)
+    h, w = cam.height, cam.width
+    idx = np.zeros((h, w), np.uint32)
+    vert = np.zeros((h, w, 4), np.float32)
+    nrm = np.zeros((h, w, 4), np.float32)
+    rgbd = np.zeros((h, w, 4), np.float32)
+    rc = lib().orc_render_solver_maps(_p(vc), _p(nr), _p(ct), C.c_int(vc.shape[0]), C.c_int(w), C.c_int(h),
+                                      C.c_float(cam.fx), C.c_float(cam.fy), C.c_float(cam.cx), C.c_float(cam.cy),
+                                      _p(m), C.c_float(max_depth), C.c_float(current_time),
+                                      C.c_float(conf_threshold), C.c_float(time_threshold), C.c_int(footprint),
+                                      _p(idx), _p(vert), _p(nrm), _p(rgbd))
+    assert rc == 0
+    return idx, vert, nrm, rgbd
 
 
 def measure_maps(depth_mm, fx, fy, cx, cy, clip_near=0.1, clip_far=3.0, radius_scale=1.0):

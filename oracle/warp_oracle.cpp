@@ -112,6 +112,11 @@ struct KnnHeap {
         for (int i = 0; i < CAP; ++i) { distance[i] = init_d; index[i] = 0; }
         update_heap();
     }
+    // the reference's constructor from given distances and ids (brute_force_knn.cuh:62-70)
+    KnnHeap(const float *d, const uint16_t *ids) {
+        for (int i = 0; i < CAP; ++i) { distance[i] = d[i]; index[i] = ids[i]; }
+        update_heap();
+    }
     void update_heap() {
         max_id = 0;
         max_distance = distance[0];
@@ -1118,14 +1123,20 @@ int orc_init_nodes(const float *pts4, int n, float node_radius, float *out4, int
 }
 
 // UpdateNodeDistanceKernel + BuildNodeGraphKernel (NodeGraph.cu:10-101): half squared
-// distances, K nearest including self, exp weights normalized.  The weights use
-// expf here; the device code uses __expf, so weights agree to a few ulps only.
-int orc_node_graph(const float *nodes4, int n, int k, float node_radius, uint16_t *knn, float *spatial_w) {
+// distances, K nearest including self, exp weights, divided by their sum when `normalize`
+// (USE_INTERPOLATE_WEIGHT_NORMALIZATION, NodeGraph.cu:87-99).  A pair with a deleted node
+// (status[2 i + 1] == 0xFFFFFFFF, NodeGraph.h:18) has the half of 1e6 (infinite) as distance
+// (NodeGraph.cu:20-35).  The weights use expf here; the device code uses __expf, so weights
+// agree to a few ulps only.
+int orc_node_graph_ex(const float *nodes4, const uint32_t *status, int n, int k, float node_radius, int normalize,
+                      uint16_t *knn, float *spatial_w) {
     if (k != 4 && k != 8) return -3;
     const float r2 = node_radius * node_radius;
+    auto deleted = [&](int i) { return status != nullptr && status[2 * i + 1] == 0xFFFFFFFFu; };
 #pragma omp parallel for schedule(dynamic, 16)
     for (int a = 0; a < n; ++a) {
         auto dist = [&](int b) {
+            if (deleted(a) || deleted(b)) return half_to_float(float_to_half_rn(1e6f));
             const int hi = std::max(a, b), lo = std::min(a, b);
             const float dx = nodes4[4 * hi] - nodes4[4 * lo];
             const float dy = nodes4[4 * hi + 1] - nodes4[4 * lo + 1];
@@ -1138,7 +1149,10 @@ int orc_node_graph(const float *nodes4, int n, int k, float node_radius, uint16_
             for (int q = 0; q < k; ++q) { w[q] = std::exp(-dd[q] / (2 * r2)); }
             for (int q = 0; q < k; ++q) sum += w[q];
             const float inv = 1.0f / sum;
-            for (int q = 0; q < k; ++q) { knn[(size_t)a * k + q] = ii[q]; spatial_w[(size_t)a * k + q] = w[q] * inv; }
+            for (int q = 0; q < k; ++q) {
+                knn[(size_t)a * k + q] = ii[q];
+                spatial_w[(size_t)a * k + q] = normalize ? w[q] * inv : w[q];
+            }
         };
         if (k == 4) {
             KnnHeap<4> h(1e3f);
@@ -1155,23 +1169,44 @@ int orc_node_graph(const float *nodes4, int n, int k, float node_radius, uint16_
     return 0;
 }
 
-// SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94).
-int orc_skinning(const float *nodes4, int n_nodes, const float *verts4, int n_verts, float node_radius,
-                 uint16_t *knn, float *spatial_w, float *connect_w, int threads) {
+int orc_node_graph(const float *nodes4, int n, int k, float node_radius, uint16_t *knn, float *spatial_w) {
+    return orc_node_graph_ex(nodes4, nullptr, n, k, node_radius, 1, knn, spatial_w);
+}
+
+// SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94) and IncSkinnerKernel (:211-302).
+// A deleted node enters at distance 1e6 (Skinner.cu:39-48).  With prev_nodes > 0 the surfels
+// first_vert .. n_verts - 1 start their heap from their current neighbours (knn on input) at their
+// distances and take the nodes prev_nodes .. n_nodes - 1; otherwise every surfel starts at 1e6
+// and takes all nodes.  Weights exp(-d / (2 r^2)), divided by their sum when `normalize`.
+int orc_skinning_ex(const float *nodes4, const uint32_t *status, int n_nodes, int prev_nodes, const float *verts4,
+                    int first_vert, int n_verts, float node_radius, int normalize, uint16_t *knn, float *spatial_w,
+                    float *connect_w, int threads) {
+    if (prev_nodes < 0 || prev_nodes > n_nodes || first_vert < 0 || first_vert > n_verts) return -1;
     const float r2 = node_radius * node_radius;
     const int th = set_threads(threads);
+    auto deleted = [&](int i) { return status != nullptr && status[2 * i + 1] == 0xFFFFFFFFu; };
 #pragma omp parallel for num_threads(th) schedule(static)
-    for (int v = 0; v < n_verts; ++v) {
+    for (int v = first_vert; v < n_verts; ++v) {
         const float *p = verts4 + 4ull * v;
         KnnHeap<4> h(1e6f);
-        for (int i = 0; i < n_nodes; ++i) {
+        if (prev_nodes > 0) {
+            float d0[4];
+            uint16_t i0[4];
+            for (int i = 0; i < 4; ++i) {
+                i0[i] = knn[4ull * v + i];
+                const float *q = nodes4 + 4ull * std::min<int>(i0[i], n_nodes - 1);
+                d0[i] = sq3_fused(p[0] - q[0], p[1] - q[1], p[2] - q[2]);
+            }
+            h = KnnHeap<4>(d0, i0);
+        }
+        for (int i = prev_nodes; i < n_nodes; ++i) {
             const float *q = nodes4 + 4ull * i;
-            h.update((uint16_t)i, sq3_fused(p[0] - q[0], p[1] - q[1], p[2] - q[2]));
+            h.update((uint16_t)i, deleted(i) ? 1e6f : sq3_fused(p[0] - q[0], p[1] - q[1], p[2] - q[2]));
         }
         h.sort();
         float w[4], sum = 0.f;
         for (int i = 0; i < 4; ++i) {
-            const float *q = nodes4 + 4ull * h.index[i];
+            const float *q = nodes4 + 4ull * std::min<int>(h.index[i], n_nodes - 1);
             const float d = sq3_fused(p[0] - q[0], p[1] - q[1], p[2] - q[2]);
             w[i] = std::exp(-d / (2.f * r2));
             sum += w[i];
@@ -1179,11 +1214,17 @@ int orc_skinning(const float *nodes4, int n_nodes, const float *verts4, int n_ve
         const float inv = 1.f / sum;
         for (int i = 0; i < 4; ++i) {
             knn[4ull * v + i] = h.index[i];
-            spatial_w[4ull * v + i] = inv * w[i];
+            spatial_w[4ull * v + i] = normalize ? inv * w[i] : w[i];
             connect_w[4ull * v + i] = 1.f;
         }
     }
     return 0;
+}
+
+int orc_skinning(const float *nodes4, int n_nodes, const float *verts4, int n_verts, float node_radius,
+                 uint16_t *knn, float *spatial_w, float *connect_w, int threads) {
+    return orc_skinning_ex(nodes4, nullptr, n_nodes, 0, verts4, 0, n_verts, node_radius, 1, knn, spatial_w, connect_w,
+                           threads);
 }
 
 int orc_compact_pixels(int width, int height, const uint32_t *index_map, const float *flow,
@@ -1509,3 +1550,66 @@ int orc_measure_maps(const uint16_t *depth_mm, int width, int height, float fx, 
 }
 
 }  // extern "C"
+
+// Renderer::DrawSolverMaps with shaders/solver_map.vert:21-53 and solver_map.frag:10-17
+// (libs/star/geometry/render/RendererDraw.cu:105-175); the clear values of GLClearValues.h:21-34.
+int orc_render_solver_maps(const float *vc4, const float *nr4, const float *ct4, int n, int W, int H, float fx,
+                           float fy, float cx, float cy, const float *m, float max_depth, float current_time,
+                           float conf_threshold, float time_threshold, int fp, uint32_t *index_map, float *vertex4,
+                           float *normal4, float *rgbd4) {
+    if (n < 0 || W <= 0 || H <= 0 || fp < 0) return -1;
+    const size_t npix = (size_t)W * H;
+    std::vector<float> best_z(npix, 0.f);
+    std::vector<int64_t> best_id(npix, -1);
+    std::vector<float> surfel_z((size_t)std::max(n, 1), 0.f);
+    for (int i = 0; i < n; ++i) {
+        const float *v = vc4 + 4ull * i;
+        // vec4 world2camera * vec4(v.xyz, 1.0), one row at a time
+        const float x = ((m[0] * v[0] + m[1] * v[1]) + m[2] * v[2]) + m[3];
+        const float y = ((m[4] * v[0] + m[5] * v[1]) + m[6] * v[2]) + m[7];
+        const float z = ((m[8] * v[0] + m[9] * v[1]) + m[10] * v[2]) + m[11];
+        surfel_z[i] = z;
+        if (!(z > 0.f) || !(z < max_depth)) continue;   // z > max depth or z <= 0; z = max depth fails the depth test
+        const float t = ct4 ? ct4[4ull * i + 2] : current_time;
+        if (v[3] < conf_threshold && std::fabs(t - current_time) >= time_threshold) continue;
+        const float fpx = std::floor((fx * x) / z + cx + 0.5f);
+        const float fpy = std::floor((fy * y) / z + cy + 0.5f);
+        if (!(fpx >= (float)(-fp) && fpx < (float)(W + fp) && fpy >= (float)(-fp) && fpy < (float)(H + fp))) continue;
+        const int px = (int)fpx, py = (int)fpy;
+        for (int dy = -fp; dy <= fp; ++dy)
+            for (int dx = -fp; dx <= fp; ++dx) {
+                const int qx = px + dx, qy = py + dy;
+                if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
+                const size_t q = (size_t)qy * W + qx;
+                // depth test: nearer wins; at equal depth the surfel drawn first (lower id) stays
+                if (best_id[q] < 0 || z < best_z[q]) { best_z[q] = z; best_id[q] = i; }
+            }
+    }
+    for (size_t q = 0; q < npix; ++q) {
+        float *vo = vertex4 ? vertex4 + 4 * q : nullptr;
+        float *no = normal4 ? normal4 + 4 * q : nullptr;
+        float *ro = rgbd4 ? rgbd4 + 4 * q : nullptr;
+        if (best_id[q] < 0) {
+            index_map[q] = 0xFFFFFFFFu;
+            for (int c = 0; c < 4; ++c) {
+                if (vo) vo[c] = 0.f;
+                if (no) no[c] = 0.f;
+                if (ro) ro[c] = 0.f;
+            }
+            continue;
+        }
+        const size_t id = (size_t)best_id[q];
+        index_map[q] = (uint32_t)id;
+        if (vo) { vo[0] = vc4[4 * id]; vo[1] = vc4[4 * id + 1]; vo[2] = vc4[4 * id + 2]; vo[3] = 1.f; }
+        if (no) { no[0] = nr4[4 * id]; no[1] = nr4[4 * id + 1]; no[2] = nr4[4 * id + 2]; no[3] = 0.f; }
+        if (ro) {
+            int32_t enc = 0;
+            if (ct4) std::memcpy(&enc, ct4 + 4 * id, 4);   // floatBitsToInt(color_time.x)
+            ro[0] = (float)((enc & 0x00FF0000) >> 16) / 127.5f - 1.0f;
+            ro[1] = (float)((enc & 0x0000FF00) >> 8) / 127.5f - 1.0f;
+            ro[2] = (float)(enc & 0x000000FF) / 127.5f - 1.0f;
+            ro[3] = 1.0f / surfel_z[id];
+        }
+    }
+    return 0;
+}

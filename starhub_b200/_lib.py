@@ -36,9 +36,17 @@ EXPORTED = [
     "ws_splat_maps_noalloc", "ws_server_create", "ws_server_destroy", "ws_server_add_scene",
     "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
     "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv", "ws_spmv_matrix_free", "ws_autotune",
-    "ws_selftest_wait_timeout", "ws_selftest_grid_barrier_timeout",
+    "ws_selftest_wait_timeout", "ws_selftest_grid_barrier_timeout", "ws_render_solver_maps",
+    "ws_build_node_graph_ex", "ws_skinning_ex", "ws_skinning_incremental",
     "ws_set_tuning",
 ]
+
+
+class WsRenderParams(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("fx", C.c_float), ("fy", C.c_float), ("cx", C.c_float),
+                ("cy", C.c_float), ("world2camera", C.c_float * 16), ("max_depth", C.c_float),
+                ("current_time", C.c_float), ("confidence_threshold", C.c_float), ("time_threshold", C.c_float),
+                ("footprint", C.c_int)]
 
 
 class WsConfig(C.Structure):
@@ -176,6 +184,10 @@ def load() -> C.CDLL:
         "ws_spmv_matrix_free": (i, [vp, vp, vp, vp]),
         "ws_selftest_wait_timeout": (i, [vp]),
         "ws_selftest_grid_barrier_timeout": (i, [vp]),
+        "ws_render_solver_maps": (i, [vp, vp, vp, i, C.POINTER(WsRenderParams), vp, vp, vp, vp, vp]),
+        "ws_build_node_graph_ex": (i, [vp, vp, i, i, f, i, vp, vp, vp, vp]),
+        "ws_skinning_ex": (i, [vp, vp, i, vp, i, f, i, vp, vp, vp, vp]),
+        "ws_skinning_incremental": (i, [vp, vp, i, i, vp, i, i, f, i, vp, vp, vp, vp]),
         "ws_autotune": (i, [vp, i, vp, C.POINTER(WsTuning)]),
         "ws_set_tuning": (i, [vp, C.POINTER(WsTuning)]),
     }

@@ -419,14 +419,27 @@ __global__ void k_node_boxes(const float4 *nodes, int n, float4 *lo, float4 *hi)
 // the same expression on the gaps bounds every member's half distance from below, and the
 // heap only takes a distance strictly below its maximum.  Every heap update of the full scan
 // happens in the same order, so ids, weights and their ties come out the same.
+//
+// With node_status, a pair with a deleted node (status .y == kDeletedNodeStatus, NodeGraph.h:18)
+// gets the half of 1e6, which is infinite (NodeGraph.cu:20-35), so it never enters a heap; a
+// deleted node's own row keeps the heap's initial entries.  The boxes may still hold deleted
+// nodes: that only makes them larger, and the skip stays exact.  `normalize` divides the weights
+// by their sum (USE_INTERPOLATE_WEIGHT_NORMALIZATION, NodeGraph.cu:87-99); without it they are the
+// raw __expf values, as the reference's geometry library compiles them.
+constexpr uint32_t kDeletedNodeStatus = 0xffffffffu;
+__device__ __forceinline__ bool node_deleted(const uint2 *status, int i) {
+    return status != nullptr && status[i].y == kDeletedNodeStatus;
+}
+
 template <int K>
-__global__ void k_node_graph(const float4 *nodes, int n, float r2, const float4 *box_lo, const float4 *box_hi,
-                             uint16_t *knn, float *w, uint16_t *edges) {
+__global__ void k_node_graph(const float4 *nodes, const uint2 *status, int n, float r2, int normalize,
+                             const float4 *box_lo, const float4 *box_hi, uint16_t *knn, float *w, uint16_t *edges) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
         const float4 va = nodes[a];
         Heap<K> h;
         h.init(1e3f);
-        for (int r0 = 0, run = 0; r0 < n; r0 += kGraphRun, ++run) {
+        const bool a_deleted = node_deleted(status, a);
+        for (int r0 = 0, run = 0; r0 < n && !a_deleted; r0 += kGraphRun, ++run) {
             const float4 lo = box_lo[run], hi = box_hi[run];
             const float gx = fmaxf(fmaxf(lo.x - va.x, va.x - hi.x), 0.f);
             const float gy = fmaxf(fmaxf(lo.y - va.y, va.y - hi.y), 0.f);
@@ -438,7 +451,8 @@ __global__ void k_node_graph(const float4 *nodes, int n, float r2, const float4 
                 const float4 hi_v = (a >= b) ? va : vb, lo_v = (a >= b) ? vb : va;
                 const float dx = hi_v.x - lo_v.x, dy = hi_v.y - lo_v.y, dz = hi_v.z - lo_v.z;
                 const float dist = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-                h.update((uint16_t)b, __half2float(__float2half_rn(dist)));
+                h.update((uint16_t)b, node_deleted(status, b) ? __half2float(__float2half_rn(1e6f))
+                                                               : __half2float(__float2half_rn(dist)));
             }
         }
         h.sort();
@@ -451,7 +465,7 @@ __global__ void k_node_graph(const float4 *nodes, int n, float r2, const float4 
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             knn[(size_t)a * K + q] = h.id[q];
-            w[(size_t)a * K + q] = wv[q] * inv;
+            w[(size_t)a * K + q] = normalize ? wv[q] * inv : wv[q];
             // BuildNodeGraphPairKernel (NodeGraph.cu:103-118)
             edges[3 * ((size_t)a * K + q)] = (uint16_t)a;
             edges[3 * ((size_t)a * K + q) + 1] = h.id[q];
@@ -460,37 +474,62 @@ __global__ void k_node_graph(const float4 *nodes, int n, float r2, const float4 
     }
 }
 
-// SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94); nodes staged in shared memory.
-__global__ void __launch_bounds__(256) k_skinning(const float4 *nodes, int n_nodes, const float4 *verts, int n_verts,
-                                                   float r2, ushort4 *knn, float4 *sw, float4 *cw) {
+// SkinnerKernel (libs/star/geometry/node_graph/Skinner.cu:10-94) and IncSkinnerKernel (:211-302);
+// nodes staged in shared memory.  A deleted node (status .y == kDeletedNodeStatus) enters the
+// heap at distance 1e6 (Skinner.cu:39-48).  Full skinning (first_vert = 0, prev_nodes = 0) starts
+// every heap at 1e6; the incremental form re-skins surfels first_vert .. n_verts - 1: the heap
+// starts from the surfel's current neighbours at their distances and takes the nodes
+// prev_nodes .. n_nodes - 1.  `normalize` divides the weights by their sum
+// (USE_INTERPOLATE_WEIGHT_NORMALIZATION, Skinner.cu:70-74, 278-282).
+__global__ void __launch_bounds__(256) k_skinning(const float4 *nodes, const uint2 *status, int n_nodes,
+                                                   int prev_nodes, const float4 *verts, int first_vert, int n_verts,
+                                                   float r2, int normalize, ushort4 *knn, float4 *sw, float4 *cw) {
     __shared__ float4 tile[1024];
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    const float4 p = v < n_verts ? verts[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+    __shared__ unsigned char gone[1024];
+    const int v = first_vert + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const bool live = v < n_verts;
+    const float4 p = live ? verts[v] : make_float4(0.f, 0.f, 0.f, 0.f);
     Heap<4> h;
-    h.init(1e6f);
-    for (int base = 0; base < n_nodes; base += 1024) {
+    if (prev_nodes > 0 && live) {
+        const ushort4 k4 = knn[v];
+        const uint16_t ids[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float4 q = nodes[min((int)ids[i], n_nodes - 1)];
+            h.d[i] = sq3_fused(p.x - q.x, p.y - q.y, p.z - q.z);
+            h.id[i] = ids[i];
+        }
+        h.refresh();
+    } else {
+        h.init(1e6f);
+    }
+    for (int base = prev_nodes; base < n_nodes; base += 1024) {
         const int cnt = min(1024, n_nodes - base);
         __syncthreads();
-        for (int i = threadIdx.x; i < cnt; i += blockDim.x) tile[i] = nodes[base + i];
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+            tile[i] = nodes[base + i];
+            gone[i] = node_deleted(status, base + i) ? 1 : 0;
+        }
         __syncthreads();
         for (int i = 0; i < cnt; ++i) {
             const float4 q = tile[i];
-            h.update((uint16_t)(base + i), sq3_fused(p.x - q.x, p.y - q.y, p.z - q.z));
+            h.update((uint16_t)(base + i), gone[i] ? 1e6f : sq3_fused(p.x - q.x, p.y - q.y, p.z - q.z));
         }
     }
-    if (v >= n_verts) return;
+    if (!live) return;
     h.sort();
     float wv[4], sum = 0.f;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float4 q = nodes[h.id[i]];
+        const float4 q = nodes[min((int)h.id[i], n_nodes - 1)];
         const float dd = sq3_fused(p.x - q.x, p.y - q.y, p.z - q.z);
         wv[i] = __expf(-dd / (2.f * r2));
         sum += wv[i];
     }
     const float inv = 1.f / sum;
     knn[v] = make_ushort4(h.id[0], h.id[1], h.id[2], h.id[3]);
-    sw[v] = make_float4(inv * wv[0], inv * wv[1], inv * wv[2], inv * wv[3]);
+    sw[v] = normalize ? make_float4(inv * wv[0], inv * wv[1], inv * wv[2], inv * wv[3])
+                      : make_float4(wv[0], wv[1], wv[2], wv[3]);
     cw[v] = make_float4(1.f, 1.f, 1.f, 1.f);
 }
 
@@ -561,6 +600,83 @@ __global__ void k_splat_resolve(const unsigned long long *zbuf, int npix, const 
             index[p] = id;
             if (vmap) { const float4 v = av[id]; vmap[p] = make_float4(v.x, v.y, v.z, 1.f); }
             if (nmap) { const float4 nn = an[id]; nmap[p] = make_float4(nn.x, nn.y, nn.z, 0.f); }
+        }
+    }
+}
+
+// ---- Solver maps as the reference's solver-map pass draws them --------------------------------
+// Renderer::DrawSolverMaps (libs/star/geometry/render/RendererDraw.cu:105-160) draws every surfel as
+// a point with shaders/solver_map.vert:21-53 and solver_map.frag:10-17.  Restated per surfel:
+//   * v_cam = world2camera (v, 1), summed ((m0 x + m1 y) + m2 z) + m3 per row;
+//   * culled when v_cam.z > max depth, v_cam.z <= 0, or the surfel is unstable and not recent:
+//     confidence (vertex_confid.w) < threshold.x and |time (color_time.z) - current time| >= threshold.y
+//     (threshold.y = -1 culls every unstable surfel, DrawSolverMaps without recent observation);
+//   * pixel floor(fx x / z + cx + 0.5), floor(fy y / z + cy + 0.5) (the shader's 0.5 shift: the point
+//     lands in the pixel that holds its window position), and `footprint` pixels around it;
+//   * the depth test keeps the nearest z (the depth buffer clears to the far plane, so z = max depth
+//     never passes it); equal depths keep the lower surfel id (the first one drawn);
+//   * outputs: reference vertex (xyz, 1), reference normal (xyz, 0), surfel id, and the normalized
+//     rgbd (colour bytes of color_time.x / 127.5 - 1, 1 / z); untouched pixels keep the clear values
+//     (zeros, id 0xFFFFFFFF), GLClearValues.h:21-34.
+// The depth compare runs on the float camera z, where the GL depth buffer holds a quantised window
+// depth; two surfels closer than that quantum can resolve differently there.
+struct RenderArgs {
+    int W, H, fp;
+    float fx, fy, cx, cy, max_depth, current_time, conf_threshold, time_threshold;
+    float m[12];   // world2camera rows 0..2, row-major
+};
+
+__device__ __forceinline__ float row_dot(const float *m, float4 v) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], v.x), __fmul_rn(m[1], v.y)), __fmul_rn(m[2], v.z)), m[3]);
+}
+
+__global__ void k_render_keys(const float4 *vc, const float4 *ct, int n, RenderArgs a, unsigned long long *zbuf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 v = vc[i];
+        const float z = row_dot(a.m + 8, v);
+        if (!(z > 0.f) || !(z < a.max_depth)) continue;
+        const float t = ct ? ct[i].z : a.current_time;
+        if (v.w < a.conf_threshold && fabsf(__fsub_rn(t, a.current_time)) >= a.time_threshold) continue;
+        const float x = row_dot(a.m, v), y = row_dot(a.m + 4, v);
+        const float fpx = floorf(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(a.fx, x), z), a.cx), 0.5f));
+        const float fpy = floorf(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(a.fy, y), z), a.cy), 0.5f));
+        // a point more than the footprint outside the image covers no pixel (this also keeps the
+        // conversion to int in range)
+        if (!(fpx >= (float)(-a.fp) && fpx < (float)(a.W + a.fp) && fpy >= (float)(-a.fp) && fpy < (float)(a.H + a.fp)))
+            continue;
+        const int px = (int)fpx, py = (int)fpy;
+        const unsigned long long key = ((unsigned long long)__float_as_uint(z) << 32) | (unsigned)i;
+        for (int dy = -a.fp; dy <= a.fp; ++dy)
+            for (int dx = -a.fp; dx <= a.fp; ++dx) {
+                const int qx = px + dx, qy = py + dy;
+                if (qx < 0 || qy < 0 || qx >= a.W || qy >= a.H) continue;
+                atomicMin(zbuf + (size_t)qy * a.W + qx, key);
+            }
+    }
+}
+
+__global__ void k_render_resolve(const unsigned long long *zbuf, int npix, const float4 *vc, const float4 *nr,
+                                 const float4 *ct, uint32_t *index, float4 *vmap, float4 *nmap, float4 *rgbd) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const unsigned long long k = zbuf[p];
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k == ~0ull) {
+            index[p] = kInvalidIndex;
+            if (vmap) vmap[p] = zero;
+            if (nmap) nmap[p] = zero;
+            if (rgbd) rgbd[p] = zero;
+            continue;
+        }
+        const uint32_t id = (uint32_t)(k & 0xffffffffu);
+        index[p] = id;
+        if (vmap) { const float4 v = vc[id]; vmap[p] = make_float4(v.x, v.y, v.z, 1.f); }
+        if (nmap) { const float4 nn = nr[id]; nmap[p] = make_float4(nn.x, nn.y, nn.z, 0.f); }
+        if (rgbd) {
+            const int enc = ct ? __float_as_int(ct[id].x) : 0;
+            const float z = __uint_as_float((uint32_t)(k >> 32));
+            rgbd[p] = make_float4(__fsub_rn(__fdiv_rn((float)((enc & 0x00FF0000) >> 16), 127.5f), 1.f),
+                                  __fsub_rn(__fdiv_rn((float)((enc & 0x0000FF00) >> 8), 127.5f), 1.f),
+                                  __fsub_rn(__fdiv_rn((float)(enc & 0x000000FF), 127.5f), 1.f), __fdiv_rn(1.f, z));
         }
     }
 }
@@ -793,8 +909,8 @@ int ws_expand_nodes(const float *vertices, int num_vertices, float node_radius, 
     return WS_OK;
 }
 
-int ws_build_node_graph(const float *nodes, int n, int k, float node_radius, uint16_t *knn, float *w, uint16_t *edges,
-                        void *stream) {
+int ws_build_node_graph_ex(const float *nodes, const uint32_t *node_status, int n, int k, float node_radius,
+                           int normalize_weights, uint16_t *knn, float *w, uint16_t *edges, void *stream) {
     if (!nodes || n <= 0 || n > 65535 || !knn || !w || !edges || (k != 4 && k != 8)) return WS_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float r2 = node_radius * node_radius;
@@ -803,29 +919,53 @@ int ws_build_node_graph(const float *nodes, int n, int k, float node_radius, uin
     float4 *boxes = nullptr;
     if (cudaMallocAsync(reinterpret_cast<void **>(&boxes), 32ull * runs, st) != cudaSuccess) return WS_ERR_CUDA;
     const float4 *nd = reinterpret_cast<const float4 *>(nodes);
+    const uint2 *status = reinterpret_cast<const uint2 *>(node_status);
+    const int norm = normalize_weights ? 1 : 0;
     ws::k_node_boxes<<<ws::grid_of(runs, 128), 128, 0, st>>>(nd, n, boxes, boxes + runs);
     const int threads = 64;
     const int grid = (n + threads - 1) / threads;
     if (k == 4)
-        ws::k_node_graph<4><<<grid, threads, 0, st>>>(nd, n, r2, boxes, boxes + runs, knn, w, edges);
+        ws::k_node_graph<4><<<grid, threads, 0, st>>>(nd, status, n, r2, norm, boxes, boxes + runs, knn, w, edges);
     else
-        ws::k_node_graph<8><<<grid, threads, 0, st>>>(nd, n, r2, boxes, boxes + runs, knn, w, edges);
+        ws::k_node_graph<8><<<grid, threads, 0, st>>>(nd, status, n, r2, norm, boxes, boxes + runs, knn, w, edges);
     const cudaError_t launched = cudaGetLastError();
     const cudaError_t freed = cudaFreeAsync(boxes, st);
     return launched == cudaSuccess && freed == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }
 
-int ws_skinning(const float *nodes, int n_nodes, const float *verts, int n_verts, float node_radius, uint16_t *knn,
-                float *sw, float *cw, void *stream) {
-    if (!nodes || n_nodes <= 0 || n_nodes > 65535 || !verts || n_verts < 0 || !knn || !sw || !cw)
+int ws_build_node_graph(const float *nodes, int n, int k, float node_radius, uint16_t *knn, float *w, uint16_t *edges,
+                        void *stream) {
+    return ws_build_node_graph_ex(nodes, nullptr, n, k, node_radius, 1, knn, w, edges, stream);
+}
+
+int ws_skinning_incremental(const float *nodes, const uint32_t *node_status, int num_nodes, int num_prev_nodes,
+                            const float *verts, int num_verts, int num_remaining_surfels, float node_radius,
+                            int normalize_weights, uint16_t *knn, float *sw, float *cw, void *stream) {
+    if (!nodes || num_nodes <= 0 || num_nodes > 65535 || !verts || num_verts < 0 || !knn || !sw || !cw ||
+        num_prev_nodes < 0 || num_prev_nodes > num_nodes || num_remaining_surfels < 0 ||
+        num_remaining_surfels > num_verts)
         return WS_ERR_INVALID_ARGUMENT;
-    if (n_verts == 0) return WS_OK;
+    const int count = num_verts - num_remaining_surfels;
+    if (count == 0) return WS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float r2 = node_radius * node_radius;
-    ws::k_skinning<<<(n_verts + 255) / 256, 256, 0, st>>>(
-        reinterpret_cast<const float4 *>(nodes), n_nodes, reinterpret_cast<const float4 *>(verts), n_verts, r2,
-        reinterpret_cast<ushort4 *>(knn), reinterpret_cast<float4 *>(sw), reinterpret_cast<float4 *>(cw));
+    ws::k_skinning<<<(count + 255) / 256, 256, 0, st>>>(
+        reinterpret_cast<const float4 *>(nodes), reinterpret_cast<const uint2 *>(node_status), num_nodes,
+        num_prev_nodes, reinterpret_cast<const float4 *>(verts), num_remaining_surfels, num_verts, r2,
+        normalize_weights ? 1 : 0, reinterpret_cast<ushort4 *>(knn), reinterpret_cast<float4 *>(sw),
+        reinterpret_cast<float4 *>(cw));
     return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
+int ws_skinning_ex(const float *nodes, const uint32_t *node_status, int num_nodes, const float *verts, int num_verts,
+                   float node_radius, int normalize_weights, uint16_t *knn, float *sw, float *cw, void *stream) {
+    return ws_skinning_incremental(nodes, node_status, num_nodes, 0, verts, num_verts, 0, node_radius,
+                                   normalize_weights, knn, sw, cw, stream);
+}
+
+int ws_skinning(const float *nodes, int n_nodes, const float *verts, int n_verts, float node_radius, uint16_t *knn,
+                float *sw, float *cw, void *stream) {
+    return ws_skinning_ex(nodes, nullptr, n_nodes, verts, n_verts, node_radius, 1, knn, sw, cw, stream);
 }
 
 int ws_forward_warp(const float *se3, int num_nodes, const float *verts, const float *normals, int n,
@@ -850,7 +990,10 @@ int ws_splat_maps(const float *verts, const float *attr_verts, const float *attr
     unsigned long long *zbuf = nullptr;
     const size_t npix = (size_t)W * H;
     if (cudaMallocAsync(&zbuf, 8 * npix, st) != cudaSuccess) return WS_ERR_CUDA;
-    cudaMemsetAsync(zbuf, 0xff, 8 * npix, st);
+    if (cudaMemsetAsync(zbuf, 0xff, 8 * npix, st) != cudaSuccess) {
+        cudaFreeAsync(zbuf, st);
+        return WS_ERR_CUDA;
+    }
     if (n > 0)
         ws::k_splat<<<ws::grid_of(n, 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(verts), n, W, H, fx, fy, cx,
                                                          cy, footprint, zbuf);
@@ -881,6 +1024,38 @@ int ws_splat_maps_noalloc(const float *verts, const float *attr_verts, const flo
     ws::k_splat_resolve<<<ws::grid_of((long long)npix, 256), 256, 0, st>>>(
         zbuf, (int)npix, reinterpret_cast<const float4 *>(attr_verts), reinterpret_cast<const float4 *>(attr_normals),
         index_map, reinterpret_cast<float4 *>(vertex_map), reinterpret_cast<float4 *>(normal_map));
+    return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
+int ws_render_solver_maps(const float *vertex_confid, const float *normal_radius, const float *color_time,
+                          int num_surfels, const ws_render_params *params, uint32_t *index_map, float *vertex_map,
+                          float *normal_map, float *rgbd_map, void *stream) {
+    if (!params || !vertex_confid || num_surfels < 0 || !index_map) return WS_ERR_INVALID_ARGUMENT;
+    const ws_render_params &p = *params;
+    if (p.width <= 0 || p.height <= 0 || p.footprint < 0 || p.footprint > 8 || !(p.max_depth > 0.f))
+        return WS_ERR_INVALID_ARGUMENT;
+    if (normal_map && !normal_radius) return WS_ERR_INVALID_ARGUMENT;
+    ws::RenderArgs a;
+    a.W = p.width; a.H = p.height; a.fp = p.footprint;
+    a.fx = p.fx; a.fy = p.fy; a.cx = p.cx; a.cy = p.cy;
+    a.max_depth = p.max_depth; a.current_time = p.current_time;
+    a.conf_threshold = p.confidence_threshold; a.time_threshold = p.time_threshold;
+    for (int q = 0; q < 12; ++q) a.m[q] = p.world2camera[q];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t npix = (size_t)p.width * p.height;
+    unsigned long long *zbuf = nullptr;
+    if (cudaMallocAsync(&zbuf, 8 * npix, st) != cudaSuccess) return WS_ERR_CUDA;
+    if (cudaMemsetAsync(zbuf, 0xff, 8 * npix, st) != cudaSuccess) {
+        cudaFreeAsync(zbuf, st);
+        return WS_ERR_CUDA;
+    }
+    const float4 *vc = reinterpret_cast<const float4 *>(vertex_confid);
+    const float4 *ct = reinterpret_cast<const float4 *>(color_time);
+    if (num_surfels > 0) ws::k_render_keys<<<ws::grid_of(num_surfels, 256), 256, 0, st>>>(vc, ct, num_surfels, a, zbuf);
+    ws::k_render_resolve<<<ws::grid_of((long long)npix, 256), 256, 0, st>>>(
+        zbuf, (int)npix, vc, reinterpret_cast<const float4 *>(normal_radius), ct, index_map,
+        reinterpret_cast<float4 *>(vertex_map), reinterpret_cast<float4 *>(normal_map), reinterpret_cast<float4 *>(rgbd_map));
+    cudaFreeAsync(zbuf, st);
     return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }
 

@@ -368,6 +368,43 @@ class GpuGeometry:
                                            self._stream()), "ws_build_node_graph")
         return (knn.cpu().numpy().view(np.uint16), w.cpu().numpy(), edges.cpu().numpy().view(np.uint16))
 
+    def node_graph_ex(self, nodes, k, node_radius, status=None, normalize=True):
+        """ws_build_node_graph_ex: knn, weights and edges with a node status and the choice of weights."""
+        nd = _dev(nodes, self.device, torch.float32)
+        stt = None if status is None else _dev(np.ascontiguousarray(status, np.uint32).view(np.int32), self.device)
+        n = int(nd.shape[0])
+        knn = torch.empty((n, k), dtype=torch.int16, device=self.device)
+        w = torch.empty((n, k), dtype=torch.float32, device=self.device)
+        edges = torch.empty((n * k, 3), dtype=torch.int16, device=self.device)
+        check(self.lib.ws_build_node_graph_ex(_ptr(nd), _ptr(stt), n, k, float(node_radius), 1 if normalize else 0,
+                                              _ptr(knn), _ptr(w), _ptr(edges), self._stream()), "ws_build_node_graph_ex")
+        return (knn.cpu().numpy().view(np.uint16), w.cpu().numpy(), edges.cpu().numpy().view(np.uint16))
+
+    def skinning_ex(self, nodes, verts, node_radius, status=None, normalize=True, prev_nodes=0, first_vert=0,
+                    knn=None):
+        """ws_skinning_ex, or with prev_nodes > 0 ws_skinning_incremental starting surfels first_vert.. from
+        `knn`; returns (knn, spatial weights, connect weights) of all surfels (rows before first_vert as given)."""
+        nd = _dev(nodes, self.device, torch.float32)
+        v = _dev(verts, self.device, torch.float32)
+        stt = None if status is None else _dev(np.ascontiguousarray(status, np.uint32).view(np.int32), self.device)
+        s = int(v.shape[0])
+        if knn is None:
+            kt = torch.zeros((s, 4), dtype=torch.int16, device=self.device)
+        else:
+            kt = _dev(np.ascontiguousarray(knn, np.uint16).view(np.int16), self.device)
+        sw = torch.zeros((s, 4), dtype=torch.float32, device=self.device)
+        cw = torch.zeros((s, 4), dtype=torch.float32, device=self.device)
+        if prev_nodes > 0 or first_vert > 0:
+            check(self.lib.ws_skinning_incremental(_ptr(nd), _ptr(stt), int(nd.shape[0]), int(prev_nodes), _ptr(v), s,
+                                                   int(first_vert), float(node_radius), 1 if normalize else 0,
+                                                   _ptr(kt), _ptr(sw), _ptr(cw), self._stream()),
+                  "ws_skinning_incremental")
+        else:
+            check(self.lib.ws_skinning_ex(_ptr(nd), _ptr(stt), int(nd.shape[0]), _ptr(v), s, float(node_radius),
+                                          1 if normalize else 0, _ptr(kt), _ptr(sw), _ptr(cw), self._stream()),
+                  "ws_skinning_ex")
+        return kt.cpu().numpy().view(np.uint16), sw.cpu().numpy(), cw.cpu().numpy()
+
     def skinning(self, nodes, verts, node_radius):
         nd = _dev(nodes, self.device, torch.float32)
         v = _dev(verts, self.device, torch.float32)
@@ -403,6 +440,26 @@ class GpuGeometry:
                                        clip_near, clip_far, radius_scale, _ptr(vert), _ptr(nrm), self._stream()),
               "ws_measure_maps")
         return vert.cpu().numpy(), nrm.cpu().numpy()
+
+    def render_solver_maps(self, vertex_confid, normal_radius, color_time, cam, world2camera, max_depth,
+                           current_time, conf_threshold=1.0, time_threshold=3.0, footprint=0):
+        """ws_render_solver_maps: (index (H, W) uint32, vertex, normal, rgbd (H, W, 4) float32)."""
+        from ._lib import WsRenderParams
+        vc = _dev(vertex_confid, self.device, torch.float32)
+        nr = _dev(normal_radius, self.device, torch.float32)
+        ct = _dev(color_time, self.device, torch.float32)
+        p = WsRenderParams()
+        p.width, p.height = cam.width, cam.height
+        p.fx, p.fy, p.cx, p.cy = cam.fx, cam.fy, cam.cx, cam.cy
+        p.world2camera[:] = [float(v) for v in np.asarray(world2camera, np.float32).reshape(-1)]
+        p.max_depth, p.current_time = max_depth, current_time
+        p.confidence_threshold, p.time_threshold, p.footprint = conf_threshold, time_threshold, footprint
+        idx = torch.empty((cam.height, cam.width), dtype=torch.int32, device=self.device)
+        maps = [torch.empty((cam.height, cam.width, 4), dtype=torch.float32, device=self.device) for _ in range(3)]
+        check(self.lib.ws_render_solver_maps(_ptr(vc), _ptr(nr), _ptr(ct), int(vc.shape[0]), C.byref(p), _ptr(idx),
+                                             _ptr(maps[0]), _ptr(maps[1]), _ptr(maps[2]), self._stream()),
+              "ws_render_solver_maps")
+        return (idx.cpu().numpy().view(np.uint32),) + tuple(m.cpu().numpy() for m in maps)
 
     def splat(self, verts, cam, footprint):
         v = _dev(verts, self.device, torch.float32)

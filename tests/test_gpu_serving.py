@@ -133,3 +133,32 @@ def test_served_frame_within_tolerance_of_the_fp64_oracle(streams, orc):
     ref = orc.solve(host, gn_iters=5, pcg_iters=20)
     err = twist_error(out.cpu().numpy(), ref, host.nodes)
     assert err <= TWIST_TOL, err
+
+
+def test_chained_frames_of_a_large_stream_match_the_fp64_oracle(ws, orc):
+    """Serving's own configuration at its upper size: one stream of about 9k nodes (the scene
+    family of the serving workload, 8-NN graph, 130 surfels per node), frames 0-3 submitted back
+    to back; the server solves each from the warp its previous frame produced.  Each frame's
+    solution is checked against the FP64 oracle started from the oracle's solution of the
+    previous frame, within 1e-4 relative twist error and 1e-5 m."""
+    import torch
+    from starhub_b200 import serving
+    from starhub_b200.scenes import position_error, twist_error
+    (s,) = serving.build_streams([9000], frames=4, seed=11)
+    assert s.ds.num_nodes > 8000 and s.scene.graph_k == 8
+    outs = [torch.zeros((s.ds.num_nodes, 8), device="cuda") for _ in range(4)]
+    with _server([s], executors=2) as srv:
+        sid = srv.add_scene(s.ds)
+        rids = [_submit(srv, sid, s, k, outs[k]) for k in range(4)]
+        assert all(srv.wait(r)["status"] == 0 for r in rids)
+    torch.cuda.synchronize()
+    prev = None
+    for k in range(4):
+        fr = s.frame(k)
+        host = dataclasses.replace(s.scene, meas_vertex=fr.measure_vertex.cpu().numpy(),
+                                   meas_normal=fr.measure_normal.cpu().numpy())
+        ref = orc.solve(host, gn_iters=5, pcg_iters=20, init_dq=prev)
+        got = outs[k].cpu().numpy()
+        assert twist_error(got, ref, host.nodes) <= TWIST_TOL, (k, twist_error(got, ref, host.nodes))
+        assert position_error(host, got, ref) <= 1e-5, k
+        prev = ref

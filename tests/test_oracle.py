@@ -258,3 +258,34 @@ def test_voxel_keys_sort_as_signed_ints(orc):
     pts = np.array([[0.0, 0.0, 1.0, 1.0], [0.0, 0.0, -6.0, 1.0]], np.float32)   # vz = 100, vz = -600
     out = orc.OracleGeometry().voxel_subsample(pts, voxel)
     np.testing.assert_array_equal(out[:, 2], np.array([-6.0, 1.0], np.float32))
+
+
+def test_render_solver_maps_rules(orc):
+    """The oracle's restatement of the solver-map pass (shaders/solver_map.vert:29-33) on a hand
+    case: nearest surfel wins a pixel, equal depth keeps the lower id, z >= max depth and z <= 0
+    are culled, an unstable surfel is culled unless recently observed."""
+    from starhub_b200.scenes import Camera
+    cam = Camera(8, 6, 10.0, 10.0, 4.0, 3.0)
+    vc = np.array([[0.0, 0.0, 1.0, 5.0],      # pixel (4, 3), z = 1
+                   [0.0, 0.0, 0.5, 5.0],      # same pixel, nearer: wins
+                   [0.0, 0.0, 0.5, 5.0],      # same depth, higher id: loses
+                   [0.1, 0.0, 2.0, 5.0],      # z = max depth: culled
+                   [0.0, 0.1, -1.0, 5.0],     # behind the camera: culled
+                   [0.2, 0.0, 1.0, 0.5],      # unstable, observed at t = 9 (|9 - 10| < 3): drawn
+                   [-0.2, 0.0, 1.0, 0.5]],    # unstable, observed at t = 2: culled
+                  np.float32)
+    nr = np.tile(np.array([[0, 0, -1, 0.002]], np.float32), (len(vc), 1))
+    ct = np.zeros((len(vc), 4), np.float32)
+    ct[:, 2] = [10, 10, 10, 10, 10, 9, 2]
+    idx, vmap, nmap, rgbd = orc.render_solver_maps(vc, nr, ct, cam, np.eye(4), max_depth=2.0, current_time=10.0)
+    assert idx[3, 4] == 1
+    assert idx[3, 6] == 5                       # floor(10 * 0.2 / 1 + 4 + 0.5) = 6
+    assert (idx != 0xFFFFFFFF).sum() == 2
+    np.testing.assert_array_equal(vmap[3, 4], [0.0, 0.0, 0.5, 1.0])
+    np.testing.assert_array_equal(nmap[3, 4], [0.0, 0.0, -1.0, 0.0])
+    assert rgbd[3, 4, 3] == np.float32(2.0)
+    assert (vmap[idx == 0xFFFFFFFF] == 0).all()
+    # without the recent-observation pass every unstable surfel is culled
+    idx2, _, _, _ = orc.render_solver_maps(vc, nr, ct, cam, np.eye(4), max_depth=2.0, current_time=10.0,
+                                           time_threshold=-1.0)
+    assert (idx2 != 0xFFFFFFFF).sum() == 1
