@@ -21,6 +21,8 @@ constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;
 constexpr uint32_t kItemRowStart = 0x80000000u;   // item_col: the row's first (diagonal) item
 constexpr int kRowsPerGroup = 16;   // PCG rows (nodes) per scene-aligned reduction group (divides 32)
+// PCG phase-A work units per warp: the units are balanced by stored blocks and taken by ticket.
+constexpr int kPcgUnitsPerWarp = 2;
 
 // Dense-term record layouts, chosen per batch.  With the optical-flow term (some scene of the
 // batch has lambda_of != 0) a record holds C = 3 channels in 128 B: gradients 0..17 (three

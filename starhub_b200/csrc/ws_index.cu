@@ -444,9 +444,9 @@ __global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *item_ptr, co
     }
 }
 
-// First row group of every PCG warp, chosen so that the warps' stored blocks (items) are
-// about equal: warp w starts at the first group whose first item is at or past w / warps
-// of all items.
+// First row group of every PCG work unit (kPcgUnitsPerWarp per warp), chosen so that the units'
+// stored blocks (items) are about equal: unit w starts at the first group whose first item is at
+// or past w / units of all items.
 __global__ void k_pcg_ranges(const uint32_t *item_ptr, const uint32_t *group_row, uint32_t groups,
                              uint32_t total_nodes, uint32_t cap_items, uint32_t warps, uint32_t *warp_groups) {
     const uint32_t total = min(item_ptr[total_nodes], cap_items);
@@ -555,7 +555,7 @@ void index_build(Workspace &w, cudaStream_t st) {
 }
 
 void pcg_ranges(Workspace &w, cudaStream_t st) {
-    const uint32_t warps = (uint32_t)(pcg_launch_blocks(w) * pcg_warps_per_block());
+    const uint32_t warps = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
     k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.item_ptr, w.chunk_row, w.total_chunks,
                                                                       w.total_nodes, w.cap_items, warps,
                                                                       w.pcg_warp_groups);

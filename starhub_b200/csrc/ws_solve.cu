@@ -846,9 +846,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
 // Persistent block PCG (BlockPCG<6>::SolveNoConvergeCheck,
 // libs/star/pcg_solver/BlockPCG.cuh:67-190, 325-484) for every scene of the batch.
 //
-// Rows (nodes) are grouped in scene-aligned groups of kRowsPerGroup; every warp
-// owns a contiguous range of groups (balanced by stored blocks) and walks their rows,
-// with no block-level synchronisation.
+// Rows (nodes) are grouped in scene-aligned groups of kRowsPerGroup.  Phase A (the SpMV) works on
+// units, contiguous ranges of groups balanced by stored blocks (kPcgUnitsPerWarp per warp), which
+// the warps take by ticket: one counter grows through the launch, tickets it*U .. (it+1)*U - 1
+// are the units of iteration it, and a warp keeps the ticket that ended its iteration for the
+// next one.  So the warps that finish early take the remaining units instead of waiting for the
+// slowest, and every unit is processed once per iteration.  The per-row phases (init, phase B,
+// the twist update) take equal numbers of groups per warp.  No block-level synchronisation.
 // Per iteration: phase A  d = s + beta d (recomputed for neighbours from s and the
 // previous d), q = A d from each stored block read once (the transposed products go
 // to the lower rows through a contribution buffer), <d, A d>;  phase B  alpha,
@@ -869,7 +873,9 @@ struct PcgArgs {
     const uint32_t *item_ptr;      // [nodes + 1] first item of every row in the symmetric store
     const uint4 *item_info;        // per item: column, CSR slot of the transposed use, row, scene
     const uint32_t *item_col;      // per item: column | kItemRowStart on a row's diagonal item
-    const uint32_t *warp_groups;   // [warps + 1] first row group of each warp
+    const uint32_t *warp_groups;   // [units + 1] first row group of each phase-A work unit
+    uint32_t total_units;          // kPcgUnitsPerWarp x the launch's warps
+    uint32_t *tickets;             // work-unit tickets, growing through a launch (zeroed before it)
     const float *sym_blocks;       // per item: the 6x6 block, row-major
     const float *inv_diag, *jtr;
     float *contrib;                // per lower entry (row j, column i < j): B^T v_i left for row j
@@ -1093,7 +1099,8 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 // A warp's items are contiguous, so its blocks stream in as whole lines:
 //   * the item records of chunk j + 2 are loaded while chunk j is computed;
 //   * the blocks (9 x 16 B each, contiguous) and the column vector records of chunk j + 1
-//     are copied into shared memory with cp.async, also while chunk j is computed;
+//     are copied into shared memory with cp.async, also while chunk j is computed, and the
+//     blocks of chunk j + 3 are requested into L2 by a bulk prefetch;
 //   * a row's diagonal item (always its first) publishes v_i through a ring in shared
 //     memory, where the row's later items, in this chunk or a later one, read it;
 //   * the lane that ends a row sums the row's products in item order, continuing a row
@@ -1119,6 +1126,15 @@ __device__ __forceinline__ uint4 load_item(const uint4 *info, uint32_t u, uint32
     uint4 v = make_uint4(0u, kInvalidIndex, kInvalidIndex, 0u);
     if (u < end) v = __ldg(info + u);
     return v;
+}
+
+// Asks L2 for the blocks of items u .. u + 31 (below u_end) ahead of their cp.async copies: one
+// bulk prefetch of up to 32 contiguous 144-byte blocks, issued by one lane.
+__device__ __forceinline__ void l2_prefetch_blocks(const float *blocks, uint32_t u, uint32_t u_end) {
+    if (u < u_end) {
+        const uint32_t bytes = 144u * min(32u, u_end - u);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(blocks + 36ull * u), "r"(bytes) : "memory");
+    }
 }
 
 __device__ __forceinline__ void cp_async16(float *dst, const float *src) {
@@ -1191,6 +1207,7 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
         // chunk j + 1 in flight, chunk j + 2 records requested
         PcgOperands next;
         issue_chunk(A, vec_in, u0 + 32 * (j + 1), u1, nxt, stage[(j + 1) & 1], lane, next);
+        if (lane == 0) l2_prefetch_blocks(A.sym_blocks, u0 + 32 * (j + 3), u1);   // two chunks further
         const uint4 after = load_item(A.item_info, u0 + 32 * (j + 2) + lane, u1);
         cp_async_wait_prior();
         __syncwarp();
@@ -1383,11 +1400,6 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
-    // phase A: this warp's contiguous range of row groups, balanced by stored blocks
-    const uint32_t g_begin = min(A.warp_groups[gwarp], A.total_groups);
-    const uint32_t g_end = max(g_begin, min(A.warp_groups[gwarp + 1], A.total_groups));
-    const uint32_t r_begin = g_begin < A.total_groups ? A.group_row[g_begin] : A.total_nodes;
-    const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
     // init, phase B and the twist update work per row, so they take an equal number of groups
     // per warp instead; every phase reads what others wrote only after a wait for all the groups
     // of the scene, so the two partitions need not agree
@@ -1414,14 +1426,32 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
     }
     publish_range(A, b_begin, b_end, 2, 0, lane);
-    if (!wait_scenes(A, g_begin, g_end, 1, 1u, lane)) return;
+
+    // the warp's next phase-A ticket (see the header comment)
+    uint32_t ticket = 0;
+    if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
+    ticket = __shfl_sync(0xffffffffu, ticket, 0);
 
     for (int it = 0; it < A.pcg_iters; ++it) {
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
         float *sd_new = (it & 1) ? A.sd0 : A.sd1;
-        // ---- phase A: d = s + beta d, q = A d, <d, q> ----
-        stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
-        publish_range(A, g_begin, g_end, 0, it, lane);
+        // ---- phase A: d = s + beta d, q = A d, <d, q>, unit by unit ----
+        const uint32_t first = (uint32_t)it * A.total_units;
+        while (ticket < first + A.total_units) {
+            const uint32_t u = ticket - first;
+            const uint32_t g_begin = min(A.warp_groups[u], A.total_groups);
+            const uint32_t g_end = max(g_begin, min(A.warp_groups[u + 1], A.total_groups));
+            if (g_begin < g_end) {
+                const uint32_t r_begin = A.group_row[g_begin];
+                const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
+                // the unit's scenes have finished the last iteration's phase B (init for the first)
+                if (!wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 1u, lane)) return;
+                stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
+                publish_range(A, g_begin, g_end, 0, it, lane);
+            }
+            if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
+            ticket = __shfl_sync(0xffffffffu, ticket, 0);
+        }
         if (!wait_scenes(A, b_begin, b_end, 0, (uint32_t)it + 1u, lane)) return;
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
         for (uint32_t g = b_begin; g < b_end; g += kGroupsPerStep) {
@@ -1449,7 +1479,6 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
             if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
         }
         publish_range(A, b_begin, b_end, 1, it + 1, lane);
-        if (it + 1 < A.pcg_iters && !wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 2u, lane)) return;
     }
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
     //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
@@ -1503,28 +1532,25 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 // resolve in L2 (y of the whole batch fits there), so DRAM sees the blocks, the item records,
 // x and y once each: no contribution buffer and no second pass.  Sums meet in no fixed order.
 // The kernel streams a warp's contiguous blocks through kSpmvBuffers shared-memory buffers of
-// 4.6 KB: a chunk's blocks arrive with cp.async (every copy instruction moves 512 contiguous
-// bytes), each lane moves its item's block into registers, and the buffer at once takes the
-// copies of the chunk kSpmvBuffers ahead, which overlap the arithmetic of the chunks between.
-// x of the items' columns is loaded a chunk ahead into registers, the items' 4-byte column
-// words (item_col: the column, with the row's start marked) two chunks ahead.  Warp v takes part v % kSpmvSplit of PCG range v / kSpmvSplit (by row groups), so the
-// ranges are the PCG's, at kSpmvSplit times the warps.
+// 4.6 KB: a chunk's 32 blocks (4608 contiguous bytes) arrive as one 1-D bulk copy
+// (cp.async.bulk, issued by lane 0, its bytes counted on the buffer's mbarrier), each lane moves
+// its item's block into registers, and the buffer at once takes the bulk copy of the chunk
+// kSpmvBuffers ahead, which overlaps the arithmetic of the chunks between.  x of the items'
+// columns is loaded a chunk ahead into registers, the items' 4-byte column words (item_col: the
+// column, with the row's start marked) two chunks ahead.  Warp v takes part v % kSpmvSplit of the
+// PCG's work units kPcgUnitsPerWarp (v / kSpmvSplit) .. + kPcgUnitsPerWarp - 1 (by row groups), so
+// the ranges are the PCG's, at kSpmvSplit times the warps.
 constexpr int kSpmvRing = 64;
 constexpr int kSpmvBuffers = 2;
 constexpr int kSpmvSplit = 1;
 constexpr int kSpmvBlocksPerSm = 3;   // kSpmvSplit x the PCG's 3 blocks per SM: one wave of 12 warps per SM
-constexpr int kSpmvWarpFloats = kSpmvBuffers * 32 * 36 + kSpmvRing * 8 + 32 * 8;
+// per warp: the buffers, the row ring, the lanes' products and one 16-byte slot per mbarrier, a
+// multiple of 4 floats, so that every warp's buffers start on the 16-byte boundary a bulk copy needs
+constexpr int kSpmvWarpFloats = kSpmvBuffers * 32 * 36 + kSpmvRing * 8 + 32 * 8 + 4 * kSpmvBuffers;
+static_assert(kSpmvWarpFloats % 4 == 0, "warp areas on 16-byte boundaries");
+// polls of an mbarrier phase before a wait gives up (each poll may suspend the thread a while)
+constexpr int kSpmvMaxPolls = 1 << 22;
 constexpr size_t kSpmvSmemBytes = sizeof(float) * (kPcgThreads / 32) * kSpmvWarpFloats;
-__device__ __forceinline__ void spmv_issue_blocks(const PcgArgs &A, uint32_t u, uint32_t u_end, float *buf, int lane) {
-    const uint32_t nparts = u < u_end ? 9u * min(32u, u_end - u) : 0u;
-    const float *src = A.sym_blocks + 36ull * u;
-#pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        const uint32_t part = 32u * p + lane;
-        if (part < nparts) cp_async16(buf + 4 * part, src + 4ull * part);
-    }
-    cp_async_commit();
-}
 // Item word of the standalone SpMV: column | kItemRowStart on a row's first (diagonal) item,
 // kInvalidIndex past the end of the range.
 __device__ __forceinline__ uint32_t load_col(const uint32_t *cols, uint32_t u, uint32_t end) {
@@ -1539,6 +1565,39 @@ __device__ __forceinline__ void spmv_load_x(const PcgArgs &A, const float *x, ui
         x1 = __ldg(reinterpret_cast<const float2 *>(x + 8ull * col + 4));
     }
 }
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+// Lane 0: the blocks of items u .. u + 31 (below u_end) into `buf` by one bulk copy whose bytes
+// complete the current phase of `bar`; past the range, a plain arrival completes it.  The proxy
+// fence orders the lanes' earlier reads of `buf` (ordered before it by the caller's __syncwarp)
+// before the bulk copy's writes.  Block addresses are multiples of 144 bytes from a 256-byte
+// aligned base, so every copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
+__device__ __forceinline__ void spmv_bulk_blocks(const PcgArgs &A, uint32_t u, uint32_t u_end, float *buf,
+                                                 unsigned long long *bar) {
+    if (u >= u_end) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+        return;
+    }
+    const unsigned bytes = 144u * min(32u, u_end - u);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_addr(buf)), "l"(A.sym_blocks + 36ull * u), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+// Waits for phase `parity` of `bar` to complete; false when kSpmvMaxPolls polls ran out.  The
+// warp agrees on the outcome, so a timeout leaves it converged.
+__device__ __forceinline__ bool spmv_wait(unsigned long long *bar, unsigned parity) {
+    bool ok = false;
+    for (int i = 0; i < kSpmvMaxPolls && !ok; ++i) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+        ok = done != 0;
+    }
+    return __all_sync(0xffffffffu, ok);
+}
 __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs A, const float *x, float *y) {
     // per warp: the chunk buffers, x of recent rows (by row), each lane's B x_col
     extern __shared__ __align__(16) float spmv_smem[];
@@ -1546,10 +1605,12 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     float *bufs = spmv_smem + (threadIdx.x >> 5) * kSpmvWarpFloats;
     float *ring = bufs + kSpmvBuffers * 32 * 36;
     float *prod = ring + kSpmvRing * 8;
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(prod + 32 * 8);   // 16-byte aligned
+    unsigned phases = 0;   // bit k: parity of the next completion of buffer k
     const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t pv = v / kSpmvSplit, part = v % kSpmvSplit;
-    const uint32_t pg0 = min(A.warp_groups[pv], A.total_groups);
-    const uint32_t pg1 = max(pg0, min(A.warp_groups[pv + 1], A.total_groups));
+    const uint32_t pg0 = min(A.warp_groups[kPcgUnitsPerWarp * pv], A.total_groups);
+    const uint32_t pg1 = max(pg0, min(A.warp_groups[kPcgUnitsPerWarp * (pv + 1)], A.total_groups));
     const uint32_t g0 = pg0 + ((pg1 - pg0) * part + kSpmvSplit - 1) / kSpmvSplit;
     const uint32_t g1 = pg0 + ((pg1 - pg0) * (part + 1) + kSpmvSplit - 1) / kSpmvSplit;
     if (g0 >= g1) return;
@@ -1560,8 +1621,13 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     float4 xa;
     float2 xb;
     spmv_load_x(A, x, cur, xa, xb);
-#pragma unroll
-    for (int k = 0; k < kSpmvBuffers; ++k) spmv_issue_blocks(A, u0 + 32u * k, u1, bufs + k * 32 * 36, lane);
+    if (lane == 0) {
+        for (int k = 0; k < kSpmvBuffers; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bars + k)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        for (int k = 0; k < kSpmvBuffers; ++k) spmv_bulk_blocks(A, u0 + 32u * k, u1, bufs + k * 32 * 36, bars + k);
+    }
+    __syncwarp();
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     uint32_t carry_row = kInvalidIndex;
     // the row of the item before the chunk; the range starts with row r0's diagonal item, so
@@ -1585,15 +1651,19 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         }
         // every copy group commits in order: this chunk's is done when at most the
         // kSpmvBuffers - 1 later ones are pending
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kSpmvBuffers - 1) : "memory");
-        __syncwarp();
+        const int bk = chunk % kSpmvBuffers;
+        if (!spmv_wait(bars + bk, (phases >> bk) & 1u)) {
+            if (lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
+            break;
+        }
+        phases ^= 1u << bk;
         float4 b[9];
 #pragma unroll
         for (int q = 0; q < 9; ++q) b[q] = reinterpret_cast<const float4 *>(buf + 36 * lane)[q];
         __syncwarp();
         // the buffer is free: the blocks kSpmvBuffers chunks ahead and the next x arrive while
         // this chunk is computed
-        spmv_issue_blocks(A, u + 32u * kSpmvBuffers, u1, buf, lane);
+        if (lane == 0) spmv_bulk_blocks(A, u + 32u * kSpmvBuffers, u1, buf, bars + bk);
         spmv_load_x(A, x, nxt, xa, xb);
         float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
@@ -1662,7 +1732,10 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         cur = nxt;
         nxt = after;
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");   // the last (empty) copy group
+    // every buffer has one phase outstanding (a copy, or an arrival past the range): wait for it,
+    // so that no bulk copy still writes when the block's shared memory is released
+    for (int k = 0; k < kSpmvBuffers; ++k)
+        if (!spmv_wait(bars + k, (phases >> k) & 1u) && lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
 }
 
 // ---------------------------------------------------------------------------
@@ -1949,6 +2022,8 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.item_col = w.item_col;
     a.contrib = w.contrib;
     a.warp_groups = w.pcg_warp_groups;
+    a.total_units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
+    a.tickets = w.pcg_tickets;
     a.sym_blocks = w.sym_blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
@@ -1975,6 +2050,7 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     // tickets and generations start at zero every launch, so a launch that timed out half-way
     // cannot leak into the next
     cudaMemsetAsync(w.scene_counter, 0, sizeof(uint32_t) * kSceneSync * (size_t)w.num_scenes, st);
+    cudaMemsetAsync(w.pcg_tickets, 0, sizeof(uint32_t), st);
     void *args[] = {&a};
     count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);

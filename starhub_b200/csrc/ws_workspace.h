@@ -99,7 +99,9 @@ struct Workspace {
     uint32_t *item_col = nullptr;                            // [cap_items]
     float *sym_blocks = nullptr;                             // [cap_items * 36]
     float *contrib = nullptr;                                // [cap_half * 8]
-    uint32_t *pcg_warp_groups = nullptr;                     // [pcg_grid * warps per block + 1]
+    uint32_t *pcg_warp_groups = nullptr;                     // [kPcgUnitsPerWarp * pcg_grid * warps per block + 1]:
+                                                             // first row group of every PCG work unit
+    uint32_t *pcg_tickets = nullptr;                         // [1]: PCG work-unit tickets, zeroed per launch
     float *mf_ux = nullptr;             // matrix-free SpMV scratch: J x per dense term and edge (float4),
                                         // allocated on first use
 

