@@ -189,11 +189,11 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.item_info, w.cap_items));
     A(dalloc(&w.item_col, w.cap_items));
     A(dalloc(&w.sym_blocks, (size_t)w.cap_items * 36));
-    A(dalloc(&w.contrib, (size_t)std::max<uint32_t>(1u, w.cap_half) * 8));
+    A(dalloc(&w.contrib, (size_t)std::max<uint32_t>(1u, w.cap_half) * 6));
     A(dalloc(&w.inv_diag, (size_t)w.cap_nodes * 36));
     A(dalloc(&w.diag64, (size_t)w.cap_nodes * 21));
     for (float **v : {&w.jtr, &w.x, &w.r, &w.q}) A(dalloc(v, (size_t)w.cap_nodes * ws::kVecStride));
-    for (float **v : {&w.sd0, &w.sd1}) A(dalloc(v, (size_t)w.cap_nodes * 2 * ws::kVecStride));
+    for (float **v : {&w.sd0, &w.sd1}) A(dalloc(v, (size_t)w.cap_nodes * ws::kSdStride));
     A(dalloc(&w.se3, (size_t)w.cap_nodes * 8));
     A(dalloc(&w.centers, w.cap_nodes));
     A(dalloc(&w.chunk_partial, w.cap_chunks));
@@ -860,15 +860,15 @@ int ws_get_system(ws_solver *h, int scene, uint32_t *rowptr, uint32_t *cols, flo
         const auto ip = download(w.item_ptr + sc.node_base, (size_t)sc.num_nodes + 1);
         const uint32_t ub = ip.front(), ue = ip.back();
         const auto sb = download(w.sym_blocks + 36ull * ub, 36ull * (ue - ub));
-        const auto info = download(w.item_info + ub, (size_t)(ue - ub));
+        const auto cols = download(w.item_col + ub, (size_t)(ue - ub));   // upper items carry no row mark
         const uint32_t nb = (uint32_t)sc.node_base;
         auto upper = [&](uint32_t i, uint32_t col) -> const float * {   // local row i, global column
             uint32_t lo = ip[i] + 1, hi = ip[i + 1];
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (info[mid - ub].x < col) lo = mid + 1; else hi = mid;
+                if (cols[mid - ub] < col) lo = mid + 1; else hi = mid;
             }
-            if (lo >= ip[i + 1] || info[lo - ub].x != col) return nullptr;
+            if (lo >= ip[i + 1] || cols[lo - ub] != col) return nullptr;
             return sb.data() + 36ull * (lo - ub);
         };
         for (int i = 0; i < sc.num_nodes; ++i)

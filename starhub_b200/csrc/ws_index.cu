@@ -399,9 +399,9 @@ __global__ void k_col_kv(const uint32_t *half_col, const uint32_t *counts, uint3
 // k among the pairs sorted by column (then row).
 __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, const uint32_t *counts,
                         const uint32_t *half_row, const uint32_t *half_col, const uint32_t *row_first,
-                        const uint32_t *row_cnt_lo, const uint32_t *rowptr, const uint32_t *node_scene,
-                        uint32_t cap_blocks, uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx,
-                        uint4 *item_info, uint32_t *item_col, int *err) {
+                        const uint32_t *row_cnt_lo, const uint32_t *rowptr, uint32_t cap_blocks,
+                        uint32_t *slot_up, uint32_t *slot_lo, uint32_t *colidx, uint2 *item_info,
+                        uint32_t *item_col, int *err) {
     const uint32_t n = counts[kCntHalf];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t col = sorted_col[k];
@@ -424,21 +424,21 @@ __global__ void k_slots(const uint32_t *sorted_col, const uint32_t *sorted_h, co
         slot_up[h] = s_up;
         colidx[s_lo] = row;
         colidx[s_up] = half_col[h];
-        item_info[h + row + 1u] = make_uint4(half_col[h], k, row, node_scene[row]);
+        item_info[h + row + 1u] = make_uint2(half_col[h], k);
         item_col[h + row + 1u] = half_col[h];
     }
 }
 
-// Diagonal slot of every row, plus the packed (col, ref, row, scene) record of each slot of
-// the row that the PCG streams.
+// Diagonal slot of every row, and the item records of the row's diagonal item (the row, marked
+// as a row start, and its scene).
 __global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *item_ptr, const uint32_t *node_scene,
-                            uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx, uint4 *item_info,
+                            uint32_t total_nodes, uint32_t cap_blocks, uint32_t *colidx, uint2 *item_info,
                             uint32_t *item_col, int *err) {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_nodes; g += gridDim.x * blockDim.x) {
         const uint32_t s = rowptr[g];
         if (s < cap_blocks) colidx[s] = g;
         // the row's first item is its diagonal block
-        item_info[item_ptr[g]] = make_uint4(g, kInvalidIndex, g, node_scene[g]);
+        item_info[item_ptr[g]] = make_uint2(g | kItemRowStart, node_scene[g]);
         item_col[item_ptr[g]] = g | kItemRowStart;
         if (g + 1 == total_nodes && rowptr[total_nodes] > cap_blocks) set_error(err, WS_ERR_CAPACITY);
     }
@@ -545,7 +545,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     const uint32_t *scol = col_alt ? w.col_key_alt : w.col_key;
     const uint32_t *sh = col_alt ? w.col_val_alt : w.col_val;
     k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,
-                                                                    w.row_first, w.row_cnt_lo, w.rowptr, w.node_scene,
+                                                                    w.row_first, w.row_cnt_lo, w.rowptr,
                                                                     w.cap_blocks, w.half_slot_up, w.half_slot_lo, w.colidx,
                                                                     w.item_info, w.item_col, w.error_flag);
     k_diag_cols<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.rowptr, w.item_ptr, w.node_scene, N, w.cap_blocks,

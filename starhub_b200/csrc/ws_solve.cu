@@ -851,8 +851,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
 // the warps take by ticket: one counter grows through the launch, tickets it*U .. (it+1)*U - 1
 // are the units of iteration it, and a warp keeps the ticket that ended its iteration for the
 // next one.  So the warps that finish early take the remaining units instead of waiting for the
-// slowest, and every unit is processed once per iteration.  The per-row phases (init, phase B,
-// the twist update) take equal numbers of groups per warp.  No block-level synchronisation.
+// slowest, and every unit is processed once per iteration.  Phase B takes units of
+// kPcgBUnitGroups row groups the same way from a second counter.  Init and the twist update take
+// equal numbers of groups per warp.  No block-level synchronisation.
 // Per iteration: phase A  d = s + beta d (recomputed for neighbours from s and the
 // previous d), q = A d from each stored block read once (the transposed products go
 // to the lower rows through a contribution buffer), <d, A d>;  phase B  alpha,
@@ -860,9 +861,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
 // A warp keeps its group's partial in FP64 registers, stores it, and the last group
 // of a scene to finish (a fenced atomic ticket) sums that scene's group partials in
 // group order, publishes alpha or beta and bumps the scene's generation counter; the
-// sums therefore never depend on the rest of the batch.  After each phase a warp waits
-// only for the scenes of its own rows; a wait is bounded, and a timed-out wait sets
-// WS_ERR_TIMEOUT and the warp leaves.
+// sums therefore never depend on the rest of the batch.  Before a unit a warp waits only for
+// the scenes of the unit's rows; a wait is bounded, and a timed-out wait sets WS_ERR_TIMEOUT and
+// the warp leaves.
 // ---------------------------------------------------------------------------
 
 struct PcgArgs {
@@ -871,16 +872,18 @@ struct PcgArgs {
     uint32_t total_groups;
     const uint32_t *rowptr;        // block-CSR row pointers (lower slots follow the diagonal)
     const uint32_t *item_ptr;      // [nodes + 1] first item of every row in the symmetric store
-    const uint4 *item_info;        // per item: column, CSR slot of the transposed use, row, scene
+    const uint2 *item_info;        // per item: column | kItemRowStart, lower entry (upper) or scene (diagonal)
     const uint32_t *item_col;      // per item: column | kItemRowStart on a row's diagonal item
     const uint32_t *warp_groups;   // [units + 1] first row group of each phase-A work unit
     uint32_t total_units;          // kPcgUnitsPerWarp x the launch's warps
-    uint32_t *tickets;             // work-unit tickets, growing through a launch (zeroed before it)
+    uint32_t *tickets;             // phase-A work-unit tickets, growing through a launch (zeroed before it)
+    uint32_t total_bunits;         // phase-B units: kPcgBUnitGroups row groups each
+    uint32_t *btickets;            // phase-B unit tickets, like `tickets`
     const float *sym_blocks;       // per item: the 6x6 block, row-major
     const float *inv_diag, *jtr;
-    float *contrib;                // per lower entry (row j, column i < j): B^T v_i left for row j
+    float *contrib;                // per lower entry (row j, column i < j): B^T v_i left for row j (6 floats)
     float *x, *r, *q;
-    float *sd0, *sd1;         // [node][16]: s (6, padded to 8) then d (6, padded); swapped every iteration
+    float *sd0, *sd1;         // [node][kSdStride]: s (6) then d (6); swapped every iteration
     double *group_partial;
     double *scalars;          // per scene: [0] delta, [1] alpha, [2] beta, [3] last reduced value
     // per scene, kSceneSync words: [0] phase-A tickets, [1] phase-B / init tickets (arrivals of
@@ -1067,6 +1070,14 @@ __device__ __forceinline__ void load6(const float *p, float *v) {
     const float2 b = __ldcg(reinterpret_cast<const float2 *>(p + 4));
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
 }
+__device__ __forceinline__ void load6_f2(const float *p, float *v) {   // 8-byte aligned source
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float2 a = __ldcg(reinterpret_cast<const float2 *>(p) + k);
+        v[2 * k] = a.x;
+        v[2 * k + 1] = a.y;
+    }
+}
 __device__ __forceinline__ void store6(float *p, const float *v) {
     reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
     reinterpret_cast<float2 *>(p + 4)[0] = make_float2(v[4], v[5]);
@@ -1097,12 +1108,16 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 // are numbered by row, then column, so the owner of row j adds its contributions
 // afterwards from one contiguous range, in column order (the CSR slot order).
 // A warp's items are contiguous, so its blocks stream in as whole lines:
-//   * the item records of chunk j + 2 are loaded while chunk j is computed;
-//   * the blocks (9 x 16 B each, contiguous) and the column vector records of chunk j + 1
-//     are copied into shared memory with cp.async, also while chunk j is computed, and the
-//     blocks of chunk j + 3 are requested into L2 by a bulk prefetch;
-//   * a row's diagonal item (always its first) publishes v_i through a ring in shared
-//     memory, where the row's later items, in this chunk or a later one, read it;
+//   * the 32 blocks of a chunk (4608 contiguous bytes) arrive as one 1-D bulk copy
+//     (cp.async.bulk, issued by lane 0, its bytes counted on the buffer's mbarrier) into one of
+//     two buffers; a buffer takes the copy of the chunk two ahead as soon as the lanes hold its
+//     blocks in registers, and the blocks of the chunk three ahead are requested into L2 by a
+//     bulk prefetch;
+//   * the item records (8 bytes) of chunk j + 2 are loaded while chunk j is computed, and the
+//     column s/d records (48 bytes, cp.async) of chunk j + 1;
+//   * a row's diagonal item (always its first) publishes v_i and its scene's beta through a
+//     ring in shared memory, where the row's later items, in this chunk or a later one, read
+//     them; rows follow from counting the items that start a row;
 //   * the lane that ends a row sums the row's products in item order, continuing a row
 //     that began in an earlier chunk from a carried partial sum.
 // This is phase A of a PCG iteration: v = d = s + beta d_old (recomputed for every column
@@ -1113,22 +1128,73 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 // results do not depend on which warp handled the row or on the batch.
 // ---------------------------------------------------------------------------
 constexpr int kPcgThreads = 128;                              // 4 warps per block
-constexpr int kPcgSlot = 52;                                  // block (36) + column vector record (16) per item
-constexpr int kPcgChunkFloats = 32 * kPcgSlot;
+constexpr int kPcgBlockFloats = 32 * 36;                      // one chunk's blocks
+constexpr int kPcgRecFloats = 32 * kSdStride;                 // one chunk's column records
 constexpr int kPcgRing = 64;                                  // rows kept in the per-warp rings
-constexpr int kPcgWarpFloats = 2 * kPcgChunkFloats + kPcgRing * 8 + 2 * kPcgRing;
+// per warp: two block buffers, two record buffers, the v/beta ring (8 floats a row), the
+// <d, A d> ring (a double a row) and two mbarriers; a multiple of 4 floats, so that every
+// warp's block buffers start on the 16-byte boundary a bulk copy needs
+constexpr int kPcgWarpFloats = 2 * kPcgBlockFloats + 2 * kPcgRecFloats + kPcgRing * 8 + 2 * kPcgRing + 4;
+static_assert(kPcgWarpFloats % 4 == 0, "warp areas on 16-byte boundaries");
 constexpr size_t kPcgSmemBytes = sizeof(float) * kPcgWarpFloats * (kPcgThreads / 32);
+// polls of an mbarrier phase before a wait gives up (each poll may suspend the thread a while)
+constexpr int kBulkMaxPolls = 1 << 22;
 
-// Item record (column, lower entry of the transposed use or kInvalidIndex for the diagonal,
-// row, scene); row = kInvalidIndex past the end of the range.  Loaded raw and only read
-// one chunk later, so the load never stalls the warp.
-__device__ __forceinline__ uint4 load_item(const uint4 *info, uint32_t u, uint32_t end) {
-    uint4 v = make_uint4(0u, kInvalidIndex, kInvalidIndex, 0u);
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+// Lane 0: the blocks of items u .. u + 31 (below u_end) into `buf` by one bulk copy whose bytes
+// complete the current phase of `bar`; past the range, a plain arrival completes it.  The proxy
+// fence orders the lanes' earlier reads of `buf` (ordered before it by a __syncwarp) before the
+// bulk copy's writes.  Block addresses are multiples of 144 bytes from a 256-byte aligned base,
+// so every copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
+__device__ __forceinline__ void bulk_blocks(const float *blocks, uint32_t u, uint32_t u_end, float *buf,
+                                            unsigned long long *bar) {
+    if (u >= u_end) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+        return;
+    }
+    const unsigned bytes = 144u * min(32u, u_end - u);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_addr(buf)), "l"(blocks + 36ull * u), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Lane 0: `n` mbarriers, each completed by one arrival (with its copy's bytes).
+__device__ __forceinline__ void bulk_init(unsigned long long *bars, int n) {
+    for (int k = 0; k < n; ++k)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bars + k)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// Waits for phase `parity` of `bar` to complete; false when kBulkMaxPolls polls ran out.  The
+// warp agrees on the outcome, so a timeout leaves it converged.
+__device__ __forceinline__ bool bulk_wait(unsigned long long *bar, unsigned parity) {
+    bool ok = false;
+    for (int i = 0; i < kBulkMaxPolls && !ok; ++i) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(smem_addr(bar)), "r"(parity)
+                     : "memory");
+        ok = done != 0;
+    }
+    return __all_sync(0xffffffffu, ok);
+}
+
+// Item record: column | kItemRowStart on a row's diagonal item, then the lower entry of the
+// transposed use (upper item) or the row's scene (diagonal item); column kInvalidIndex past
+// the end of the range.  Loaded raw and only read one chunk later, so the load never stalls
+// the warp.
+__device__ __forceinline__ uint2 load_item(const uint2 *info, uint32_t u, uint32_t end) {
+    uint2 v = make_uint2(kInvalidIndex, kInvalidIndex);
     if (u < end) v = __ldg(info + u);
     return v;
 }
 
-// Asks L2 for the blocks of items u .. u + 31 (below u_end) ahead of their cp.async copies: one
+// Asks L2 for the blocks of items u .. u + 31 (below u_end) ahead of their bulk copies: one
 // bulk prefetch of up to 32 contiguous 144-byte blocks, issued by one lane.
 __device__ __forceinline__ void l2_prefetch_blocks(const float *blocks, uint32_t u, uint32_t u_end) {
     if (u < u_end) {
@@ -1144,56 +1210,57 @@ __device__ __forceinline__ void cp_async16(float *dst, const float *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Operands of one chunk held in registers: the item record and (PCG) beta of its scene.
-struct PcgOperands {
-    uint4 item;
-    double beta;
-};
-
-// Starts the chunk of items u .. u + 31 (those below u_end): copies of the blocks and of
-// each item's column s/d record (64 B) into `stage`, and a register load of beta.  The
-// 16-byte parts (9 per block, 4 per record) are spread flat over the lanes, so every copy
-// instruction of the blocks reads 512 contiguous bytes.
-__device__ __forceinline__ void issue_chunk(const PcgArgs &A, const float *vec_in, uint32_t u, uint32_t u_end, uint4 x,
-                                           float *stage, int lane, PcgOperands &op) {
-    constexpr int kVecParts = 4;
-    op.item = x;
-    const float *vec = nullptr;
-    if (x.z != kInvalidIndex) {
-        vec = vec_in + 16ull * min(x.x, A.total_nodes - 1);
-        op.beta = __ldcg(A.scalars + 8ull * min(x.w, A.num_scenes - 1) + 2);
-    }
-    const uint32_t nparts = u < u_end ? 9u * min(32u, u_end - u) : 0u;
-    const float *src = A.sym_blocks + 36ull * u;
+// Starts the column side of a chunk: each lane copies its item's s/d record (3 x 16 B) into
+// its slot of `recs` and, on a diagonal item, loads its scene's beta into `beta`.
+__device__ __forceinline__ void issue_records(const PcgArgs &A, const float *vec_in, uint2 it, float *recs, int lane,
+                                             float &beta) {
+    beta = 0.f;
+    if (it.x != kInvalidIndex) {
+        const float *src = vec_in + (size_t)kSdStride * min(it.x & ~kItemRowStart, A.total_nodes - 1);
+        float *dst = recs + kSdStride * lane;
 #pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        const uint32_t part = 32u * p + lane, e = part / 9u, piece = part - 9u * e;
-        if (part < nparts) cp_async16(stage + kPcgSlot * e + 4 * piece, src + 4ull * part);
-    }
-#pragma unroll
-    for (int p = 0; p < kVecParts; ++p) {
-        const int part = 32 * p + lane, e = part / kVecParts, piece = part - kVecParts * e;
-        const float *v = reinterpret_cast<const float *>(
-            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vec), e));
-        if (v) cp_async16(stage + kPcgSlot * e + 36 + 4 * piece, v + 4 * piece);
+        for (int p = 0; p < kSdStride / 4; ++p) cp_async16(dst + 4 * p, src + 4 * p);
+        if (it.x & kItemRowStart) beta = (float)__ldcg(A.scalars + 8ull * min(it.y, A.num_scenes - 1) + 2);
     }
     cp_async_commit();
 }
 
-__device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
+__device__ __forceinline__ void store6_f2(float *p, const float *v) {   // 8-byte aligned destination
+#pragma unroll
+    for (int k = 0; k < 3; ++k) reinterpret_cast<float2 *>(p)[k] = make_float2(v[2 * k], v[2 * k + 1]);
+}
+
+// Phase A over items u0 .. u1 (rows r0 .. r1 - 1, groups g0 .. g1 - 1); false after a timed-out
+// wait for a bulk copy (WS_ERR_TIMEOUT is set).
+__device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
                              float *out, float *wsm, int lane) {
-    if (g0 >= g1) return;
-    float *stage[2] = {wsm, wsm + kPcgChunkFloats};
-    float *vring = wsm + 2 * kPcgChunkFloats;                           // [kPcgRing][8] v of the row, by row
+    if (g0 >= g1) return true;
+    float *blocks = wsm;                                                // [2][32][36]
+    float *recs = wsm + 2 * kPcgBlockFloats;                            // [2][32][kSdStride]
+    float *vring = recs + 2 * kPcgRecFloats;                            // [kPcgRing][8]: v of the row, beta
     double *gring = reinterpret_cast<double *>(vring + kPcgRing * 8);   // [kPcgRing] <d, A d> by row
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(gring + kPcgRing);
     const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
     const uint32_t nchunks = u1 > u0 ? (u1 - u0 + 31) / 32 : 0;
-    uint4 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
-    PcgOperands cur;
-    issue_chunk(A, vec_in, u0, u1, load_item(A.item_info, u0 + lane, u1), stage[0], lane, cur);
+    if (lane == 0) {
+        bulk_init(bars, 2);
+        bulk_blocks(A.sym_blocks, u0, u1, blocks, bars);
+        bulk_blocks(A.sym_blocks, u0 + 32, u1, blocks + kPcgBlockFloats, bars + 1);
+        l2_prefetch_blocks(A.sym_blocks, u0 + 64, u1);
+    }
+    __syncwarp();
+    unsigned phases = 0;   // bit k: parity of the next completion of buffer k's mbarrier
+    bool ok = true;
+    uint2 cur = load_item(A.item_info, u0 + lane, u1);
+    uint2 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
+    float beta_cur;
+    issue_records(A, vec_in, cur, recs, lane, beta_cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     double carry_dot = 0.0;
     uint32_t carry_row = kInvalidIndex;
+    // the row of the item before the chunk; the range starts with row r0's diagonal item, so
+    // an item's row is this plus the row starts up to and including it (unsigned wrap at r0 = 0)
+    uint32_t row_before = r0 - 1u;
     // first rows of groups win .. win + 31 (lane i holds group win + i), reloaded as groups complete
     uint32_t win = g0;
     uint32_t win_row = g0 + lane < A.total_groups ? A.group_row[g0 + lane] : A.total_nodes;
@@ -1204,45 +1271,65 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
     };
     uint32_t group = g0, group_end = group_first(g0 + 1);
     for (uint32_t j = 0; j < nchunks; ++j) {
-        // chunk j + 1 in flight, chunk j + 2 records requested
-        PcgOperands next;
-        issue_chunk(A, vec_in, u0 + 32 * (j + 1), u1, nxt, stage[(j + 1) & 1], lane, next);
-        if (lane == 0) l2_prefetch_blocks(A.sym_blocks, u0 + 32 * (j + 3), u1);   // two chunks further
-        const uint4 after = load_item(A.item_info, u0 + 32 * (j + 2) + lane, u1);
+        const int bk = (int)(j & 1u);
+        // column records of chunk j + 1 in flight, item records of chunk j + 2 requested
+        float beta_next;
+        issue_records(A, vec_in, nxt, recs + (bk ^ 1) * kPcgRecFloats, lane, beta_next);
+        if (lane == 0) l2_prefetch_blocks(A.sym_blocks, u0 + 32 * (j + 3), u1);
+        const uint2 after = load_item(A.item_info, u0 + 32 * (j + 2) + lane, u1);
+        if (!bulk_wait(bars + bk, (phases >> bk) & 1u)) {
+            if (lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
+            ok = false;
+            break;
+        }
+        phases ^= 1u << bk;
         cp_async_wait_prior();
         __syncwarp();
-        const bool valid = cur.item.z != kInvalidIndex;
-        const uint32_t xrow = valid ? min(cur.item.z, A.total_nodes - 1) : kInvalidIndex;
-        const uint32_t tslot = cur.item.y;
-        const bool diag = tslot == kInvalidIndex;
-        float *mine = stage[j & 1] + kPcgSlot * lane;
-        float vc[6];   // v of the item's column
+        const bool valid = cur.x != kInvalidIndex;
+        const bool diag = valid && (cur.x & kItemRowStart) != 0;
+        const unsigned row_starts = __ballot_sync(0xffffffffu, diag);
+        const uint32_t row = row_before + (uint32_t)__popc(row_starts & (0xffffffffu >> (31 - lane)));
+        row_before += (uint32_t)__popc(row_starts);
+        const uint32_t xrow = valid ? min(row, A.total_nodes - 1) : kInvalidIndex;
+        float *mine = recs + bk * kPcgRecFloats + kSdStride * lane;
+        float *vslot = vring + 8 * (xrow & (kPcgRing - 1));
+        float sv[6], dv[6];
         if (valid) {
-            const float4 s0 = reinterpret_cast<const float4 *>(mine + 36)[0];
-            const float2 s1 = reinterpret_cast<const float2 *>(mine + 40)[0];
-            const float beta = (float)cur.beta;
-            const float4 d0 = reinterpret_cast<const float4 *>(mine + 44)[0];
-            const float2 d1 = reinterpret_cast<const float2 *>(mine + 48)[0];
-            vc[0] = s0.x + beta * d0.x; vc[1] = s0.y + beta * d0.y; vc[2] = s0.z + beta * d0.z;
-            vc[3] = s0.w + beta * d0.w; vc[4] = s1.x + beta * d1.x; vc[5] = s1.y + beta * d1.y;
-            if (diag) {
-                float4 *vr = reinterpret_cast<float4 *>(vring + 8 * (xrow & (kPcgRing - 1)));
-                vr[0] = make_float4(vc[0], vc[1], vc[2], vc[3]);
-                vr[1] = make_float4(vc[4], vc[5], 0.f, 0.f);
+            const float4 a = reinterpret_cast<const float4 *>(mine)[0];
+            const float4 b = reinterpret_cast<const float4 *>(mine)[1];
+            const float4 c = reinterpret_cast<const float4 *>(mine)[2];
+            sv[0] = a.x; sv[1] = a.y; sv[2] = a.z; sv[3] = a.w; sv[4] = b.x; sv[5] = b.y;
+            dv[0] = b.z; dv[1] = b.w; dv[2] = c.x; dv[3] = c.y; dv[4] = c.z; dv[5] = c.w;
+            if (diag) {   // the row's v and beta for its later items
+                reinterpret_cast<float4 *>(vslot)[0] = make_float4(sv[0] + beta_cur * dv[0], sv[1] + beta_cur * dv[1],
+                                                                   sv[2] + beta_cur * dv[2], sv[3] + beta_cur * dv[3]);
+                reinterpret_cast<float4 *>(vslot)[1] =
+                    make_float4(sv[4] + beta_cur * dv[4], sv[5] + beta_cur * dv[5], beta_cur, 0.f);
             }
         }
         __syncwarp();
+        float vr[6], vc[6];   // v of the item's row and column
+        float4 blk[9];
         if (valid) {
-            const float4 v0 = reinterpret_cast<const float4 *>(vring + 8 * (xrow & (kPcgRing - 1)))[0];
-            const float2 v1 = reinterpret_cast<const float2 *>(vring + 8 * (xrow & (kPcgRing - 1)) + 4)[0];
-            const float vr[6] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y};   // v of the item's row
-            // B v_col and B^T v_row from one pass over the block, a float4 at a time
+            const float4 v0 = reinterpret_cast<const float4 *>(vslot)[0];
+            const float4 v1 = reinterpret_cast<const float4 *>(vslot)[1];
+            vr[0] = v0.x; vr[1] = v0.y; vr[2] = v0.z; vr[3] = v0.w; vr[4] = v1.x; vr[5] = v1.y;
+            const float beta = v1.z;   // the item's column lies in its row's scene
+#pragma unroll
+            for (int i = 0; i < 6; ++i) vc[i] = sv[i] + beta * dv[i];
+            const float4 *src = reinterpret_cast<const float4 *>(blocks + bk * kPcgBlockFloats + 36 * lane);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) blk[q] = src[q];
+        }
+        __syncwarp();
+        // the buffer is free: it takes the blocks of the chunk two ahead
+        if (lane == 0) bulk_blocks(A.sym_blocks, u0 + 32 * (j + 2), u1, blocks + bk * kPcgBlockFloats, bars + bk);
+        if (valid) {
+            // B v_col and B^T v_row from one pass over the block
             float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            const float4 *blk = reinterpret_cast<const float4 *>(mine);
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
-                const float4 v = blk[q];
-                const float e4[4] = {v.x, v.y, v.z, v.w};
+                const float e4[4] = {blk[q].x, blk[q].y, blk[q].z, blk[q].w};
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int e = 4 * q + k, r = e / 6, c = e % 6;
@@ -1250,11 +1337,7 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
                     t[c] += e4[k] * vr[r];
                 }
             }
-            if (!diag) {
-                float4 *co = reinterpret_cast<float4 *>(A.contrib + 8ull * min(tslot, A.cap_half - 1));
-                co[0] = make_float4(t[0], t[1], t[2], t[3]);
-                co[1] = make_float4(t[4], t[5], 0.f, 0.f);
-            }
+            if (!diag) store6_f2(A.contrib + 6ull * min(cur.y, A.cap_half - 1), t);
             double dot = 0.0;
             if (A.fp64) {
 #pragma unroll
@@ -1266,22 +1349,23 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
                 for (int i = 0; i < 6; ++i) f += vr[i] * a[i];
                 dot = (double)(diag ? f : 2.f * f);
             }
-            float4 *pp = reinterpret_cast<float4 *>(mine);   // the block is in registers now
-            pp[0] = make_float4(a[0], a[1], a[2], a[3]);
+            // the record is in registers now: its slot takes the products
+            reinterpret_cast<float4 *>(mine)[0] = make_float4(a[0], a[1], a[2], a[3]);
             reinterpret_cast<float2 *>(mine + 4)[0] = make_float2(a[4], a[5]);
             reinterpret_cast<double *>(mine + 6)[0] = dot;
         }
         __syncwarp();
-        // row segments of this chunk
-        const uint32_t next_first = __shfl_sync(0xffffffffu, next.item.z, 0);
+        // row segments of this chunk: an item ends its row when the next item starts another
+        // row or the range ends
+        const uint32_t next_first = __shfl_sync(0xffffffffu, nxt.x, 0);
+        const uint32_t word_dn = __shfl_down_sync(0xffffffffu, cur.x, 1);
+        const uint32_t following = (lane == 31) ? next_first : word_dn;
         const uint32_t row_up = __shfl_up_sync(0xffffffffu, xrow, 1);
-        const uint32_t row_dn = __shfl_down_sync(0xffffffffu, xrow, 1);
-        const uint32_t following = (lane == 31) ? next_first : row_dn;
         const bool starts = valid && (lane == 0 || row_up != xrow);
         const unsigned start_mask = __ballot_sync(0xffffffffu, starts);
         const unsigned valid_mask = __ballot_sync(0xffffffffu, valid);
         const int last = 31 - __clz(valid_mask);
-        const bool ends_row = valid && following != xrow;
+        const bool ends_row = valid && (following == kInvalidIndex || (following & kItemRowStart) != 0);
         const bool owner = valid && (ends_row || lane == last);
         float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         double dsum = 0.0;
@@ -1292,28 +1376,25 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
                 for (int i = 0; i < 6; ++i) sum[i] = carry[i];
                 dsum = carry_dot;
             }
-            const float *chunk = stage[j & 1];
+            const float *chunk = recs + bk * kPcgRecFloats;
             // sequential in item order; unrolled so that the loads of later items overlap
 #pragma unroll 4
             for (int l = first; l <= lane; ++l) {
-                const float4 a = reinterpret_cast<const float4 *>(chunk + kPcgSlot * l)[0];
-                const float2 b = reinterpret_cast<const float2 *>(chunk + kPcgSlot * l + 4)[0];
+                const float4 a = reinterpret_cast<const float4 *>(chunk + kSdStride * l)[0];
+                const float2 b = reinterpret_cast<const float2 *>(chunk + kSdStride * l + 4)[0];
                 sum[0] += a.x;
                 sum[1] += a.y;
                 sum[2] += a.z;
                 sum[3] += a.w;
                 sum[4] += b.x;
                 sum[5] += b.y;
-                dsum += reinterpret_cast<const double *>(chunk + kPcgSlot * l + 6)[0];
+                dsum += reinterpret_cast<const double *>(chunk + kSdStride * l + 6)[0];
             }
             if (ends_row) {
-                const float *dn = vring + 8 * (xrow & (kPcgRing - 1));
                 float4 *qo = reinterpret_cast<float4 *>(A.q + 8ull * xrow);
-                float4 *dno = reinterpret_cast<float4 *>(out + 16ull * xrow + 8);
                 qo[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
                 qo[1] = make_float4(sum[4], sum[5], 0.f, 0.f);
-                dno[0] = make_float4(dn[0], dn[1], dn[2], dn[3]);
-                dno[1] = make_float4(dn[4], dn[5], 0.f, 0.f);
+                store6_f2(out + (size_t)kSdStride * xrow + 6, vslot);   // d of the row
                 gring[xrow & (kPcgRing - 1)] = A.fp64 ? dsum : (double)(float)dsum;
             }
         }
@@ -1348,12 +1429,24 @@ __device__ void stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
             }
             group_end = group_first(group + 1);
         }
-        cur = next;
+        cur = nxt;
         nxt = after;
+        beta_cur = beta_next;
     }
-    // drain the last (empty) copy group before the stage buffers are reused
+    // drain the last (empty) copy group, and the phase still outstanding on each block buffer
+    // (a copy or an arrival past the range), before the buffers are reused
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+    for (int k = 0; k < 2; ++k)
+        if (!bulk_wait(bars + k, (phases >> k) & 1u)) {
+            if (lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
+            ok = false;
+        }
+    // the next range initialises the mbarriers afresh (after a timeout the launch ends instead)
+    if (ok && lane == 0)
+        for (int k = 0; k < 2; ++k)
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bars + k)) : "memory");
     __syncwarp();
+    return ok;
 }
 
 // Adds to v the contributions B^T v_i that the upper items of the rows i < row left as the
@@ -1365,20 +1458,21 @@ __device__ __forceinline__ void add_lower(const PcgArgs &A, uint32_t row, float 
     n = s0 < A.cap_half ? min(n, A.cap_half - s0) : 0u;
 #pragma unroll 4
     for (uint32_t k = 0; k < n; ++k) {
-        const float4 a = __ldcg(reinterpret_cast<const float4 *>(A.contrib + 8ull * (s0 + k)));
-        const float2 b = __ldcg(reinterpret_cast<const float2 *>(A.contrib + 8ull * (s0 + k) + 4));
+        const float2 *c = reinterpret_cast<const float2 *>(A.contrib + 6ull * (s0 + k));
+        const float2 a = __ldcg(c), b = __ldcg(c + 1), d = __ldcg(c + 2);
         v[0] += a.x;
         v[1] += a.y;
-        v[2] += a.z;
-        v[3] += a.w;
-        v[4] += b.x;
-        v[5] += b.y;
+        v[2] += b.x;
+        v[3] += b.y;
+        v[4] += d.x;
+        v[5] += d.y;
     }
 }
 
 // One step of the per-node phases: lane l takes row l % kRowsPerGroup of group
 // g + l / kRowsPerGroup (a scene's last group may have fewer rows).
 constexpr int kGroupsPerStep = 32 / kRowsPerGroup;
+constexpr int kPcgBUnitGroups = 4;   // row groups per phase-B work unit
 struct NodeStep {
     uint32_t gg, node, scene;
     bool group_ok, valid;
@@ -1400,9 +1494,9 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     float *wsm = pcg_smem + (threadIdx.x >> 5) * kPcgWarpFloats;
-    // init, phase B and the twist update work per row, so they take an equal number of groups
-    // per warp instead; every phase reads what others wrote only after a wait for all the groups
-    // of the scene, so the two partitions need not agree
+    // init and the twist update work per row, so they take an equal number of groups per warp;
+    // every phase reads what others wrote only after a wait for all the groups of the scene, so
+    // the partitions of the phases need not agree
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t b_begin = (uint32_t)((unsigned long long)A.total_groups * gwarp / nwarps);
     const uint32_t b_end = (uint32_t)((unsigned long long)A.total_groups * (gwarp + 1) / nwarps);
@@ -1418,8 +1512,8 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
             load6(A.jtr + 8ull * n.node, rv);
             matvec6(A.inv_diag + 36ull * n.node, rv, sv);
             store6(A.r + 8ull * n.node, rv);
-            store6(A.sd0 + 16ull * n.node, sv);
-            store6(A.sd0 + 16ull * n.node + 8, zero);
+            store6(A.sd0 + (size_t)kSdStride * n.node, sv);
+            store6_f2(A.sd0 + (size_t)kSdStride * n.node + 6, zero);
             store6(A.x + 8ull * n.node, zero);
         }
         const double part = node_dot_group(A, rv, sv, n.valid);
@@ -1427,10 +1521,14 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     }
     publish_range(A, b_begin, b_end, 2, 0, lane);
 
-    // the warp's next phase-A ticket (see the header comment)
-    uint32_t ticket = 0;
-    if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
+    // the warp's next phase-A and phase-B tickets (see the header comment)
+    uint32_t ticket = 0, bticket = 0;
+    if (lane == 0) {
+        ticket = atomicAdd(A.tickets, 1u);
+        bticket = atomicAdd(A.btickets, 1u);
+    }
     ticket = __shfl_sync(0xffffffffu, ticket, 0);
+    bticket = __shfl_sync(0xffffffffu, bticket, 0);
 
     for (int it = 0; it < A.pcg_iters; ++it) {
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
@@ -1446,40 +1544,50 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
                 const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
                 // the unit's scenes have finished the last iteration's phase B (init for the first)
                 if (!wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 1u, lane)) return;
-                stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane);
+                if (!stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane)) return;
                 publish_range(A, g_begin, g_end, 0, it, lane);
             }
             if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
             ticket = __shfl_sync(0xffffffffu, ticket, 0);
         }
-        if (!wait_scenes(A, b_begin, b_end, 0, (uint32_t)it + 1u, lane)) return;
-        // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
-        for (uint32_t g = b_begin; g < b_end; g += kGroupsPerStep) {
-            const NodeStep n = node_step(A, g, b_end, lane);
-            float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (n.valid) {
-                const float alpha = (float)__ldcg(A.scalars + 8ull * n.scene + 1);
-                float xv[6], dv[6], qv[6];
-                load6(A.x + 8ull * n.node, xv);
-                load6(sd_new + 16ull * n.node + 8, dv);
-                load6(A.r + 8ull * n.node, rv);
-                load6(A.q + 8ull * n.node, qv);
-                add_lower(A, n.node, qv);
+        // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s>, unit by unit ----
+        const uint32_t bfirst = (uint32_t)it * A.total_bunits;
+        while (bticket < bfirst + A.total_bunits) {
+            const uint32_t g_begin = (bticket - bfirst) * (uint32_t)kPcgBUnitGroups;
+            const uint32_t g_end = min(g_begin + (uint32_t)kPcgBUnitGroups, A.total_groups);
+            // the unit's scenes have finished phase A and published alpha
+            if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
+            for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
+                const NodeStep n = node_step(A, g, g_end, lane);
+                float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (n.valid) {
+                    const float alpha = (float)__ldcg(A.scalars + 8ull * n.scene + 1);
+                    float xv[6], dv[6], qv[6];
+                    load6(A.x + 8ull * n.node, xv);
+                    load6_f2(sd_new + (size_t)kSdStride * n.node + 6, dv);
+                    load6(A.r + 8ull * n.node, rv);
+                    load6(A.q + 8ull * n.node, qv);
+                    add_lower(A, n.node, qv);
 #pragma unroll
-                for (int i = 0; i < 6; ++i) {
-                    xv[i] += alpha * dv[i];
-                    rv[i] -= alpha * qv[i];
+                    for (int i = 0; i < 6; ++i) {
+                        xv[i] += alpha * dv[i];
+                        rv[i] -= alpha * qv[i];
+                    }
+                    matvec6(A.inv_diag + 36ull * n.node, rv, sv);
+                    store6(A.x + 8ull * n.node, xv);
+                    store6(A.r + 8ull * n.node, rv);
+                    store6(sd_new + (size_t)kSdStride * n.node, sv);
                 }
-                matvec6(A.inv_diag + 36ull * n.node, rv, sv);
-                store6(A.x + 8ull * n.node, xv);
-                store6(A.r + 8ull * n.node, rv);
-                store6(sd_new + 16ull * n.node, sv);
+                const double part = node_dot_group(A, rv, sv, n.valid);
+                if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
             }
-            const double part = node_dot_group(A, rv, sv, n.valid);
-            if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
+            publish_range(A, g_begin, g_end, 1, it + 1, lane);
+            if (lane == 0) bticket = atomicAdd(A.btickets, 1u);
+            bticket = __shfl_sync(0xffffffffu, bticket, 0);
         }
-        publish_range(A, b_begin, b_end, 1, it + 1, lane);
     }
+    // x of the warp's rows was last written by whichever warps took their phase-B units
+    if (!wait_scenes(A, b_begin, b_end, 1, (uint32_t)A.pcg_iters + 1u, lane)) return;
     // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
     //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
     for (uint32_t row = br_begin + lane; row < br_end; row += 32) {
@@ -1548,8 +1656,6 @@ constexpr int kSpmvBlocksPerSm = 3;   // kSpmvSplit x the PCG's 3 blocks per SM:
 // multiple of 4 floats, so that every warp's buffers start on the 16-byte boundary a bulk copy needs
 constexpr int kSpmvWarpFloats = kSpmvBuffers * 32 * 36 + kSpmvRing * 8 + 32 * 8 + 4 * kSpmvBuffers;
 static_assert(kSpmvWarpFloats % 4 == 0, "warp areas on 16-byte boundaries");
-// polls of an mbarrier phase before a wait gives up (each poll may suspend the thread a while)
-constexpr int kSpmvMaxPolls = 1 << 22;
 constexpr size_t kSpmvSmemBytes = sizeof(float) * (kPcgThreads / 32) * kSpmvWarpFloats;
 // Item word of the standalone SpMV: column | kItemRowStart on a row's first (diagonal) item,
 // kInvalidIndex past the end of the range.
@@ -1566,38 +1672,6 @@ __device__ __forceinline__ void spmv_load_x(const PcgArgs &A, const float *x, ui
     }
 }
 
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-// Lane 0: the blocks of items u .. u + 31 (below u_end) into `buf` by one bulk copy whose bytes
-// complete the current phase of `bar`; past the range, a plain arrival completes it.  The proxy
-// fence orders the lanes' earlier reads of `buf` (ordered before it by the caller's __syncwarp)
-// before the bulk copy's writes.  Block addresses are multiples of 144 bytes from a 256-byte
-// aligned base, so every copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
-__device__ __forceinline__ void spmv_bulk_blocks(const PcgArgs &A, uint32_t u, uint32_t u_end, float *buf,
-                                                 unsigned long long *bar) {
-    if (u >= u_end) {
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
-        return;
-    }
-    const unsigned bytes = 144u * min(32u, u_end - u);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                 ::"r"(smem_addr(buf)), "l"(A.sym_blocks + 36ull * u), "r"(bytes), "r"(smem_addr(bar)) : "memory");
-}
-// Waits for phase `parity` of `bar` to complete; false when kSpmvMaxPolls polls ran out.  The
-// warp agrees on the outcome, so a timeout leaves it converged.
-__device__ __forceinline__ bool spmv_wait(unsigned long long *bar, unsigned parity) {
-    bool ok = false;
-    for (int i = 0; i < kSpmvMaxPolls && !ok; ++i) {
-        unsigned done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
-        ok = done != 0;
-    }
-    return __all_sync(0xffffffffu, ok);
-}
 __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs A, const float *x, float *y) {
     // per warp: the chunk buffers, x of recent rows (by row), each lane's B x_col
     extern __shared__ __align__(16) float spmv_smem[];
@@ -1622,10 +1696,8 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     float2 xb;
     spmv_load_x(A, x, cur, xa, xb);
     if (lane == 0) {
-        for (int k = 0; k < kSpmvBuffers; ++k)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bars + k)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        for (int k = 0; k < kSpmvBuffers; ++k) spmv_bulk_blocks(A, u0 + 32u * k, u1, bufs + k * 32 * 36, bars + k);
+        bulk_init(bars, kSpmvBuffers);
+        for (int k = 0; k < kSpmvBuffers; ++k) bulk_blocks(A.sym_blocks, u0 + 32u * k, u1, bufs + k * 32 * 36, bars + k);
     }
     __syncwarp();
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1652,7 +1724,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         // every copy group commits in order: this chunk's is done when at most the
         // kSpmvBuffers - 1 later ones are pending
         const int bk = chunk % kSpmvBuffers;
-        if (!spmv_wait(bars + bk, (phases >> bk) & 1u)) {
+        if (!bulk_wait(bars + bk, (phases >> bk) & 1u)) {
             if (lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
             break;
         }
@@ -1663,7 +1735,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         __syncwarp();
         // the buffer is free: the blocks kSpmvBuffers chunks ahead and the next x arrive while
         // this chunk is computed
-        if (lane == 0) spmv_bulk_blocks(A, u + 32u * kSpmvBuffers, u1, buf, bars + bk);
+        if (lane == 0) bulk_blocks(A.sym_blocks, u + 32u * kSpmvBuffers, u1, buf, bars + bk);
         spmv_load_x(A, x, nxt, xa, xb);
         float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
@@ -1735,7 +1807,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     // every buffer has one phase outstanding (a copy, or an arrival past the range): wait for it,
     // so that no bulk copy still writes when the block's shared memory is released
     for (int k = 0; k < kSpmvBuffers; ++k)
-        if (!spmv_wait(bars + k, (phases >> k) & 1u) && lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
+        if (!bulk_wait(bars + k, (phases >> k) & 1u) && lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
 }
 
 // ---------------------------------------------------------------------------
@@ -2024,6 +2096,8 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.warp_groups = w.pcg_warp_groups;
     a.total_units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
     a.tickets = w.pcg_tickets;
+    a.total_bunits = (uint32_t)((w.total_chunks + kPcgBUnitGroups - 1) / kPcgBUnitGroups);
+    a.btickets = w.pcg_tickets + 1;
     a.sym_blocks = w.sym_blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
@@ -2050,7 +2124,7 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     // tickets and generations start at zero every launch, so a launch that timed out half-way
     // cannot leak into the next
     cudaMemsetAsync(w.scene_counter, 0, sizeof(uint32_t) * kSceneSync * (size_t)w.num_scenes, st);
-    cudaMemsetAsync(w.pcg_tickets, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(w.pcg_tickets, 0, 2 * sizeof(uint32_t), st);
     void *args[] = {&a};
     count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);

@@ -88,17 +88,18 @@ struct Workspace {
     uint32_t *colidx = nullptr;                              // [cap_blocks]
     // Symmetric block store: row by row, the diagonal block and then one block per upper pair
     // (row < col, column order).  These are the row's items, item_ptr[row] .. item_ptr[row + 1);
-    // pair h is item h + row + 1.  item_info holds per item (column, lower entry of the
-    // transposed use or kInvalidIndex, row, scene); lower entries are numbered by row, then
-    // column, and contrib holds one 8-float vector per lower entry for the SpMV.
+    // pair h is item h + row + 1.  item_info holds per item the column, with kItemRowStart set
+    // on a row's first (diagonal) item, and then the lower entry of the transposed use (an upper
+    // item) or the row's scene (a diagonal item); lower entries are numbered by row, then
+    // column, and contrib holds one 6-float vector per lower entry for the PCG.
     uint32_t cap_items = 0;                                  // cap_nodes + cap_half
     uint32_t *item_ptr = nullptr;                            // [cap_nodes + 1]
-    uint4 *item_info = nullptr;                              // [cap_items]
+    uint2 *item_info = nullptr;                              // [cap_items]
     // Per item, 4 bytes for the standalone SpMV: the column, with kItemRowStart set on a row's
     // first (diagonal) item; rows follow from counting those marks.
     uint32_t *item_col = nullptr;                            // [cap_items]
     float *sym_blocks = nullptr;                             // [cap_items * 36]
-    float *contrib = nullptr;                                // [cap_half * 8]
+    float *contrib = nullptr;                                // [cap_half * 6]
     uint32_t *pcg_warp_groups = nullptr;                     // [kPcgUnitsPerWarp * pcg_grid * warps per block + 1]:
                                                              // first row group of every PCG work unit
     uint32_t *pcg_tickets = nullptr;                         // [1]: PCG work-unit tickets, zeroed per launch
@@ -109,8 +110,8 @@ struct Workspace {
     float *inv_diag = nullptr;          // [cap_nodes * 36]
     double *diag64 = nullptr;           // [cap_nodes * 21] FP64 diagonal blocks (upper triangle)
     float *jtr = nullptr, *x = nullptr, *r = nullptr, *q = nullptr;
-    // PCG search vectors: per node s (6, padded to 8) then d (6, padded to 8), two copies
-    // that swap roles every iteration (the SpMV reads one while the other is written)
+    // PCG search vectors: per node s (6) then d (6), kSdStride floats, two copies that swap
+    // roles every iteration (the SpMV reads one while the other is written)
     float *sd0 = nullptr, *sd1 = nullptr;
     float *se3 = nullptr;               // [cap_nodes * 8] current warp
     float4 *centers = nullptr;          // [cap_nodes] twist centre per node (current GN iteration)
