@@ -52,7 +52,7 @@ def parse():
                    help="replicate the scene batch this many times for the >1 GB SpMV measurement; 1 skips it")
     p.add_argument("--node-growth-surfels", type=int, default=1_000_000,
                    help="surfels of the node-growth measurement (torus, R = 6 mm); 0 skips it")
-    p.add_argument("--serving-executors", type=int, default=2, help="solver workspaces of the serving run")
+    p.add_argument("--serving-executors", type=int, default=3, help="solver workspaces of the serving run")
     p.add_argument("--serving-requests", type=int, default=10000,
                    help="requests of the serving run (32 frame streams, 1k-16k nodes); 0 skips it")
     return p.parse_args()

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "../../include/warpsolve.h"
+#include "ws_workspace.h"
 
 namespace {
 
@@ -284,11 +285,24 @@ int ws_server_create(const ws_server_config *cfg, ws_server **out) {
     wc.precision = cfg->precision;
     wc.device = cfg->device;
     s->execs.resize(cfg->executors);
+    // The persistent PCG is a cooperative launch that needs all of its blocks resident, so two
+    // batches' PCGs overlap only when their grids fit on the SMs together: every executor's PCG
+    // gets an equal share of the blocks an SM holds (at least one per SM).
+    int sms = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device);
+    const int pcg_per_sm = std::max(1, ws::pcg_max_blocks(cfg->device) / std::max(1, sms) / cfg->executors);
     for (int i = 0; i < cfg->executors && st == WS_OK; ++i) {
         size_t free0 = 0, free1 = 0, total = 0;
         cudaMemGetInfo(&free0, &total);
         Executor &x = s->execs[i];
         st = ws_create(&wc, &x.solver);
+        if (st == WS_OK) {
+            ws_tuning t{};
+            t.node_threads = 128;
+            t.pair_threads = 128;
+            t.pcg_blocks_per_sm = pcg_per_sm;
+            st = ws_set_tuning(x.solver, &t);
+        }
         if (st == WS_OK && cudaStreamCreateWithFlags(&x.stream, cudaStreamNonBlocking) != cudaSuccess) st = WS_ERR_CUDA;
         if (st == WS_OK && cudaEventCreateWithFlags(&x.done, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess)
             st = WS_ERR_CUDA;

@@ -851,8 +851,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
 // the warps take by ticket: one counter grows through the launch, tickets it*U .. (it+1)*U - 1
 // are the units of iteration it, and a warp keeps the ticket that ended its iteration for the
 // next one.  So the warps that finish early take the remaining units instead of waiting for the
-// slowest, and every unit is processed once per iteration.  Phase B takes units of
-// kPcgBUnitGroups row groups the same way from a second counter.  Init and the twist update take
+// slowest, and every unit is processed once per iteration.  Phase B takes units of row groups
+// (about kPcgBUnitsPerWarp per warp) the same way from a second counter.  Init and the twist update take
 // equal numbers of groups per warp.  No block-level synchronisation.
 // Per iteration: phase A  d = s + beta d (recomputed for neighbours from s and the
 // previous d), q = A d from each stored block read once (the transposed products go
@@ -877,7 +877,8 @@ struct PcgArgs {
     const uint32_t *warp_groups;   // [units + 1] first row group of each phase-A work unit
     uint32_t total_units;          // kPcgUnitsPerWarp x the launch's warps
     uint32_t *tickets;             // phase-A work-unit tickets, growing through a launch (zeroed before it)
-    uint32_t total_bunits;         // phase-B units: kPcgBUnitGroups row groups each
+    uint32_t total_bunits;         // phase-B units: bunit_groups row groups each
+    uint32_t bunit_groups;
     uint32_t *btickets;            // phase-B unit tickets, like `tickets`
     const float *sym_blocks;       // per item: the 6x6 block, row-major
     const float *inv_diag, *jtr;
@@ -941,6 +942,12 @@ __device__ __forceinline__ void reduce_scene(const PcgArgs &A, uint32_t scene, i
     }
 }
 
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // Waits until every scene that owns one of the warp's groups has published generation
 // `target` of `which` (0: alpha, 1: delta and beta).  Lanes that start a run of a new
 // scene wait for that scene; the wait sleeps with backoff and gives up after about two
@@ -953,10 +960,10 @@ __device__ bool wait_scenes(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, 
         const uint32_t sc = g < g_end ? A.group_scene[g] : kInvalidIndex;
         const uint32_t prev = __shfl_up_sync(0xffffffffu, sc, 1);
         if (g < g_end && (lane == 0 || prev != sc)) {
-            const volatile uint32_t *gen = A.scene_counter + (size_t)kSceneSync * sc + 32 + which;
+            const uint32_t *gen = A.scene_counter + (size_t)kSceneSync * sc + 32 + which;
             unsigned long long waited_ns = 0;
             unsigned sleep_ns = 32;
-            while (*gen < target) {
+            while (ld_acquire(gen) < target) {
                 if (waited_ns > kBarrierTimeoutNs || *reinterpret_cast<volatile int *>(A.err) == WS_ERR_TIMEOUT) {
                     set_err(A.err, WS_ERR_TIMEOUT);
                     ok = false;
@@ -969,8 +976,9 @@ __device__ bool wait_scenes(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, 
         }
         __syncwarp();
     }
+    // the polling lanes' acquire loads, then this barrier, order the whole warp's later reads of
+    // the scenes' vectors and scalars after the publications they saw
     ok = __all_sync(0xffffffffu, ok);
-    __threadfence();   // reads of the scenes' vectors and scalars come after the generation
     return ok;
 }
 
@@ -1472,7 +1480,7 @@ __device__ __forceinline__ void add_lower(const PcgArgs &A, uint32_t row, float 
 // One step of the per-node phases: lane l takes row l % kRowsPerGroup of group
 // g + l / kRowsPerGroup (a scene's last group may have fewer rows).
 constexpr int kGroupsPerStep = 32 / kRowsPerGroup;
-constexpr int kPcgBUnitGroups = 4;   // row groups per phase-B work unit
+constexpr int kPcgBUnitsPerWarp = 3;   // phase-B work units per warp (each a run of row groups)
 struct NodeStep {
     uint32_t gg, node, scene;
     bool group_ok, valid;
@@ -1553,8 +1561,8 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s>, unit by unit ----
         const uint32_t bfirst = (uint32_t)it * A.total_bunits;
         while (bticket < bfirst + A.total_bunits) {
-            const uint32_t g_begin = (bticket - bfirst) * (uint32_t)kPcgBUnitGroups;
-            const uint32_t g_end = min(g_begin + (uint32_t)kPcgBUnitGroups, A.total_groups);
+            const uint32_t g_begin = (bticket - bfirst) * A.bunit_groups;
+            const uint32_t g_end = min(g_begin + A.bunit_groups, A.total_groups);
             // the unit's scenes have finished phase A and published alpha
             if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
             for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
@@ -2096,7 +2104,13 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.warp_groups = w.pcg_warp_groups;
     a.total_units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
     a.tickets = w.pcg_tickets;
-    a.total_bunits = (uint32_t)((w.total_chunks + kPcgBUnitGroups - 1) / kPcgBUnitGroups);
+    {
+        // about kPcgBUnitsPerWarp units per warp: two row groups each on the large batches, one on
+        // problems with a warp per group or so
+        const uint64_t slots = (uint64_t)kPcgBUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block();
+        a.bunit_groups = (uint32_t)std::max<uint64_t>(1, (w.total_chunks + slots - 1) / slots);
+        a.total_bunits = (uint32_t)((w.total_chunks + a.bunit_groups - 1) / a.bunit_groups);
+    }
     a.btickets = w.pcg_tickets + 1;
     a.sym_blocks = w.sym_blocks;
     a.inv_diag = w.inv_diag;

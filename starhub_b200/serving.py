@@ -322,7 +322,7 @@ def main():
     p.add_argument("--min-nodes", type=int, default=1000)
     p.add_argument("--max-nodes", type=int, default=16000)
     p.add_argument("--budget-gb", type=float, default=40.0)
-    p.add_argument("--executors", type=int, default=2)
+    p.add_argument("--executors", type=int, default=3)
     p.add_argument("--frames", type=int, default=8)
     p.add_argument("--seed", type=int, default=4)
     a = p.parse_args()
