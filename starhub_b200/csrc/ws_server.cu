@@ -1,9 +1,10 @@
 // ws_server.cu -- persistent request loop with continuous batching (host code).
 //
 // A server owns `executors` solvers, each with its own stream and completion event and a
-// host thread.  A free executor's thread takes, under the server lock, the oldest waiting
-// frames whose streams have no frame in flight and that fit the executor's capacities,
-// launches them as one batched solve (ws_set_batch + ws_solve), copies every solution back
+// host thread.  A free executor's thread takes, under the server lock, waiting frames whose
+// streams have no frame in flight and that fit the executor's capacities (longest waits
+// relative to their solve's size first, see form_batch), launches them as one batched solve
+// (ws_set_batch + ws_solve), copies every solution back
 // into its stream's resident warp on the same stream, waits for the batch (blocking event,
 // no spinning), and marks its requests done.  So a batch starts as soon as an executor is
 // free, requests that arrive while others are on the GPU join the next batch, and batches
@@ -97,29 +98,48 @@ bool has_ready(const ws_server *s) {
     return false;
 }
 
-// Oldest-first batch for one executor (the server lock is held).  The oldest ready frame
-// always fits an empty batch (checked at submit), so no frame waits behind later ones.
+// Batch for one executor (the server lock is held).  Ready frames are taken in the order of
+// their wait relative to the size of their own solve, wait / (1 + nodes / kSolveNodes): a lone
+// solve costs about a fixed latency plus a part that grows with the nodes, so a small scene's
+// frame, whose solve is short, comes before a larger one that has waited as long.  The first
+// frame sets the batch's scale: later ones join only up to kBatchSizeRatio times its nodes,
+// so a small frame does not wait for a much larger scene's solve.  The first frame always fits
+// an empty batch (checked at submit), and every frame's priority grows while it waits.
+constexpr double kSolveNodes = 12000.0;
+constexpr double kBatchSizeRatio = 2.0;
 std::vector<unsigned long long> form_batch(ws_server *s) {
     std::vector<unsigned long long> batch;
-    long long nodes = 0, pixels = 0, edges = 0;
     const ws_server_config &c = s->cfg;
-    for (auto it = s->waiting.begin(); it != s->waiting.end();) {
-        Request &r = s->requests.at(*it);
+    const Clock::time_point now = Clock::now();
+    std::vector<std::pair<double, unsigned long long>> order;
+    for (unsigned long long id : s->waiting) {
+        const Request &r = s->requests.at(id);
+        const Resident &sc = s->scenes.at(r.scene);
+        if (sc.in_flight) continue;
+        const double waited = ms_between(r.t_submit, now);
+        order.push_back({waited / (1.0 + sc.in.num_nodes / kSolveNodes), id});
+    }
+    // highest priority first; equal priorities keep the arrival order
+    std::stable_sort(order.begin(), order.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    long long nodes = 0, pixels = 0, edges = 0;
+    int head_nodes = 0;
+    for (const auto &o : order) {
+        Request &r = s->requests.at(o.second);
         Resident &sc = s->scenes.at(r.scene);
+        if (sc.in_flight) continue;   // the stream's earlier frame is already in this batch
+        if (!batch.empty() && sc.in.num_nodes > kBatchSizeRatio * head_nodes) continue;
         const long long px = (long long)sc.in.width * sc.in.height;
         const bool fits = (int)batch.size() < c.max_batch_scenes && nodes + sc.in.num_nodes <= c.max_batch_nodes &&
                           pixels + px <= c.max_batch_pixels && edges + sc.in.num_edges <= c.max_batch_edges;
-        if (sc.in_flight || !fits) {
-            ++it;
-            continue;
-        }
+        if (!fits) continue;
+        if (batch.empty()) head_nodes = sc.in.num_nodes;
         sc.in_flight = true;
         nodes += sc.in.num_nodes;
         pixels += px;
         edges += sc.in.num_edges;
-        batch.push_back(*it);
-        it = s->waiting.erase(it);
+        batch.push_back(o.second);
     }
+    for (unsigned long long id : batch) s->waiting.erase(std::find(s->waiting.begin(), s->waiting.end(), id));
     return batch;
 }
 
