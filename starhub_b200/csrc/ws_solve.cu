@@ -1120,7 +1120,8 @@ __device__ __forceinline__ void matvec6(const float *M, const float *x, float *y
 //     (cp.async.bulk, issued by lane 0, its bytes counted on the buffer's mbarrier) into one of
 //     two buffers; a buffer takes the copy of the chunk two ahead as soon as the lanes hold its
 //     blocks in registers, and the blocks of the chunk three ahead are requested into L2 by a
-//     bulk prefetch;
+//     bulk prefetch; both carry an evict-first L2 policy, so that the blocks, read once per
+//     iteration, leave L2 before the vectors and contributions the iteration reads back;
 //   * the item records (8 bytes) of chunk j + 2 are loaded while chunk j is computed, and the
 //     column s/d records (48 bytes, cp.async) of chunk j + 1;
 //   * a row's diagonal item (always its first) publishes v_i and its scene's beta through a
@@ -1151,13 +1152,21 @@ constexpr int kBulkMaxPolls = 1 << 22;
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
+// L2 policy of the block streams: each stored block is read once per product, so its lines are
+// the first to leave L2, and the vectors, item records and contributions that the same product
+// reads back stay there.
+__device__ __forceinline__ uint64_t evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(pol));
+    return pol;
+}
 // Lane 0: the blocks of items u .. u + 31 (below u_end) into `buf` by one bulk copy whose bytes
-// complete the current phase of `bar`; past the range, a plain arrival completes it.  The proxy
-// fence orders the lanes' earlier reads of `buf` (ordered before it by a __syncwarp) before the
-// bulk copy's writes.  Block addresses are multiples of 144 bytes from a 256-byte aligned base,
-// so every copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
+// complete the current phase of `bar`, with L2 policy `pol`; past the range, a plain arrival
+// completes it.  The proxy fence orders the lanes' earlier reads of `buf` (ordered before it by a
+// __syncwarp) before the bulk copy's writes.  Block addresses are multiples of 144 bytes from a
+// 256-byte aligned base, so every copy starts on a 16-byte boundary and moves a multiple of 16 bytes.
 __device__ __forceinline__ void bulk_blocks(const float *blocks, uint32_t u, uint32_t u_end, float *buf,
-                                            unsigned long long *bar) {
+                                            unsigned long long *bar, uint64_t pol) {
     if (u >= u_end) {
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
         return;
@@ -1166,9 +1175,10 @@ __device__ __forceinline__ void bulk_blocks(const float *blocks, uint32_t u, uin
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                 ::"r"(smem_addr(buf)), "l"(blocks + 36ull * u), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;\n"
+        ::"r"(smem_addr(buf)), "l"(blocks + 36ull * u), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+        : "memory");
 }
 // Lane 0: `n` mbarriers, each completed by one arrival (with its copy's bytes).
 __device__ __forceinline__ void bulk_init(unsigned long long *bars, int n) {
@@ -1192,6 +1202,7 @@ __device__ __forceinline__ bool bulk_wait(unsigned long long *bar, unsigned pari
     return __all_sync(0xffffffffu, ok);
 }
 
+
 // Item record: column | kItemRowStart on a row's diagonal item, then the lower entry of the
 // transposed use (upper item) or the row's scene (diagonal item); column kInvalidIndex past
 // the end of the range.  Loaded raw and only read one chunk later, so the load never stalls
@@ -1203,11 +1214,13 @@ __device__ __forceinline__ uint2 load_item(const uint2 *info, uint32_t u, uint32
 }
 
 // Asks L2 for the blocks of items u .. u + 31 (below u_end) ahead of their bulk copies: one
-// bulk prefetch of up to 32 contiguous 144-byte blocks, issued by one lane.
-__device__ __forceinline__ void l2_prefetch_blocks(const float *blocks, uint32_t u, uint32_t u_end) {
+// bulk prefetch of up to 32 contiguous 144-byte blocks, issued by one lane, with L2 policy `pol`.
+__device__ __forceinline__ void l2_prefetch_blocks(const float *blocks, uint32_t u, uint32_t u_end, uint64_t pol) {
     if (u < u_end) {
         const uint32_t bytes = 144u * min(32u, u_end - u);
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(blocks + 36ull * u), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;\n" ::"l"(blocks + 36ull * u),
+                     "r"(bytes), "l"(pol)
+                     : "memory");
     }
 }
 
@@ -1250,11 +1263,12 @@ __device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(gring + kPcgRing);
     const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
     const uint32_t nchunks = u1 > u0 ? (u1 - u0 + 31) / 32 : 0;
+    const uint64_t pol = evict_first_policy();
     if (lane == 0) {
         bulk_init(bars, 2);
-        bulk_blocks(A.sym_blocks, u0, u1, blocks, bars);
-        bulk_blocks(A.sym_blocks, u0 + 32, u1, blocks + kPcgBlockFloats, bars + 1);
-        l2_prefetch_blocks(A.sym_blocks, u0 + 64, u1);
+        bulk_blocks(A.sym_blocks, u0, u1, blocks, bars, pol);
+        bulk_blocks(A.sym_blocks, u0 + 32, u1, blocks + kPcgBlockFloats, bars + 1, pol);
+        l2_prefetch_blocks(A.sym_blocks, u0 + 64, u1, pol);
     }
     __syncwarp();
     unsigned phases = 0;   // bit k: parity of the next completion of buffer k's mbarrier
@@ -1283,7 +1297,7 @@ __device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
         // column records of chunk j + 1 in flight, item records of chunk j + 2 requested
         float beta_next;
         issue_records(A, vec_in, nxt, recs + (bk ^ 1) * kPcgRecFloats, lane, beta_next);
-        if (lane == 0) l2_prefetch_blocks(A.sym_blocks, u0 + 32 * (j + 3), u1);
+        if (lane == 0) l2_prefetch_blocks(A.sym_blocks, u0 + 32 * (j + 3), u1, pol);
         const uint2 after = load_item(A.item_info, u0 + 32 * (j + 2) + lane, u1);
         if (!bulk_wait(bars + bk, (phases >> bk) & 1u)) {
             if (lane == 0) set_err(A.err, WS_ERR_TIMEOUT);
@@ -1331,7 +1345,7 @@ __device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
         }
         __syncwarp();
         // the buffer is free: it takes the blocks of the chunk two ahead
-        if (lane == 0) bulk_blocks(A.sym_blocks, u0 + 32 * (j + 2), u1, blocks + bk * kPcgBlockFloats, bars + bk);
+        if (lane == 0) bulk_blocks(A.sym_blocks, u0 + 32 * (j + 2), u1, blocks + bk * kPcgBlockFloats, bars + bk, pol);
         if (valid) {
             // B v_col and B^T v_row from one pass over the block
             float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1649,7 +1663,8 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
 // x and y once each: no contribution buffer and no second pass.  Sums meet in no fixed order.
 // The kernel streams a warp's contiguous blocks through kSpmvBuffers shared-memory buffers of
 // 4.6 KB: a chunk's 32 blocks (4608 contiguous bytes) arrive as one 1-D bulk copy
-// (cp.async.bulk, issued by lane 0, its bytes counted on the buffer's mbarrier), each lane moves
+// (cp.async.bulk, issued by lane 0, its bytes counted on the buffer's mbarrier, with an
+// evict-first L2 policy that keeps x and y in L2), each lane moves
 // its item's block into registers, and the buffer at once takes the bulk copy of the chunk
 // kSpmvBuffers ahead, which overlaps the arithmetic of the chunks between.  x of the items'
 // columns is loaded a chunk ahead into registers, the items' 4-byte column words (item_col: the
@@ -1689,6 +1704,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     float *prod = ring + kSpmvRing * 8;
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(prod + 32 * 8);   // 16-byte aligned
     unsigned phases = 0;   // bit k: parity of the next completion of buffer k
+    const uint64_t pol = evict_first_policy();
     const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t pv = v / kSpmvSplit, part = v % kSpmvSplit;
     const uint32_t pg0 = min(A.warp_groups[kPcgUnitsPerWarp * pv], A.total_groups);
@@ -1705,7 +1721,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
     spmv_load_x(A, x, cur, xa, xb);
     if (lane == 0) {
         bulk_init(bars, kSpmvBuffers);
-        for (int k = 0; k < kSpmvBuffers; ++k) bulk_blocks(A.sym_blocks, u0 + 32u * k, u1, bufs + k * 32 * 36, bars + k);
+        for (int k = 0; k < kSpmvBuffers; ++k) bulk_blocks(A.sym_blocks, u0 + 32u * k, u1, bufs + k * 32 * 36, bars + k, pol);
     }
     __syncwarp();
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1743,7 +1759,7 @@ __global__ void __launch_bounds__(kPcgThreads, kSpmvBlocksPerSm) k_spmv(PcgArgs 
         __syncwarp();
         // the buffer is free: the blocks kSpmvBuffers chunks ahead and the next x arrive while
         // this chunk is computed
-        if (lane == 0) bulk_blocks(A.sym_blocks, u + 32u * kSpmvBuffers, u1, buf, bars + bk);
+        if (lane == 0) bulk_blocks(A.sym_blocks, u + 32u * kSpmvBuffers, u1, buf, bars + bk, pol);
         spmv_load_x(A, x, nxt, xa, xb);
         float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
