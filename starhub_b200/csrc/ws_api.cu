@@ -32,8 +32,8 @@ void free_all(ws::Workspace &w) {
     void *ptrs[] = {w.scenes, w.plan, w.counts, w.tile_scene, w.tile_count, w.node_scene, w.edge_scene,
                     w.chunk_scene, w.chunk_row, w.scan_tmp, w.sort_hist, w.sort_digit, w.d_pixels, w.d_knn,
                     w.d_sw, w.d_cw, w.d_scene, w.d_record, w.r_record, w.n2t_key, w.n2t_val, w.n2t_key_alt,
-                    w.n2t_val_alt, w.n2t_offset, w.pair_key, w.pair_key_alt, w.pair_val, w.pair_val_alt,
-                    w.pair_head, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
+                    w.n2t_val_alt, w.n2t_offset, w.row_pair_cols, w.row_pair_cnts, w.row_pair_first,
+                    w.row_entry_first, w.pair_val, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
                     w.col_key_alt, w.col_val_alt, w.colidx, w.item_ptr, w.item_info, w.item_col, w.sym_blocks, w.contrib, w.pcg_warp_groups, w.pcg_tickets, w.mf_ux, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
                     w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter,
@@ -137,8 +137,8 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     w.cap_half = std::min<uint32_t>(w.cap_half, (0xFFFFFFF0u - w.cap_nodes) / 2u);
     w.cap_blocks = w.cap_nodes + 2u * w.cap_half;
     w.cap_items = w.cap_nodes + w.cap_half;
-    const uint32_t sort_cap = std::max(std::max(w.cap_n2t, w.cap_pair_kv), w.cap_half);
-    const uint32_t scan_cap = std::max(std::max(w.cap_pair_kv, w.cap_nodes), w.cap_tiles) + 1;
+    const uint32_t sort_cap = std::max(w.cap_n2t, w.cap_half);
+    const uint32_t scan_cap = std::max(w.cap_nodes, w.cap_tiles) + 1;
     cudaError_t e = cudaSuccess;
     auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
     A(dalloc(&w.scenes, w.cap_scenes));
@@ -165,11 +165,11 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.n2t_key_alt, w.cap_n2t));
     A(dalloc(&w.n2t_val_alt, w.cap_n2t));
     A(dalloc(&w.n2t_offset, w.cap_nodes + 1));
-    A(dalloc(&w.pair_key, w.cap_pair_kv));
-    A(dalloc(&w.pair_key_alt, w.cap_pair_kv));
+    A(dalloc(&w.row_pair_cols, (size_t)w.cap_nodes * ws::kRowPairsMax));
+    A(dalloc(&w.row_pair_cnts, (size_t)w.cap_nodes * ws::kRowPairsMax));
+    A(dalloc(&w.row_pair_first, w.cap_nodes + 1));
+    A(dalloc(&w.row_entry_first, w.cap_nodes + 1));
     A(dalloc(&w.pair_val, w.cap_pair_kv));
-    A(dalloc(&w.pair_val_alt, w.cap_pair_kv));
-    A(dalloc(&w.pair_head, w.cap_pair_kv + 1));
     A(dalloc(&w.half_row, w.cap_half));
     A(dalloc(&w.half_col, w.cap_half));
     A(dalloc(&w.half_begin, w.cap_half));
@@ -334,13 +334,6 @@ int ws_set_batch(ws_solver *h, const ws_inputs *scenes, int num_scenes) {
     w.total_tiles = tb;
     w.total_chunks = cb;
     w.node_bits = ws::bits_for(nb);
-    {
-        int max_nodes = 1;
-        for (int s = 0; s < num_scenes; ++s) max_nodes = std::max(max_nodes, hs[s].num_nodes);
-        const int lb = ws::bits_for((uint64_t)max_nodes - 1u), sb = ws::bits_for((uint64_t)num_scenes - 1u);
-        w.pair_local_bits = (sb + 2 * lb <= 32) ? lb : 0;
-        w.pair_key_bits = (sb + 2 * lb <= 32) ? sb + 2 * lb : 0;
-    }
     w.have_inputs = true;
     w.have_solution = false;
     return WS_OK;
@@ -450,7 +443,7 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
     w.last_stream = st;
     const uint64_t key[] = {(uint64_t)gn_iters, (uint64_t)pcg_iters, (uint64_t)w.num_scenes, w.total_nodes,
                             w.total_edges, w.total_tiles, w.total_chunks, (uint64_t)w.node_bits,
-                            (uint64_t)w.dense_channels, (uint64_t)w.pair_local_bits, (uint64_t)w.pair_key_bits};
+                            (uint64_t)w.dense_channels};
     constexpr size_t kKey = sizeof(key) / sizeof(key[0]);
     bool same = w.graph_exec && w.graph_key.size() == kKey && std::equal(key, key + kKey, w.graph_key.begin());
     if (same) {

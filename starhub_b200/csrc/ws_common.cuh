@@ -17,6 +17,7 @@ namespace ws {
 
 constexpr int kVecStride = 8;        // floats per node in PCG vectors
 constexpr int kSdStride = 12;        // floats per node in the PCG's s/d records
+constexpr int kRowPairsMax = 64;     // upper node pairs of one row in the pair map (WS_ERR_CAPACITY beyond)
 constexpr int kDenseRecord = 32;     // floats per dense-term record, largest layout (128 B)
 constexpr int kRegRecord = 16;       // floats per reg-term record (64 B)
 constexpr uint32_t kInvalidIndex = 0xFFFFFFFFu;

@@ -220,152 +220,242 @@ __global__ void k_n2t_offsets(const uint32_t *sorted_keys, const uint32_t *count
     }
 }
 
-// Node-pair sort keys.  Wide form (64-bit): (global row << bits) | global col.  Narrow form
-// (32-bit), used when the scene id and two scene-local ids fit in 32 bits: (scene << 2 bits) |
-// (local row << bits) | local col.  The scenes of a batch hold consecutive global ids, so both
-// forms order the pairs by (global row, global column); the narrow one halves the key bytes
-// and saves radix passes.  A pair's row id is below its column id, so a valid key is never
-// all ones, which marks an unused entry.
-template <class K>
-struct PairKey {
-    int bits;    // global node bits (wide) or scene-local node bits (narrow)
-    K invalid;
-    __device__ __forceinline__ K make(uint32_t scene, uint32_t node_base, uint32_t lo, uint32_t hi) const {
-        if constexpr (sizeof(K) == 8)
-            return ((K)(node_base + lo) << bits) | (K)(node_base + hi);
-        else
-            return ((K)scene << (2 * bits)) | ((K)lo << bits) | (K)hi;
-    }
-    __device__ __forceinline__ void split(K k, const Scene *scenes, uint32_t &row, uint32_t &col) const {
-        const K mask = ((K)1 << bits) - (K)1;
-        if constexpr (sizeof(K) == 8) {
-            row = (uint32_t)(k >> bits);
-            col = (uint32_t)(k & mask);
-        } else {
-            const uint32_t nb = (uint32_t)scenes[k >> (2 * bits)].node_base;
-            row = nb + (uint32_t)((k >> bits) & mask);
-            col = nb + (uint32_t)(k & mask);
-        }
-    }
-};
+// ---------------------------------------------------------------------------
+// Node pair -> term map (computeKVNodePairKNN + sort + segmentNodePairKernel +
+// compactNodePairKeyKernel, NodePair2TermsIndex.cu:11-169), built row by row from the sorted
+// node -> term map instead of by sorting one key per (pair, term).
+// The reference's sorted list holds, for a pair i < j, one entry of term t for every way t
+// touches both nodes: for a dense or feature term, each knn slot holding i times each slot holding
+// j (slot pairs with id_a < id_b); for a non-self edge (i, j) or (j, i), one entry; in term order.
+// Row i's node -> term list holds t once per slot of i, in term order, so emitting, for each entry
+// of the list, the term's nodes above i (every knn slot above i; the other end of an edge) yields
+// exactly row i's entries, each pair's in term order.  The pairs are sorted by (row, column), so
+// row i's pairs and entries are one contiguous range after those of the rows before it.
+// Pass 1 (one warp per row) counts each column's entries in a small hash table in shared memory
+// and keeps the row's columns sorted; two scans give every row its first pair and first entry;
+// pass 2 writes the pairs and places every entry at its pair's next free position.
+// ---------------------------------------------------------------------------
+constexpr int kRowHash = 128;        // hash slots per warp (twice kRowPairsMax)
+constexpr int kRowWarps = 4;         // warps per block of the two row passes
+constexpr int kRowLanesEntries = 4;  // list entries per lane and pass (loads in flight)
+constexpr int kRowChunk = 32 * kRowLanesEntries;   // list entries per pass
+constexpr int kRowStage = 3 * kRowChunk;           // their candidates (at most 3 each)
+constexpr uint32_t kNoCol = 0xFFFFFFFFu;
 
-// computeKVNodePairKNN / buildKeyValuePairKernel (NodePair2TermsIndex.cu:11-92): 6 (i<j) pairs per
-// dense term in i-major order, one per non-self reg edge, feature terms like dense terms.
-template <class K>
-__device__ __forceinline__ K knn_pair_key(const ushort4 k4, uint32_t q, uint32_t scene, uint32_t base,
-                                          const PairKey<K> &pk) {
-    const uint16_t a[4] = {k4.x, k4.y, k4.z, k4.w};
-    uint32_t off = 0;
+// The columns above `row` that list entry `t` (scene-local term id) adds to row `row`'s pairs, in
+// c[0..2] (kNoCol where none); returns their number (at most 3).
+__device__ __forceinline__ int row_pair_columns(const Scene &sc, const Plan &p, const ushort4 *dense_knn,
+                                                uint32_t row, uint32_t t, uint32_t (&c)[3], int *err) {
+    const uint32_t nb = (uint32_t)sc.node_base, nd = p.dense_count, ne = (uint32_t)sc.num_edges,
+                   nn = (uint32_t)sc.num_nodes;
+    c[0] = c[1] = c[2] = kNoCol;
+    int n = 0;
+    auto push = [&](uint32_t v) {
+        c[0] = n == 0 ? v : c[0];
+        c[1] = n == 1 ? v : c[1];
+        c[2] = n == 2 ? v : c[2];
+        n = min(n + 1, 3);
+    };
+    if (t < nd || t >= nd + ne + nn) {   // dense or feature term: its knn slots above the row
+        const ushort4 k4 = t < nd ? dense_knn[p.dense_begin + t] : clamp_knn(sc.feature_knn[t - nd - ne - nn], sc, err);
+        if (nb + k4.x > row) push(nb + k4.x);
+        if (nb + k4.y > row) push(nb + k4.y);
+        if (nb + k4.z > row) push(nb + k4.z);
+        if (nb + k4.w > row) push(nb + k4.w);
+    } else if (t < nd + ne) {            // edge: its other end
+        uint16_t x, y;
+        edge_ends(sc, t - nd, x, y, err);
+        const uint32_t other = (nb + x == row) ? nb + y : nb + x;
+        if (x != y && other > row) push(other);
+    }
+    return n;
+}
+
+// Row `row`'s candidate columns of list entries base .. base + kRowChunk - 1 (below end), staged
+// in list order as (column, term); returns their number.  Lane l reads entries base + 32 q + l, so
+// every load instruction is coalesced and a lane has kRowLanesEntries gathers in flight.
+__device__ __forceinline__ uint32_t stage_row_candidates(const Scene &sc, const Plan &p, const ushort4 *dense_knn,
+                                                         const uint32_t *n2t_val, uint32_t row, uint32_t base,
+                                                         uint32_t end, uint32_t *st_col, uint32_t *st_term, int lane,
+                                                         int *err) {
+    uint32_t t[kRowLanesEntries];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int q = 0; q < kRowLanesEntries; ++q) {
+        const uint32_t e = base + 32u * q + (uint32_t)lane;
+        t[q] = e < end ? n2t_val[e] : kNoCol;
+    }
+    uint32_t carry = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (a[i] < a[j]) {
-                if (off == q) return pk.make(scene, base, a[i], a[j]);
-                ++off;
+    for (int q = 0; q < kRowLanesEntries; ++q) {
+        uint32_t col[3] = {kNoCol, kNoCol, kNoCol};
+        const int n = t[q] != kNoCol ? row_pair_columns(sc, p, dense_knn, row, t[q], col, err) : 0;
+        const uint32_t incl = warp_incl_scan_u32((uint32_t)n);
+        const uint32_t off = carry + incl - (uint32_t)n;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k < n) {
+                st_col[off + k] = col[k];
+                st_term[off + k] = t[q];
             }
-    return pk.invalid;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+    return carry;
 }
 
-// Pair keys and values.  Per scene the entries sit at plan.pair_base as [6 per dense term |
-// 1 per edge | 6 per feature].  The 6 keys of one dense term follow knn_pair_key: slot pairs
-// (i, j) with id_i < id_j, i then j ascending; fewer than 6 when ids repeat, the rest invalid.
-template <class K>
-__global__ void k_pair_kv_dense(const Scene *scenes, const Plan *plan, const uint32_t *counts,
-                                const uint32_t *term_scene, const ushort4 *dense_knn, K *keys, uint32_t *vals,
-                                PairKey<K> pk) {
-    const uint32_t n = counts[kCntDense];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const uint32_t s = term_scene[t];
+__device__ __forceinline__ uint32_t col_hash(uint32_t c) { return (c * 2654435761u) >> (32 - 7); }
+
+__global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_count(
+    const Scene *scenes, const Plan *plan, const uint32_t *node_scene, uint32_t total_nodes,
+    const uint32_t *n2t_offset, const uint32_t *n2t_val, const ushort4 *dense_knn, uint32_t *row_cols,
+    uint32_t *row_cnts, uint32_t *row_pairs, uint32_t *row_entries, int *err) {
+    static_assert(kRowHash == 128, "col_hash gives 7 bits");
+    __shared__ uint32_t hkey[kRowWarps][kRowHash], hcnt[kRowWarps][kRowHash];
+    __shared__ uint32_t lcol[kRowWarps][kRowHash], lcnt[kRowWarps][kRowHash];
+    __shared__ uint32_t st_col[kRowWarps][kRowStage], st_term[kRowWarps][kRowStage];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t *keys = hkey[wib], *cnts = hcnt[wib];
+    const unsigned lower = (1u << lane) - 1u;
+    const uint32_t warps = gridDim.x * kRowWarps;
+    for (uint32_t row = blockIdx.x * kRowWarps + wib; row < total_nodes; row += warps) {
+        for (int k = lane; k < kRowHash; k += 32) {
+            keys[k] = kNoCol;
+            cnts[k] = 0;
+        }
+        __syncwarp();
+        const uint32_t s = node_scene[row];
+        const Scene &sc = scenes[s];
         const Plan &p = plan[s];
-        const uint32_t lt = t - p.dense_begin, base = p.pair_base + 6u * lt, nb = scenes[s].node_base;
-        const ushort4 k4 = dense_knn[t];
-        const uint16_t a[4] = {k4.x, k4.y, k4.z, k4.w};
-        K out[6] = {pk.invalid, pk.invalid, pk.invalid, pk.invalid, pk.invalid, pk.invalid};
-        int q = 0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (a[i] < a[j] && q < 6) out[q++] = pk.make(s, nb, a[i], a[j]);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            keys[base + k] = out[k];
-            vals[base + k] = lt;
+        const uint32_t beg = n2t_offset[row], end = n2t_offset[row + 1];
+        bool full = false;
+        for (uint32_t base = beg; base < end; base += kRowChunk) {
+            const uint32_t total =
+                stage_row_candidates(sc, p, dense_knn, n2t_val, row, base, end, st_col[wib], st_term[wib], lane, err);
+            for (uint32_t v0 = 0; v0 < total; v0 += 32) {
+                const uint32_t v = v0 + (uint32_t)lane;
+                const uint32_t c = v < total ? st_col[wib][v] : kNoCol;
+                const unsigned peers = __match_any_sync(0xffffffffu, c);
+                if (c != kNoCol && (peers & lower) == 0) {   // one insertion per column and pass
+                    uint32_t slot = col_hash(c);
+                    bool placed = false;
+                    for (int probe = 0; probe < kRowHash && !placed; ++probe) {
+                        const uint32_t prev = atomicCAS(&keys[slot], kNoCol, c);
+                        if (prev == kNoCol || prev == c) {
+                            atomicAdd(&cnts[slot], (uint32_t)__popc(peers));
+                            placed = true;
+                        }
+                        slot = (slot + 1) & (kRowHash - 1);
+                    }
+                    if (!placed) full = true;
+                }
+            }
+            __syncwarp();
         }
-    }
-}
-
-template <class K>
-__global__ void k_pair_kv_tail(const Scene *scenes, const Plan *plan, K *keys, uint32_t *vals, PairKey<K> pk,
-                               int *err) {
-    const Scene &sc = scenes[blockIdx.y];
-    const Plan &p = plan[blockIdx.y];
-    const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes, nf = sc.num_features;
-    const uint32_t len = ne + 6u * nf, base = p.pair_base + 6u * nd;
-    for (uint32_t j0 = blockIdx.x * blockDim.x + threadIdx.x; j0 < len; j0 += gridDim.x * blockDim.x) {
-        uint32_t j = j0;
-        K key;
-        uint32_t val;
-        if (j < ne) {
-            uint16_t x, y;
-            edge_ends(sc, j, x, y, err);
-            const uint32_t lo = min(x, y), hi = max(x, y);
-            key = (x != y) ? pk.make(blockIdx.y, sc.node_base, lo, hi) : pk.invalid;
-            val = nd + j;
-        } else {
-            j -= ne;
-            const uint32_t f = j / 6u;
-            key = knn_pair_key<K>(clamp_knn(sc.feature_knn[f], sc, err), j - 6u * f, blockIdx.y, sc.node_base, pk);
-            val = nd + ne + nn + f;
+        // the table's columns, compacted in slot order, then ranked by column
+        uint32_t n_cols = 0;
+        for (int q = 0; q < kRowHash / 32; ++q) {
+            const uint32_t c = keys[32 * q + lane];
+            const unsigned occ = __ballot_sync(0xffffffffu, c != kNoCol);
+            if (c != kNoCol) {
+                const uint32_t idx = n_cols + (uint32_t)__popc(occ & lower);
+                lcol[wib][idx] = c;
+                lcnt[wib][idx] = cnts[32 * q + lane];
+            }
+            n_cols += (uint32_t)__popc(occ);
         }
-        keys[base + j0] = key;
-        vals[base + j0] = val;
+        __syncwarp();
+        full = __any_sync(0xffffffffu, full) || n_cols > (uint32_t)kRowPairsMax;
+        if (full) {
+            if (lane == 0) set_error(err, WS_ERR_CAPACITY);
+            n_cols = 0;
+        }
+        uint32_t entries = 0;
+        for (uint32_t x = (uint32_t)lane; x < n_cols; x += 32) {
+            const uint32_t c = lcol[wib][x];
+            uint32_t rank = 0;
+            for (uint32_t y = 0; y < n_cols; ++y) rank += lcol[wib][y] < c ? 1u : 0u;
+            row_cols[(size_t)kRowPairsMax * row + rank] = c;
+            row_cnts[(size_t)kRowPairsMax * row + rank] = lcnt[wib][x];
+            entries += lcnt[wib][x];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) entries += __shfl_xor_sync(0xffffffffu, entries, o);
+        if (lane == 0) {
+            row_pairs[row] = n_cols;
+            row_entries[row] = full ? 0u : entries;
+        }
+        __syncwarp();
     }
 }
 
-
-// segmentNodePairKernel (NodePair2TermsIndex.cu:94-128): 1 at the first key of every unique pair;
-// also records the number of valid (non-invalid) keys.
-template <class K>
-__global__ void k_pair_marks(const K *keys, const uint32_t *counts, uint32_t *marks, K invalid, uint32_t *counts_out) {
-    const uint32_t n = counts[kCntPairKV];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const K k = keys[i];
-        const bool valid = k != invalid;
-        marks[i] = (valid && (i == 0 || keys[i - 1] != k)) ? 1u : 0u;
-        if (valid && (i + 1 == n || keys[i + 1] == invalid)) counts_out[kCntPairValid] = i + 1;
-        if (i == 0 && !valid) counts_out[kCntPairValid] = 0;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && n == 0) counts_out[kCntPairValid] = 0;
-}
-
-// compactNodePairKeyKernel (NodePair2TermsIndex.cu:130-169): unique pairs and their term ranges.
-template <class K>
-__global__ void k_half_fill(const K *keys, const uint32_t *head_off, const Scene *scenes, uint32_t *counts,
-                            PairKey<K> pk, uint32_t cap_half, uint32_t *half_row, uint32_t *half_col,
-                            uint32_t *half_begin, uint32_t *half_end, uint32_t *row_cnt_up, uint32_t *row_cnt_lo,
-                            int *err) {
-    const uint32_t n = counts[kCntPairKV];
-    const uint32_t nhalf = head_off[n];
-    const uint32_t nvalid = counts[kCntPairValid];
+__global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_fill(
+    const Scene *scenes, const Plan *plan, const uint32_t *node_scene, uint32_t total_nodes,
+    const uint32_t *n2t_offset, const uint32_t *n2t_val, const ushort4 *dense_knn, const uint32_t *row_cols,
+    const uint32_t *row_cnts, const uint32_t *pair_first, const uint32_t *entry_first, uint32_t cap_half,
+    uint32_t cap_kv, uint32_t *half_row, uint32_t *half_col, uint32_t *half_begin, uint32_t *half_end,
+    uint32_t *row_cnt_lo, uint32_t *pair_val, uint32_t *counts, int *err) {
+    __shared__ uint32_t s_col[kRowWarps][kRowPairsMax], s_next[kRowWarps][kRowPairsMax];
+    __shared__ uint32_t st_col[kRowWarps][kRowStage], st_term[kRowWarps][kRowStage];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lower = (1u << lane) - 1u;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        counts[kCntHalf] = min(nhalf, cap_half);
-        if (nhalf > cap_half) set_error(err, WS_ERR_CAPACITY);
+        counts[kCntHalf] = min(pair_first[total_nodes], cap_half);
+        if (pair_first[total_nodes] > cap_half) set_error(err, WS_ERR_CAPACITY);
     }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t h = head_off[i];
-        if (head_off[i + 1] == h) continue;        // not the first key of a unique pair
-        if (h >= cap_half) continue;
-        uint32_t row, col;
-        pk.split(keys[i], scenes, row, col);
-        half_row[h] = row;
-        half_col[h] = col;
-        half_begin[h] = i;
-        if (h > 0 && h - 1 < cap_half) half_end[h - 1] = i;
-        if (h + 1 == nhalf) half_end[h] = nvalid;
-        atomicAdd(&row_cnt_up[row], 1u);
-        atomicAdd(&row_cnt_lo[col], 1u);
+    const uint32_t warps = gridDim.x * kRowWarps;
+    for (uint32_t row = blockIdx.x * kRowWarps + wib; row < total_nodes; row += warps) {
+        const uint32_t h0 = pair_first[row], n_cols = pair_first[row + 1] - h0;
+        // the row's pairs: columns ascending, entry ranges one after another from the row's first
+        uint32_t carry = entry_first[row];
+        for (uint32_t k0 = 0; k0 < n_cols; k0 += 32) {
+            const uint32_t k = k0 + (uint32_t)lane;
+            const uint32_t c = k < n_cols ? row_cols[(size_t)kRowPairsMax * row + k] : kNoCol;
+            const uint32_t n = k < n_cols ? row_cnts[(size_t)kRowPairsMax * row + k] : 0u;
+            const uint32_t incl = warp_incl_scan_u32(n);
+            const uint32_t begin = carry + incl - n;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+            if (k < n_cols) {
+                s_col[wib][k] = c;
+                s_next[wib][k] = begin;
+                const uint32_t h = h0 + k;
+                if (h < cap_half) {
+                    half_row[h] = row;
+                    half_col[h] = c;
+                    half_begin[h] = begin;
+                    half_end[h] = begin + n;
+                    atomicAdd(&row_cnt_lo[c], 1u);
+                }
+            }
+        }
+        __syncwarp();
+        if (n_cols == 0) continue;
+        const uint32_t s = node_scene[row];
+        const Scene &sc = scenes[s];
+        const Plan &p = plan[s];
+        const uint32_t beg = n2t_offset[row], end = n2t_offset[row + 1];
+        for (uint32_t base = beg; base < end; base += kRowChunk) {
+            const uint32_t total =
+                stage_row_candidates(sc, p, dense_knn, n2t_val, row, base, end, st_col[wib], st_term[wib], lane, err);
+            for (uint32_t v0 = 0; v0 < total; v0 += 32) {
+                const uint32_t v = v0 + (uint32_t)lane;
+                const uint32_t c = v < total ? st_col[wib][v] : kNoCol;
+                const unsigned peers = __match_any_sync(0xffffffffu, c);
+                uint32_t k = 0;
+                if (c != kNoCol) {   // the column's place among the row's (binary search)
+                    uint32_t lo = 0, hi = n_cols;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (s_col[wib][mid] < c) lo = mid + 1; else hi = mid;
+                    }
+                    k = lo;
+                    const uint32_t pos = s_next[wib][min(k, n_cols - 1)] + (uint32_t)__popc(peers & lower);
+                    if (k < n_cols && s_col[wib][k] == c && pos < cap_kv) pair_val[pos] = st_term[wib][v];
+                }
+                __syncwarp();
+                if (c != kNoCol && (peers & lower) == 0 && k < n_cols) s_next[wib][k] += (uint32_t)__popc(peers);
+                __syncwarp();
+            }
+        }
     }
 }
 
@@ -472,30 +562,23 @@ static inline int grid_for(uint32_t n, int threads, int num_sms) {
     return (int)std::max<uint32_t>(1u, std::min<uint32_t>(want, cap));
 }
 
-// Pair keys and values, their stable sort, and the unique pairs with their term ranges.
-template <class K>
-static void pair_index(Workspace &w, PairKey<K> pk, int key_bits, cudaStream_t st) {
-    const int S = w.num_scenes;
-    K *keys = reinterpret_cast<K *>(w.pair_key), *keys_alt = reinterpret_cast<K *>(w.pair_key_alt);
-    k_pair_kv_dense<K><<<grid_for(w.cap_pixels, 256, w.num_sms), 256, 0, st>>>(w.scenes, w.plan, w.counts, w.d_scene,
-                                                                                w.d_knn, keys, w.pair_val, pk);
-    k_pair_kv_tail<K><<<dim3(16, S), 256, 0, st>>>(w.scenes, w.plan, keys, w.pair_val, pk, w.error_flag);
-    count_launch(w);
-    const bool pair_alt = radix_sort<K>(keys, w.pair_val, keys_alt, w.pair_val_alt, w.counts + kCntPairKV, 0,
-                                        w.cap_pair_kv, key_bits, w.sort_hist, w.sort_digit, st);
-    count_launch(w, 1 + 3 * ((key_bits + 7) / 8));
-    const K *sorted = pair_alt ? keys_alt : keys;
-    w.pair_sorted_val = pair_alt ? w.pair_val_alt : w.pair_val;
-    const int pg = grid_for(w.cap_pair_kv, 256, w.num_sms);
-    k_pair_marks<K><<<pg, 256, 0, st>>>(sorted, w.counts, w.pair_head, pk.invalid, w.counts);
-    exclusive_scan(w.pair_head, w.pair_head, w.counts + kCntPairKV, 0, w.cap_pair_kv, w.scan_tmp, st);
-    // pair_head now holds exclusive offsets; a unique pair starts where two consecutive offsets differ
-    cudaMemsetAsync(w.row_cnt_up, 0, sizeof(uint32_t) * w.cap_nodes, st);
+// Node pair -> term map, row by row from the node -> term map (see k_pair_rows_count).
+static void pair_index(Workspace &w, cudaStream_t st) {
+    const uint32_t N = w.total_nodes;
+    const int grid = grid_for(N * 32u, 32 * kRowWarps, w.num_sms);
+    k_pair_rows_count<<<grid, 32 * kRowWarps, 0, st>>>(w.scenes, w.plan, w.node_scene, N, w.n2t_offset,
+                                                      w.n2t_sorted_val, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
+                                                      w.row_cnt_up, w.row_entry_first, w.error_flag);
+    exclusive_scan(w.row_cnt_up, w.row_pair_first, nullptr, N, w.cap_nodes, w.scan_tmp, st);
+    exclusive_scan(w.row_entry_first, w.row_entry_first, nullptr, N, w.cap_nodes, w.scan_tmp, st);
     cudaMemsetAsync(w.row_cnt_lo, 0, sizeof(uint32_t) * w.cap_nodes, st);
-    k_half_fill<K><<<pg, 256, 0, st>>>(sorted, w.pair_head, w.scenes, w.counts, pk, w.cap_half, w.half_row,
-                                       w.half_col, w.half_begin, w.half_end, w.row_cnt_up, w.row_cnt_lo,
-                                       w.error_flag);
-    count_launch(w, 1 + 3 + 1);
+    k_pair_rows_fill<<<grid, 32 * kRowWarps, 0, st>>>(w.scenes, w.plan, w.node_scene, N, w.n2t_offset,
+                                                     w.n2t_sorted_val, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
+                                                     w.row_pair_first, w.row_entry_first, w.cap_half, w.cap_pair_kv,
+                                                     w.half_row, w.half_col, w.half_begin, w.half_end, w.row_cnt_lo,
+                                                     w.pair_val, w.counts, w.error_flag);
+    w.pair_sorted_val = w.pair_val;
+    count_launch(w, 1 + 3 + 3 + 1);
 }
 
 void index_build(Workspace &w, cudaStream_t st) {
@@ -524,15 +607,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     k_n2t_offsets<<<grid_for(N + 1, 256, w.num_sms), 256, 0, st>>>(w.n2t_sorted_key, w.counts, N, w.n2t_offset);
     count_launch(w);
     // 3. node pair -> term
-    if (w.pair_local_bits > 0) {
-        const int kb = w.pair_key_bits;
-        const uint32_t inv = kb >= 32 ? 0xFFFFFFFFu : ((1u << kb) - 1u);
-        pair_index<uint32_t>(w, PairKey<uint32_t>{w.pair_local_bits, inv}, kb, st);
-    } else {
-        const int kb = 2 * w.node_bits;
-        const unsigned long long inv = kb >= 64 ? ~0ull : ((1ull << kb) - 1ull);
-        pair_index<unsigned long long>(w, PairKey<unsigned long long>{w.node_bits, inv}, kb, st);
-    }
+    pair_index(w, st);
     // 4. block CSR
     k_row_first<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_row, w.counts, w.row_first);
     k_row_len<<<grid_for(N, 256, w.num_sms), 256, 0, st>>>(w.row_cnt_up, w.row_cnt_lo, N, w.rowptr, w.item_ptr);

@@ -34,9 +34,6 @@ struct Workspace {
     int num_scenes = 0;
     uint32_t total_nodes = 0, total_edges = 0, total_tiles = 0, total_chunks = 0, total_features = 0;
     int node_bits = 1;
-    // narrow (32-bit) node-pair sort keys: scene-local id bits, 0 when the batch needs wide keys;
-    // pair_key_bits = scene bits + 2 local bits
-    int pair_local_bits = 0, pair_key_bits = 0;
     std::vector<Scene> h_scenes;
     bool have_inputs = false;
     bool have_solution = false;
@@ -71,11 +68,12 @@ struct Workspace {
     const uint32_t *n2t_sorted_val = nullptr;                // points into val or val_alt
     const uint32_t *n2t_sorted_key = nullptr;
 
-    // pair->term
-    unsigned long long *pair_key = nullptr, *pair_key_alt = nullptr;   // [cap_pair_kv]
-    uint32_t *pair_val = nullptr, *pair_val_alt = nullptr;
+    // pair->term, built row by row: per row its upper pairs' columns and entry counts (at most
+    // kRowPairsMax a row), its first pair and first entry; pair_val holds every pair's term list
+    uint32_t *row_pair_cols = nullptr, *row_pair_cnts = nullptr;   // [cap_nodes * kRowPairsMax]
+    uint32_t *row_pair_first = nullptr, *row_entry_first = nullptr;   // [cap_nodes + 1]
+    uint32_t *pair_val = nullptr;                            // [cap_pair_kv]
     const uint32_t *pair_sorted_val = nullptr;
-    uint32_t *pair_head = nullptr;                           // [cap_pair_kv + 1] marks, then offsets
     uint32_t *half_row = nullptr, *half_col = nullptr;       // [cap_half]
     uint32_t *half_begin = nullptr, *half_end = nullptr;
     uint32_t *half_slot_up = nullptr, *half_slot_lo = nullptr;

@@ -149,11 +149,10 @@ def test_depth_only_scene_same_in_a_batch_with_flow(ws, tiny_scene, precision):
     np.testing.assert_array_equal(mixed[1], alone)
 
 
-def test_wide_pair_keys_give_the_narrow_results(ws, tiny_scene):
-    """Node-pair sort keys are 32-bit (scene, local row, local column) when they fit and 64-bit
-    (global row, global column) otherwise.  65 scenes (7 scene bits) with a 5k-node one (13
-    local bits) need 33 bits, so this batch sorts with 64-bit keys, while each scene alone
-    sorts with 32-bit keys: the results must agree bit for bit."""
+def test_many_scenes_and_a_large_one_give_the_solo_results(ws, tiny_scene):
+    """65 scenes, one of them with 5k nodes (global node ids above 2^16 in the batch, 13-bit
+    local ids): the node-pair map built row by row and every solve in the batch must equal the
+    scenes' solo results bit for bit."""
     from starhub_b200 import scenes
     from starhub_b200.solver import DeviceScene, GpuGeometry
     big = scenes.make_scene(scenes.spec_for_nodes(5000, scenes.config_spec(2)), GpuGeometry(), seed=77)
