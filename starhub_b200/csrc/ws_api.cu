@@ -151,8 +151,8 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.chunk_scene, w.cap_chunks));
     A(dalloc(&w.chunk_row, w.cap_chunks));
     A(dalloc(&w.scan_tmp, scan_cap / ws::kScanTile + 4));
-    A(dalloc(&w.sort_hist, 256ull * ws::sort_max_tiles(sort_cap)));
-    A(dalloc(&w.sort_digit, 256));
+    A(dalloc(&w.sort_hist, (size_t)ws::kSortMaxDigits * ws::sort_max_tiles(sort_cap)));
+    A(dalloc(&w.sort_digit, ws::kSortMaxDigits));
     A(dalloc(&w.d_pixels, w.cap_pixels));
     A(dalloc(&w.d_knn, w.cap_pixels));
     A(dalloc(&w.d_sw, w.cap_pixels));

@@ -601,7 +601,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     count_launch(w);
     const bool n2t_alt = radix_sort<uint32_t>(w.n2t_key, w.n2t_val, w.n2t_key_alt, w.n2t_val_alt, w.counts + kCntN2T, 0,
                                               w.cap_n2t, w.node_bits, w.sort_hist, w.sort_digit, st);
-    count_launch(w, 1 + 3 * ((w.node_bits + 7) / 8));
+    count_launch(w, 1 + 3 * radix_passes(w.node_bits));
     w.n2t_sorted_key = n2t_alt ? w.n2t_key_alt : w.n2t_key;
     w.n2t_sorted_val = n2t_alt ? w.n2t_val_alt : w.n2t_val;
     k_n2t_offsets<<<grid_for(N + 1, 256, w.num_sms), 256, 0, st>>>(w.n2t_sorted_key, w.counts, N, w.n2t_offset);
@@ -616,7 +616,7 @@ void index_build(Workspace &w, cudaStream_t st) {
     k_col_kv<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(w.half_col, w.counts, w.col_key, w.col_val);
     const bool col_alt = radix_sort<uint32_t>(w.col_key, w.col_val, w.col_key_alt, w.col_val_alt, w.counts + kCntHalf,
                                               0, w.cap_half, w.node_bits, w.sort_hist, w.sort_digit, st);
-    count_launch(w, 1 + 1 + 3 + 3 + 1 + 3 * ((w.node_bits + 7) / 8));
+    count_launch(w, 1 + 1 + 3 + 3 + 1 + 3 * radix_passes(w.node_bits));
     const uint32_t *scol = col_alt ? w.col_key_alt : w.col_key;
     const uint32_t *sh = col_alt ? w.col_val_alt : w.col_val;
     k_slots<<<grid_for(w.cap_half, 256, w.num_sms), 256, 0, st>>>(scol, sh, w.counts, w.half_row, w.half_col,

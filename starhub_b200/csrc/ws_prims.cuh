@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 namespace ws {
 
 constexpr int kSortThreads = 256;
@@ -125,26 +127,28 @@ inline void exclusive_scan(const uint32_t *in, uint32_t *out, const uint32_t *n_
 }
 
 // ---------------------------------------------------------------------------
-// Stable LSD radix sort of (key, u32 value), 8 bits per pass.
+// Stable LSD radix sort of (key, u32 value), D = 8 or 9 bits per pass (256 or 512 digits; each
+// thread of a 256-thread block looks after one or two of them).
 // hist layout: hist[digit * max_tiles + tile].
 // ---------------------------------------------------------------------------
-template <class K>
+template <class K, int D>
 __global__ void k_radix_upsweep(const K *keys, const uint32_t *n_dev, uint32_t n_static, int shift,
                                 uint32_t *hist, int max_tiles) {
-    __shared__ uint32_t h[256];
+    constexpr uint32_t kDigits = 1u << D;
+    __shared__ uint32_t h[kDigits];
     const uint32_t n = n_dev ? *n_dev : n_static;
-    h[threadIdx.x] = 0;
+    for (uint32_t d = threadIdx.x; d < kDigits; d += kSortThreads) h[d] = 0;
     __syncthreads();
     const uint32_t base = blockIdx.x * (uint32_t)kSortTile;
     if (base < n) {
 #pragma unroll 4
         for (int r = 0; r < kSortRounds; ++r) {
             const uint32_t idx = base + r * kSortThreads + threadIdx.x;
-            if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 255u], 1u);
+            if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & (kDigits - 1u)], 1u);
         }
     }
     __syncthreads();
-    hist[(size_t)threadIdx.x * max_tiles + blockIdx.x] = h[threadIdx.x];
+    for (uint32_t d = threadIdx.x; d < kDigits; d += kSortThreads) hist[(size_t)d * max_tiles + blockIdx.x] = h[d];
 }
 
 // Exclusive scan of one digit's tile counts (one block per digit) over the tiles in use,
@@ -175,36 +179,55 @@ static __global__ void k_radix_scan(uint32_t *hist, int max_tiles, const uint32_
     if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
 }
 
-template <class K>
+template <class K, int D>
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_scatter(const K *keys_in, const uint32_t *vals_in, K *keys_out, uint32_t *vals_out,
                 const uint32_t *n_dev, uint32_t n_static, int shift,
                 const uint32_t *hist, int max_tiles, const uint32_t *digit_total) {
-    __shared__ uint32_t digit_base[256];
-    __shared__ uint32_t run[256];
-    __shared__ uint16_t wcount[kSortThreads / 32][256];
+    constexpr uint32_t kDigits = 1u << D;
+    constexpr int kPer = (int)kDigits / kSortThreads;   // digits per thread
+    static_assert(kPer == 1 || kPer == 2, "8- or 9-bit digits");
+    __shared__ uint32_t digit_base[kDigits];
+    __shared__ uint32_t run[kDigits];
+    __shared__ uint16_t wcount[kSortThreads / 32][kDigits];
     __shared__ uint32_t sm[32];
     const uint32_t n = n_dev ? *n_dev : n_static;
     const uint32_t base = blockIdx.x * (uint32_t)kSortTile;
     if (base >= n) return;                      // uniform for the whole block
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const uint32_t ex = block_excl_scan_u32(digit_total[t], nullptr, sm);
-    digit_base[t] = ex + hist[(size_t)t * max_tiles + blockIdx.x];
-    run[t] = 0;
+    {
+        // thread t owns digits kPer t .. kPer t + kPer - 1
+        uint32_t tot[kPer], sum = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            tot[k] = digit_total[kPer * t + k];
+            sum += tot[k];
+        }
+        uint32_t ex = block_excl_scan_u32(sum, nullptr, sm);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const uint32_t d = (uint32_t)(kPer * t + k);
+            digit_base[d] = ex + hist[(size_t)d * max_tiles + blockIdx.x];
+            run[d] = 0;
+            ex += tot[k];
+        }
+    }
     for (int r = 0; r < kSortRounds; ++r) {
         const uint32_t idx = base + r * kSortThreads + t;
         const bool valid = idx < n;
         K key = 0;
         uint32_t val = 0;
-        uint32_t d = 256u;
+        uint32_t d = kDigits;
         if (valid) {
             key = keys_in[idx];
             val = vals_in[idx];
-            d = (uint32_t)(key >> shift) & 255u;
+            d = (uint32_t)(key >> shift) & (kDigits - 1u);
         }
         __syncthreads();
 #pragma unroll
-        for (int w = 0; w < kSortThreads / 32; ++w) wcount[w][t] = 0;
+        for (int w = 0; w < kSortThreads / 32; ++w)
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) wcount[w][kPer * t + k] = 0;
         __syncthreads();
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const int rank_w = __popc(peers & ((1u << lane) - 1u));
@@ -218,38 +241,53 @@ k_radix_scatter(const K *keys_in, const uint32_t *vals_in, K *keys_out, uint32_t
             vals_out[pos] = val;
         }
         __syncthreads();
-        uint32_t tot = 0;
 #pragma unroll
-        for (int w = 0; w < kSortThreads / 32; ++w) tot += wcount[w][t];
-        run[t] += tot;
+        for (int k = 0; k < kPer; ++k) {
+            uint32_t tot = 0;
+#pragma unroll
+            for (int w = 0; w < kSortThreads / 32; ++w) tot += wcount[w][kPer * t + k];
+            run[kPer * t + k] += tot;
+        }
         if (base + (uint32_t)(r + 1) * kSortThreads >= n) break;   // uniform
     }
 }
 
 inline int sort_max_tiles(uint32_t cap) { return (int)((cap + kSortTile - 1) / kSortTile) + 1; }
+constexpr int kSortMaxDigits = 512;
 
-// Sorts `bits` low bits of the keys.  Buffers a/b ping-pong; returns true when
-// the result ended in the `alt` buffers.  hist needs 256 * sort_max_tiles(cap)
-// entries, digit_total 256.
+// Sorts `bits` low bits of the keys, 9 bits per pass when that saves a pass over 8 bits.
+// Buffers a/b ping-pong; returns true when the result ended in the `alt` buffers.  hist needs
+// kSortMaxDigits * sort_max_tiles(cap) entries, digit_total kSortMaxDigits.
 template <class K>
 inline bool radix_sort(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt,
                        const uint32_t *n_dev, uint32_t n_static, uint32_t cap, int bits,
                        uint32_t *hist, uint32_t *digit_total, cudaStream_t st) {
     const int max_tiles = sort_max_tiles(cap);
+    const int step = ((bits + 8) / 9 < (bits + 7) / 8) ? 9 : 8;
     bool in_alt = false;
-    for (int shift = 0; shift < bits; shift += 8) {
+    for (int shift = 0; shift < bits; shift += step) {
         K *ki = in_alt ? keys_alt : keys;
         uint32_t *vi = in_alt ? vals_alt : vals;
         K *ko = in_alt ? keys : keys_alt;
         uint32_t *vo = in_alt ? vals : vals_alt;
-        k_radix_upsweep<K><<<max_tiles, kSortThreads, 0, st>>>(ki, n_dev, n_static, shift, hist, max_tiles);
-        k_radix_scan<<<256, 256, 0, st>>>(hist, max_tiles, n_dev, n_static, digit_total);
-        k_radix_scatter<K><<<max_tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_dev, n_static, shift, hist,
-                                                                max_tiles, digit_total);
+        if (step == 9) {
+            k_radix_upsweep<K, 9><<<max_tiles, kSortThreads, 0, st>>>(ki, n_dev, n_static, shift, hist, max_tiles);
+            k_radix_scan<<<512, 256, 0, st>>>(hist, max_tiles, n_dev, n_static, digit_total);
+            k_radix_scatter<K, 9><<<max_tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_dev, n_static, shift, hist,
+                                                                       max_tiles, digit_total);
+        } else {
+            k_radix_upsweep<K, 8><<<max_tiles, kSortThreads, 0, st>>>(ki, n_dev, n_static, shift, hist, max_tiles);
+            k_radix_scan<<<256, 256, 0, st>>>(hist, max_tiles, n_dev, n_static, digit_total);
+            k_radix_scatter<K, 8><<<max_tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n_dev, n_static, shift, hist,
+                                                                       max_tiles, digit_total);
+        }
         in_alt = !in_alt;
     }
     return in_alt;
 }
+
+// Radix passes of radix_sort for `bits` key bits.
+inline int radix_passes(int bits) { return std::min((bits + 8) / 9, (bits + 7) / 8); }
 
 inline int bits_for(uint64_t max_value) {
     int b = 1;
