@@ -65,6 +65,39 @@ def test_index_bit_exact(ws, orc, parity_scene):
         np.testing.assert_array_equal(cols[rp[n] + 1:rp[n + 1]], m["sym_cols"][m["blkrow_offset"][n]:m["blkrow_offset"][n + 1]])
 
 
+def test_index_bit_exact_with_repeated_ids_and_self_edges(ws, orc, small_scene):
+    """Surfels whose knn repeats a node (a term then touches the node pair once per pair of
+    slots, and lies in a node's list once per slot), a self edge and a repeated edge: the
+    node->term and node-pair->term maps must equal the oracle's restatement of the reference's
+    sorted key-value lists entry for entry."""
+    import dataclasses
+    sc = small_scene
+    knn = sc.surfel_knn.copy()
+    knn[::7, 2] = knn[::7, 0]                 # (a, b, a, d)
+    knn[3::11, 3] = knn[3::11, 1]             # (a, b, c, b)
+    knn[5::13, 1:] = knn[5::13, :1]           # (a, a, a, a)
+    edges = np.concatenate([sc.edges, sc.edges[:1], sc.edges[5:6]]).copy()
+    edges[-1, 1] = edges[-1, 0]               # a self edge
+    sc = dataclasses.replace(sc, surfel_knn=knn, edges=edges)
+    s, ds, _ = solve_gpu(ws, sc, 1, 1)
+    pix, dknn, sw, cw = s.dense_terms()
+    opix, oknn, osw, ocw = orc.compact_pixels(sc)
+    np.testing.assert_array_equal(dknn, oknn)
+    assert (oknn[:, 0] == oknn[:, 2]).any() and (oknn[:, 0] == oknn[:, 3]).any()
+    off, ti = s.node2term()
+    ooff, oti = orc.node2term(oknn, sc.edges, sc.num_nodes)
+    np.testing.assert_array_equal(off, ooff)
+    np.testing.assert_array_equal(ti, oti[: ooff[-1]])
+    p = s.node_pairs()
+    m = orc.nodepair2term(oknn, sc.edges, sc.num_nodes)
+    np.testing.assert_array_equal(p["rows"], m["half_rows"])
+    np.testing.assert_array_equal(p["cols"], m["half_cols"])
+    np.testing.assert_array_equal(p["begin"], m["half_begin"])
+    np.testing.assert_array_equal(p["end"], m["half_end"])
+    np.testing.assert_array_equal(p["term_index"], m["term_index"][: m["half_end"][-1]])
+    s.Sync()   # no capacity or argument error
+
+
 def to_local(step, centres):
     """Origin twists (w, t) as node-centred twists (w, t - c x w)."""
     out = step.astype(np.float64).copy()
