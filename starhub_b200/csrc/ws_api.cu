@@ -210,7 +210,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     }
     if (e == cudaSuccess) {
         w.pcg_grid = ws::pcg_max_blocks(w.device);
-        A(dalloc(&w.pcg_warp_groups, (size_t)ws::kPcgUnitsPerWarp * w.pcg_grid * ws::pcg_warps_per_block() + 1));
+        A(dalloc(&w.pcg_warp_groups, (size_t)ws::kPcgUnitsPerWarp * w.pcg_grid * ws::pcg_warps_per_block() + 2));
         A(dalloc(&w.pcg_tickets, 4));
     }
     if (e != cudaSuccess) {
@@ -443,7 +443,7 @@ int ws_solve_graph(ws_solver *h, int gn_iters, int pcg_iters, void *stream) {
     w.last_stream = st;
     const uint64_t key[] = {(uint64_t)gn_iters, (uint64_t)pcg_iters, (uint64_t)w.num_scenes, w.total_nodes,
                             w.total_edges, w.total_tiles, w.total_chunks, (uint64_t)w.node_bits,
-                            (uint64_t)w.dense_channels};
+                            (uint64_t)w.dense_channels, (uint64_t)ws::pcg_split_group(w)};
     constexpr size_t kKey = sizeof(key) / sizeof(key[0]);
     bool same = w.graph_exec && w.graph_key.size() == kKey && std::equal(key, key + kKey, w.graph_key.begin());
     if (same) {

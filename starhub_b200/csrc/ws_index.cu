@@ -534,23 +534,41 @@ __global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *item_ptr, co
     }
 }
 
-// First row group of every PCG work unit (kPcgUnitsPerWarp per warp), chosen so that the units'
-// stored blocks (items) are about equal: unit w starts at the first group whose first item is at
-// or past w / units of all items.
-__global__ void k_pcg_ranges(const uint32_t *item_ptr, const uint32_t *group_row, uint32_t groups,
-                             uint32_t total_nodes, uint32_t cap_items, uint32_t warps, uint32_t *warp_groups) {
+// First row group of every PCG phase-A work unit (kPcgUnitsPerWarp per warp), chosen so that the
+// units' stored blocks (items) are about equal.  The groups before `split` (the first half of the
+// scenes) and the groups from `split` on get separate units, their numbers in proportion to
+// their items (at least one each when both halves have groups): unit w of a half starts at the
+// first group of the half whose first item is at or past w / units of the half's items.
+// warp_groups[units] is the group count and warp_groups[units + 1] the first half's units.
+__global__ void k_pcg_ranges(const uint32_t *item_ptr, const uint32_t *group_row, uint32_t groups, uint32_t split,
+                             uint32_t total_nodes, uint32_t cap_items, uint32_t units, uint32_t *warp_groups) {
     const uint32_t total = min(item_ptr[total_nodes], cap_items);
-    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w <= warps; w += gridDim.x * blockDim.x) {
-        if (w == warps) {
-            warp_groups[w] = groups;
+    split = min(split, groups);
+    const uint32_t mid = split < groups ? min(item_ptr[min(group_row[split], total_nodes)], total) : total;
+    uint32_t ux = units;
+    if (split > 0 && split < groups && units > 1) {
+        ux = (uint32_t)(((unsigned long long)units * mid + total / 2) / max(total, 1u));
+        ux = min(max(ux, 1u), units - 1);
+    }
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w <= units + 1; w += gridDim.x * blockDim.x) {
+        if (w >= units) {
+            warp_groups[w] = (w == units) ? groups : ux;
             continue;
         }
-        const uint32_t target = (uint32_t)(((unsigned long long)total * w) / warps);
-        uint32_t lo = 0, hi = groups;
+        uint32_t lo, hi, target;
+        if (w < ux) {
+            lo = 0;
+            hi = split;
+            target = (uint32_t)(((unsigned long long)mid * w) / ux);
+        } else {
+            lo = split;
+            hi = groups;
+            target = mid + (uint32_t)(((unsigned long long)(total - mid) * (w - ux)) / (units - ux));
+        }
         while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (item_ptr[min(group_row[mid], total_nodes)] < target) lo = mid + 1;
-            else hi = mid;
+            const uint32_t m = (lo + hi) >> 1;
+            if (item_ptr[min(group_row[m], total_nodes)] < target) lo = m + 1;
+            else hi = m;
         }
         warp_groups[w] = lo;
     }
@@ -630,10 +648,10 @@ void index_build(Workspace &w, cudaStream_t st) {
 }
 
 void pcg_ranges(Workspace &w, cudaStream_t st) {
-    const uint32_t warps = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
-    k_pcg_ranges<<<grid_for(warps + 1, 256, w.num_sms), 256, 0, st>>>(w.item_ptr, w.chunk_row, w.total_chunks,
-                                                                      w.total_nodes, w.cap_items, warps,
-                                                                      w.pcg_warp_groups);
+    const uint32_t units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
+    k_pcg_ranges<<<grid_for(units + 2, 256, w.num_sms), 256, 0, st>>>(w.item_ptr, w.chunk_row, w.total_chunks,
+                                                                      pcg_split_group(w), w.total_nodes, w.cap_items,
+                                                                      units, w.pcg_warp_groups);
     count_launch(w);
 }
 

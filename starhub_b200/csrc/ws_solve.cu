@@ -847,13 +847,18 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
 // libs/star/pcg_solver/BlockPCG.cuh:67-190, 325-484) for every scene of the batch.
 //
 // Rows (nodes) are grouped in scene-aligned groups of kRowsPerGroup.  Phase A (the SpMV) works on
-// units, contiguous ranges of groups balanced by stored blocks (kPcgUnitsPerWarp per warp), which
-// the warps take by ticket: one counter grows through the launch, tickets it*U .. (it+1)*U - 1
-// are the units of iteration it, and a warp keeps the ticket that ended its iteration for the
-// next one.  So the warps that finish early take the remaining units instead of waiting for the
-// slowest, and every unit is processed once per iteration.  Phase B takes units of row groups
-// (about kPcgBUnitsPerWarp per warp) the same way from a second counter.  Init and the twist update take
-// equal numbers of groups per warp.  No block-level synchronisation.
+// units, contiguous ranges of groups balanced by stored blocks (kPcgUnitsPerWarp per warp);
+// phase B on units of bunit_groups row groups (about kPcgBUnitsPerWarp per warp).  The scenes are
+// split at a scene boundary into two halves, X and Y, that run half a phase apart: step k of the
+// schedule holds X's phase A of iteration k/2 with Y's phase B of iteration k/2 - 1 (k even), or
+// X's phase B with Y's phase A of iteration (k-1)/2 (k odd), the two parts' units interleaved in
+// proportion.  So at any time some warps stream blocks from DRAM while others do the
+// latency-bound per-row work.  The warps take the units by ticket from one counter that grows
+// through the launch (the schedule's units in order), so the warps that finish early take the
+// remaining units instead of waiting for the slowest.  A unit depends only on units of its
+// scenes in the step before, which have smaller tickets, and a warp finishes its unit before it
+// takes the next ticket, so the smallest unfinished ticket can always proceed.  Init and the
+// twist update take equal numbers of groups per warp.  No block-level synchronisation.
 // Per iteration: phase A  d = s + beta d (recomputed for neighbours from s and the
 // previous d), q = A d from each stored block read once (the transposed products go
 // to the lower rows through a contribution buffer), <d, A d>;  phase B  alpha,
@@ -874,12 +879,13 @@ struct PcgArgs {
     const uint32_t *item_ptr;      // [nodes + 1] first item of every row in the symmetric store
     const uint2 *item_info;        // per item: column | kItemRowStart, lower entry (upper) or scene (diagonal)
     const uint32_t *item_col;      // per item: column | kItemRowStart on a row's diagonal item
-    const uint32_t *warp_groups;   // [units + 1] first row group of each phase-A work unit
+    // [units + 2]: first row group of each phase-A work unit, then the group count, then the
+    // number of units of the first half (X) of the scenes
+    const uint32_t *warp_groups;
     uint32_t total_units;          // kPcgUnitsPerWarp x the launch's warps
-    uint32_t *tickets;             // phase-A work-unit tickets, growing through a launch (zeroed before it)
-    uint32_t total_bunits;         // phase-B units: bunit_groups row groups each
-    uint32_t bunit_groups;
-    uint32_t *btickets;            // phase-B unit tickets, like `tickets`
+    uint32_t split_group;          // first group of the second half (Y) of the scenes
+    uint32_t *tickets;             // work-unit tickets, growing through a launch (zeroed before it)
+    uint32_t bunit_groups;         // row groups of a phase-B unit
     const float *sym_blocks;       // per item: the 6x6 block, row-major
     const float *inv_diag, *jtr;
     float *contrib;                // per lower entry (row j, column i < j): B^T v_i left for row j (6 floats)
@@ -1543,40 +1549,57 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     }
     publish_range(A, b_begin, b_end, 2, 0, lane);
 
-    // the warp's next phase-A and phase-B tickets (see the header comment)
-    uint32_t ticket = 0, bticket = 0;
-    if (lane == 0) {
-        ticket = atomicAdd(A.tickets, 1u);
-        bticket = atomicAdd(A.btickets, 1u);
-    }
+    // the schedule (see the header comment): X's and Y's phase-A and phase-B unit counts
+    const uint32_t G = A.total_groups, gm = min(A.split_group, G), bug = A.bunit_groups;
+    const uint32_t ux = min(A.warp_groups[A.total_units + 1], A.total_units), uy = A.total_units - ux;
+    const uint32_t bx = (gm + bug - 1) / bug, by = (G - gm + bug - 1) / bug;
+    const uint32_t step_even = ux + by, step_odd = bx + uy;   // units of the steps 2, 4, .. and 1, 3, ..
+    const uint32_t I = (uint32_t)max(A.pcg_iters, 0);
+    // steps 0 .. 2I: step 0 holds X's first phase A only, step 2I Y's last phase B only
+    const uint32_t total = I == 0 ? 0u : ux + I * step_odd + (I - 1) * step_even + by;
+    uint32_t ticket = 0;
+    if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
     ticket = __shfl_sync(0xffffffffu, ticket, 0);
-    bticket = __shfl_sync(0xffffffffu, bticket, 0);
-
-    for (int it = 0; it < A.pcg_iters; ++it) {
+    while (ticket < total) {
+        // the ticket's step k and its index i there
+        uint32_t k, i;
+        if (ticket < ux) {
+            k = 0;
+            i = ticket;
+        } else {
+            const uint32_t t = ticket - ux, pair = t / (step_odd + step_even), rem = t % (step_odd + step_even);
+            k = 1 + 2 * pair + (rem < step_odd ? 0u : 1u);
+            i = rem < step_odd ? rem : rem - step_odd;
+        }
+        // the step's X and Y units, interleaved in proportion; X's come first in a tie
+        const bool odd = (k & 1u) != 0;
+        const uint32_t nx = odd ? bx : (k < 2 * I ? ux : 0u);
+        const uint32_t ny = odd ? uy : (k > 0 ? by : 0u);
+        const uint32_t x_before = (uint32_t)((unsigned long long)i * nx / (nx + ny));
+        const bool in_x = (uint32_t)((unsigned long long)(i + 1) * nx / (nx + ny)) > x_before;
+        const uint32_t j = in_x ? x_before : i - x_before;
+        // X runs phase k % 2 of iteration k / 2, Y half a phase later
+        const bool phase_a = in_x ? !odd : odd;
+        const int it = (int)(in_x ? k / 2 : (k - 1) / 2);
         const float *sd_old = (it & 1) ? A.sd1 : A.sd0;
         float *sd_new = (it & 1) ? A.sd0 : A.sd1;
-        // ---- phase A: d = s + beta d, q = A d, <d, q>, unit by unit ----
-        const uint32_t first = (uint32_t)it * A.total_units;
-        while (ticket < first + A.total_units) {
-            const uint32_t u = ticket - first;
-            const uint32_t g_begin = min(A.warp_groups[u], A.total_groups);
-            const uint32_t g_end = max(g_begin, min(A.warp_groups[u + 1], A.total_groups));
+        if (phase_a) {
+            // ---- phase A: d = s + beta d, q = A d, <d, q> ----
+            const uint32_t u = in_x ? j : ux + j;
+            const uint32_t g_begin = min(A.warp_groups[u], G);
+            const uint32_t g_end = max(g_begin, min(A.warp_groups[u + 1], G));
             if (g_begin < g_end) {
                 const uint32_t r_begin = A.group_row[g_begin];
-                const uint32_t r_end = g_end < A.total_groups ? A.group_row[g_end] : A.total_nodes;
+                const uint32_t r_end = g_end < G ? A.group_row[g_end] : A.total_nodes;
                 // the unit's scenes have finished the last iteration's phase B (init for the first)
                 if (!wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 1u, lane)) return;
                 if (!stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane)) return;
                 publish_range(A, g_begin, g_end, 0, it, lane);
             }
-            if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
-            ticket = __shfl_sync(0xffffffffu, ticket, 0);
-        }
-        // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s>, unit by unit ----
-        const uint32_t bfirst = (uint32_t)it * A.total_bunits;
-        while (bticket < bfirst + A.total_bunits) {
-            const uint32_t g_begin = (bticket - bfirst) * A.bunit_groups;
-            const uint32_t g_end = min(g_begin + A.bunit_groups, A.total_groups);
+        } else {
+            // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
+            const uint32_t g_begin = in_x ? j * bug : gm + j * bug;
+            const uint32_t g_end = min(g_begin + bug, in_x ? gm : G);
             // the unit's scenes have finished phase A and published alpha
             if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
             for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
@@ -1591,9 +1614,9 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
                     load6(A.q + 8ull * n.node, qv);
                     add_lower(A, n.node, qv);
 #pragma unroll
-                    for (int i = 0; i < 6; ++i) {
-                        xv[i] += alpha * dv[i];
-                        rv[i] -= alpha * qv[i];
+                    for (int c = 0; c < 6; ++c) {
+                        xv[c] += alpha * dv[c];
+                        rv[c] -= alpha * qv[c];
                     }
                     matvec6(A.inv_diag + 36ull * n.node, rv, sv);
                     store6(A.x + 8ull * n.node, xv);
@@ -1604,9 +1627,9 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
                 if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
             }
             publish_range(A, g_begin, g_end, 1, it + 1, lane);
-            if (lane == 0) bticket = atomicAdd(A.btickets, 1u);
-            bticket = __shfl_sync(0xffffffffu, bticket, 0);
         }
+        if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
+        ticket = __shfl_sync(0xffffffffu, ticket, 0);
     }
     // x of the warp's rows was last written by whichever warps took their phase-B units
     if (!wait_scenes(A, b_begin, b_end, 1, (uint32_t)A.pcg_iters + 1u, lane)) return;
@@ -2106,6 +2129,20 @@ void gn_assemble_pair(Workspace &w, cudaStream_t st) {
     count_launch(w);
 }
 
+uint32_t pcg_split_group(const Workspace &w) {
+    // the scene boundary nearest to half of the row groups (after the first scene at least)
+    const uint32_t half = w.total_chunks / 2;
+    uint32_t best = w.total_chunks, end = 0;
+    for (int s = 0; s < w.num_scenes && s < (int)w.h_scenes.size(); ++s) {
+        end += (uint32_t)w.h_scenes[s].num_chunks;
+        if (end >= w.total_chunks) break;
+        const uint32_t d = end > half ? end - half : half - end;
+        const uint32_t db = best > half ? best - half : half - best;
+        if (d < db) best = end;
+    }
+    return best;
+}
+
 static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     PcgArgs a;
     a.scenes = w.scenes;
@@ -2119,15 +2156,14 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.contrib = w.contrib;
     a.warp_groups = w.pcg_warp_groups;
     a.total_units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
+    a.split_group = pcg_split_group(w);
     a.tickets = w.pcg_tickets;
     {
         // about kPcgBUnitsPerWarp units per warp: two row groups each on the large batches, one on
         // problems with a warp per group or so
         const uint64_t slots = (uint64_t)kPcgBUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block();
         a.bunit_groups = (uint32_t)std::max<uint64_t>(1, (w.total_chunks + slots - 1) / slots);
-        a.total_bunits = (uint32_t)((w.total_chunks + a.bunit_groups - 1) / a.bunit_groups);
     }
-    a.btickets = w.pcg_tickets + 1;
     a.sym_blocks = w.sym_blocks;
     a.inv_diag = w.inv_diag;
     a.jtr = w.jtr;
@@ -2154,7 +2190,7 @@ cudaError_t gn_pcg(Workspace &w, int pcg_iters, cudaStream_t st) {
     // tickets and generations start at zero every launch, so a launch that timed out half-way
     // cannot leak into the next
     cudaMemsetAsync(w.scene_counter, 0, sizeof(uint32_t) * kSceneSync * (size_t)w.num_scenes, st);
-    cudaMemsetAsync(w.pcg_tickets, 0, 2 * sizeof(uint32_t), st);
+    cudaMemsetAsync(w.pcg_tickets, 0, sizeof(uint32_t), st);
     void *args[] = {&a};
     count_launch(w);
     return cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, kPcgSmemBytes, st);

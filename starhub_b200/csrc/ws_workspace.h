@@ -98,9 +98,10 @@ struct Workspace {
     uint32_t *item_col = nullptr;                            // [cap_items]
     float *sym_blocks = nullptr;                             // [cap_items * 36]
     float *contrib = nullptr;                                // [cap_half * 6]
-    uint32_t *pcg_warp_groups = nullptr;                     // [kPcgUnitsPerWarp * pcg_grid * warps per block + 1]:
-                                                             // first row group of every PCG work unit
-    uint32_t *pcg_tickets = nullptr;                         // [1]: PCG work-unit tickets, zeroed per launch
+    uint32_t *pcg_warp_groups = nullptr;                     // [kPcgUnitsPerWarp * pcg_grid * warps per block + 2]:
+                                                             // first row group of every PCG work unit, the
+                                                             // group count, the first half's unit count
+    uint32_t *pcg_tickets = nullptr;                         // [4]: [0] PCG work-unit tickets, zeroed per launch
     float *mf_ux = nullptr;             // matrix-free SpMV scratch: J x per dense term and edge (float4),
                                         // allocated on first use
 
@@ -157,6 +158,8 @@ void init_warp(Workspace &w, cudaStream_t st);
 int pcg_max_blocks(int device);
 int pcg_launch_blocks(const Workspace &w);
 void pcg_ranges(Workspace &w, cudaStream_t st);
+// First row group of the second half of the scenes in the PCG's schedule (a scene boundary).
+uint32_t pcg_split_group(const Workspace &w);
 cudaError_t gn_spmv(Workspace &w, const float *x, float *y, cudaStream_t st);
 // Runs the PCG's bounded scene wait on a generation nothing advances; *status gets the flag it left.
 cudaError_t pcg_wait_selftest(int *status, cudaStream_t st);
