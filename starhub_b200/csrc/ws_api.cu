@@ -35,7 +35,7 @@ void free_all(ws::Workspace &w) {
                     w.n2t_val_alt, w.n2t_offset, w.row_pair_cols, w.row_pair_cnts, w.row_pair_first,
                     w.row_entry_first, w.pair_val, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
-                    w.col_key_alt, w.col_val_alt, w.colidx, w.item_ptr, w.item_info, w.item_col, w.sym_blocks, w.contrib, w.pcg_warp_groups, w.pcg_tickets, w.mf_ux, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
+                    w.col_key_alt, w.col_val_alt, w.colidx, w.item_ptr, w.item_info, w.item_col, w.sym_blocks, w.contrib, w.pcg_warp_groups, w.pcg_unit_info, w.pcg_tickets, w.mf_ux, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
                     w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter,
                     w.error_flag};
     for (void *p : ptrs)
@@ -211,6 +211,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     if (e == cudaSuccess) {
         w.pcg_grid = ws::pcg_max_blocks(w.device);
         A(dalloc(&w.pcg_warp_groups, (size_t)ws::kPcgUnitsPerWarp * w.pcg_grid * ws::pcg_warps_per_block() + 2));
+        A(dalloc(&w.pcg_unit_info, 2 * (size_t)ws::kPcgUnitsPerWarp * w.pcg_grid * ws::pcg_warps_per_block()));
         A(dalloc(&w.pcg_tickets, 4));
     }
     if (e != cudaSuccess) {

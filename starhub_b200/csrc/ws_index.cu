@@ -540,37 +540,59 @@ __global__ void k_diag_cols(const uint32_t *rowptr, const uint32_t *item_ptr, co
 // their items (at least one each when both halves have groups): unit w of a half starts at the
 // first group of the half whose first item is at or past w / units of the half's items.
 // warp_groups[units] is the group count and warp_groups[units + 1] the first half's units.
-__global__ void k_pcg_ranges(const uint32_t *item_ptr, const uint32_t *group_row, uint32_t groups, uint32_t split,
-                             uint32_t total_nodes, uint32_t cap_items, uint32_t units, uint32_t *warp_groups) {
-    const uint32_t total = min(item_ptr[total_nodes], cap_items);
-    split = min(split, groups);
-    const uint32_t mid = split < groups ? min(item_ptr[min(group_row[split], total_nodes)], total) : total;
-    uint32_t ux = units;
-    if (split > 0 && split < groups && units > 1) {
-        ux = (uint32_t)(((unsigned long long)units * mid + total / 2) / max(total, 1u));
-        ux = min(max(ux, 1u), units - 1);
+// unit_info[2w], [2w + 1] describe unit w for the PCG: its groups, rows and items (first, end)
+// and the scenes of its first and last group, so that a unit starts from one load.
+struct UnitSplit {
+    uint32_t split, mid, total, ux, units, groups;
+};
+__device__ uint32_t unit_first_group(const UnitSplit &U, uint32_t w, const uint32_t *item_ptr,
+                                     const uint32_t *group_row, uint32_t total_nodes) {
+    if (w >= U.units) return U.groups;
+    uint32_t lo, hi, target;
+    if (w < U.ux) {
+        lo = 0;
+        hi = U.split;
+        target = (uint32_t)(((unsigned long long)U.mid * w) / U.ux);
+    } else {
+        lo = U.split;
+        hi = U.groups;
+        target = U.mid + (uint32_t)(((unsigned long long)(U.total - U.mid) * (w - U.ux)) / (U.units - U.ux));
+    }
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (item_ptr[min(group_row[m], total_nodes)] < target) lo = m + 1;
+        else hi = m;
+    }
+    return lo;
+}
+
+__global__ void k_pcg_ranges(const uint32_t *item_ptr, const uint32_t *group_row, const uint32_t *group_scene,
+                             uint32_t groups, uint32_t split, uint32_t total_nodes, uint32_t cap_items, uint32_t units,
+                             uint32_t *warp_groups, uint4 *unit_info) {
+    UnitSplit U;
+    U.units = units;
+    U.groups = groups;
+    U.total = min(item_ptr[total_nodes], cap_items);
+    U.split = min(split, groups);
+    U.mid = U.split < groups ? min(item_ptr[min(group_row[U.split], total_nodes)], U.total) : U.total;
+    U.ux = units;
+    if (U.split > 0 && U.split < groups && units > 1) {
+        U.ux = (uint32_t)(((unsigned long long)units * U.mid + U.total / 2) / max(U.total, 1u));
+        U.ux = min(max(U.ux, 1u), units - 1);
     }
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w <= units + 1; w += gridDim.x * blockDim.x) {
         if (w >= units) {
-            warp_groups[w] = (w == units) ? groups : ux;
+            warp_groups[w] = (w == units) ? groups : U.ux;
             continue;
         }
-        uint32_t lo, hi, target;
-        if (w < ux) {
-            lo = 0;
-            hi = split;
-            target = (uint32_t)(((unsigned long long)mid * w) / ux);
-        } else {
-            lo = split;
-            hi = groups;
-            target = mid + (uint32_t)(((unsigned long long)(total - mid) * (w - ux)) / (units - ux));
-        }
-        while (lo < hi) {
-            const uint32_t m = (lo + hi) >> 1;
-            if (item_ptr[min(group_row[m], total_nodes)] < target) lo = m + 1;
-            else hi = m;
-        }
-        warp_groups[w] = lo;
+        const uint32_t g0 = unit_first_group(U, w, item_ptr, group_row, total_nodes);
+        const uint32_t g1 = max(g0, unit_first_group(U, w + 1, item_ptr, group_row, total_nodes));
+        warp_groups[w] = g0;
+        const uint32_t r0 = g0 < groups ? min(group_row[g0], total_nodes) : total_nodes;
+        const uint32_t r1 = g1 < groups ? min(group_row[g1], total_nodes) : total_nodes;
+        const uint32_t s0 = g0 < g1 ? group_scene[g0] : 0u, s1 = g0 < g1 ? group_scene[g1 - 1] : 0u;
+        unit_info[2 * w] = make_uint4(g0, g1, r0, r1);
+        unit_info[2 * w + 1] = make_uint4(min(item_ptr[r0], cap_items), min(item_ptr[r1], cap_items), s0, s1);
     }
 }
 
@@ -649,9 +671,9 @@ void index_build(Workspace &w, cudaStream_t st) {
 
 void pcg_ranges(Workspace &w, cudaStream_t st) {
     const uint32_t units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
-    k_pcg_ranges<<<grid_for(units + 2, 256, w.num_sms), 256, 0, st>>>(w.item_ptr, w.chunk_row, w.total_chunks,
-                                                                      pcg_split_group(w), w.total_nodes, w.cap_items,
-                                                                      units, w.pcg_warp_groups);
+    k_pcg_ranges<<<grid_for(units + 2, 256, w.num_sms), 256, 0, st>>>(
+        w.item_ptr, w.chunk_row, w.chunk_scene, w.total_chunks, pcg_split_group(w), w.total_nodes, w.cap_items, units,
+        w.pcg_warp_groups, w.pcg_unit_info);
     count_launch(w);
 }
 

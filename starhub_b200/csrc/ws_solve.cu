@@ -882,6 +882,9 @@ struct PcgArgs {
     // [units + 2]: first row group of each phase-A work unit, then the group count, then the
     // number of units of the first half (X) of the scenes
     const uint32_t *warp_groups;
+    // [2 * units]: per phase-A unit {first group, end group, first row, end row}, {first item,
+    // end item, scene of the first group, scene of the last group}
+    const uint4 *unit_info;
     uint32_t total_units;          // kPcgUnitsPerWarp x the launch's warps
     uint32_t split_group;          // first group of the second half (Y) of the scenes
     uint32_t *tickets;             // work-unit tickets, growing through a launch (zeroed before it)
@@ -986,6 +989,28 @@ __device__ bool wait_scenes(const PcgArgs &A, uint32_t g_begin, uint32_t g_end, 
     // the scenes' vectors and scalars after the publications they saw
     ok = __all_sync(0xffffffffu, ok);
     return ok;
+}
+
+// wait_scenes for a unit whose groups all lie in one scene: lane 0 polls that scene's generation.
+__device__ bool wait_one_scene(const PcgArgs &A, uint32_t scene, int which, uint32_t target, int lane) {
+    bool ok = true;
+    if (lane == 0) {
+        const uint32_t *gen = A.scene_counter + (size_t)kSceneSync * min(scene, A.num_scenes - 1) + 32 + which;
+        unsigned long long waited_ns = 0;
+        unsigned sleep_ns = 32;
+        while (ld_acquire(gen) < target) {
+            if (waited_ns > kBarrierTimeoutNs || *reinterpret_cast<volatile int *>(A.err) == WS_ERR_TIMEOUT) {
+                set_err(A.err, WS_ERR_TIMEOUT);
+                ok = false;
+                break;
+            }
+            __nanosleep(sleep_ns);
+            waited_ns += sleep_ns;
+            sleep_ns = min(sleep_ns * 2u, 256u);
+        }
+    }
+    // lane 0's acquire load, then this barrier, order the warp's later reads
+    return __all_sync(0xffffffffu, __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0);
 }
 
 // Failure-detection self-test: one warp runs wait_scenes on one scene whose generation
@@ -1257,17 +1282,16 @@ __device__ __forceinline__ void store6_f2(float *p, const float *v) {   // 8-byt
     for (int k = 0; k < 3; ++k) reinterpret_cast<float2 *>(p)[k] = make_float2(v[2 * k], v[2 * k + 1]);
 }
 
-// Phase A over items u0 .. u1 (rows r0 .. r1 - 1, groups g0 .. g1 - 1); false after a timed-out
+// Phase A over items u0 .. u1 (rows from r0 on, groups g0 .. g1 - 1); false after a timed-out
 // wait for a bulk copy (WS_ERR_TIMEOUT is set).
-__device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t r1, const float *vec_in,
-                             float *out, float *wsm, int lane) {
+__device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_t r0, uint32_t u0, uint32_t u1,
+                             const float *vec_in, float *out, float *wsm, int lane) {
     if (g0 >= g1) return true;
     float *blocks = wsm;                                                // [2][32][36]
     float *recs = wsm + 2 * kPcgBlockFloats;                            // [2][32][kSdStride]
     float *vring = recs + 2 * kPcgRecFloats;                            // [kPcgRing][8]: v of the row, beta
     double *gring = reinterpret_cast<double *>(vring + kPcgRing * 8);   // [kPcgRing] <d, A d> by row
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(gring + kPcgRing);
-    const uint32_t u0 = min(A.item_ptr[r0], A.cap_items), u1 = min(A.item_ptr[r1], A.cap_items);
     const uint32_t nchunks = u1 > u0 ? (u1 - u0 + 31) / 32 : 0;
     const uint64_t pol = evict_first_policy();
     if (lane == 0) {
@@ -1281,6 +1305,10 @@ __device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
     bool ok = true;
     uint2 cur = load_item(A.item_info, u0 + lane, u1);
     uint2 nxt = load_item(A.item_info, u0 + 32 + lane, u1);
+    // first rows of groups win .. win + 31 (lane i holds group win + i), reloaded as groups
+    // complete; requested with the item records, before the column records need those
+    uint32_t win = g0;
+    uint32_t win_row = g0 + lane < A.total_groups ? A.group_row[g0 + lane] : A.total_nodes;
     float beta_cur;
     issue_records(A, vec_in, cur, recs, lane, beta_cur);
     float carry[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1289,9 +1317,6 @@ __device__ bool stream_items(const PcgArgs &A, uint32_t g0, uint32_t g1, uint32_
     // the row of the item before the chunk; the range starts with row r0's diagonal item, so
     // an item's row is this plus the row starts up to and including it (unsigned wrap at r0 = 0)
     uint32_t row_before = r0 - 1u;
-    // first rows of groups win .. win + 31 (lane i holds group win + i), reloaded as groups complete
-    uint32_t win = g0;
-    uint32_t win_row = g0 + lane < A.total_groups ? A.group_row[g0 + lane] : A.total_nodes;
     auto group_first = [&](uint32_t g) -> uint32_t {   // first row of group g (g >= win)
         if (g >= A.total_groups) return A.total_nodes;
         if (g - win < 32) return __shfl_sync(0xffffffffu, win_row, (int)(g - win));
@@ -1586,24 +1611,36 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         if (phase_a) {
             // ---- phase A: d = s + beta d, q = A d, <d, q> ----
             const uint32_t u = in_x ? j : ux + j;
-            const uint32_t g_begin = min(A.warp_groups[u], G);
-            const uint32_t g_end = max(g_begin, min(A.warp_groups[u + 1], G));
+            const uint4 ua = A.unit_info[2 * u], ub = A.unit_info[2 * u + 1];
+            const uint32_t g_begin = min(ua.x, G), g_end = max(g_begin, min(ua.y, G));
             if (g_begin < g_end) {
-                const uint32_t r_begin = A.group_row[g_begin];
-                const uint32_t r_end = g_end < G ? A.group_row[g_end] : A.total_nodes;
                 // the unit's scenes have finished the last iteration's phase B (init for the first)
-                if (!wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 1u, lane)) return;
-                if (!stream_items(A, g_begin, g_end, r_begin, r_end, sd_old, sd_new, wsm, lane)) return;
+                const bool waited = ub.z == ub.w ? wait_one_scene(A, ub.z, 1, (uint32_t)it + 1u, lane)
+                                                 : wait_scenes(A, g_begin, g_end, 1, (uint32_t)it + 1u, lane);
+                if (!waited) return;
+                const uint32_t u_begin = min(ub.x, A.cap_items), u_end = max(u_begin, min(ub.y, A.cap_items));
+                if (!stream_items(A, g_begin, g_end, ua.z, u_begin, u_end, sd_old, sd_new, wsm, lane)) return;
                 publish_range(A, g_begin, g_end, 0, it, lane);
             }
         } else {
             // ---- phase B: alpha; x += alpha d; r -= alpha q; s = M^-1 r; <r, s> ----
             const uint32_t g_begin = in_x ? j * bug : gm + j * bug;
             const uint32_t g_end = min(g_begin + bug, in_x ? gm : G);
-            // the unit's scenes have finished phase A and published alpha
-            if (!wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane)) return;
+            // the unit's scenes have finished phase A and published alpha; the first step's rows
+            // and scenes (fixed for the launch) are read first and tell which scenes to wait for
+            NodeStep n = node_step(A, g_begin, g_end, lane);
+            bool waited;
+            if (g_end - g_begin <= (uint32_t)kGroupsPerStep) {
+                const uint32_t s_lo = __reduce_min_sync(0xffffffffu, n.group_ok ? n.scene : 0xffffffffu);
+                const uint32_t s_hi = __reduce_max_sync(0xffffffffu, n.group_ok ? n.scene : 0u);
+                waited = s_lo == s_hi ? wait_one_scene(A, s_lo, 0, (uint32_t)it + 1u, lane)
+                                      : wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane);
+            } else {
+                waited = wait_scenes(A, g_begin, g_end, 0, (uint32_t)it + 1u, lane);
+            }
+            if (!waited) return;
             for (uint32_t g = g_begin; g < g_end; g += kGroupsPerStep) {
-                const NodeStep n = node_step(A, g, g_end, lane);
+                if (g != g_begin) n = node_step(A, g, g_end, lane);
                 float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, sv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 if (n.valid) {
                     const float alpha = (float)__ldcg(A.scalars + 8ull * n.scene + 1);
@@ -2155,6 +2192,7 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.item_col = w.item_col;
     a.contrib = w.contrib;
     a.warp_groups = w.pcg_warp_groups;
+    a.unit_info = w.pcg_unit_info;
     a.total_units = (uint32_t)(kPcgUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block());
     a.split_group = pcg_split_group(w);
     a.tickets = w.pcg_tickets;

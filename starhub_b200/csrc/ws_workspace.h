@@ -101,6 +101,7 @@ struct Workspace {
     uint32_t *pcg_warp_groups = nullptr;                     // [kPcgUnitsPerWarp * pcg_grid * warps per block + 2]:
                                                              // first row group of every PCG work unit, the
                                                              // group count, the first half's unit count
+    uint4 *pcg_unit_info = nullptr;                          // [2 * PCG work units]: groups, rows, items, scenes
     uint32_t *pcg_tickets = nullptr;                         // [4]: [0] PCG work-unit tickets, zeroed per launch
     float *mf_ux = nullptr;             // matrix-free SpMV scratch: J x per dense term and edge (float4),
                                         // allocated on first use
