@@ -33,7 +33,7 @@ void free_all(ws::Workspace &w) {
                     w.chunk_scene, w.chunk_row, w.scan_tmp, w.sort_hist, w.sort_digit, w.d_pixels, w.d_knn,
                     w.d_sw, w.d_cw, w.d_scene, w.d_record, w.r_record, w.n2t_key, w.n2t_val, w.n2t_key_alt,
                     w.n2t_val_alt, w.n2t_offset, w.row_pair_cols, w.row_pair_cnts, w.row_pair_first,
-                    w.row_entry_first, w.pair_val, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_slot_up,
+                    w.row_entry_first, w.pair_val, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_scene, w.half_slot_up,
                     w.half_slot_lo, w.row_cnt_up, w.row_cnt_lo, w.row_first, w.rowptr, w.col_key, w.col_val,
                     w.col_key_alt, w.col_val_alt, w.colidx, w.item_ptr, w.item_info, w.item_col, w.sym_blocks, w.contrib, w.pcg_warp_groups, w.pcg_unit_info, w.pcg_tickets, w.mf_ux, w.inv_diag, w.diag64, w.jtr, w.x, w.r, w.q,
                     w.sd0, w.sd1, w.se3, w.centers, w.chunk_partial, w.scene_scalars, w.scene_counter,
@@ -174,6 +174,7 @@ int ws_create(const ws_config *cfg, ws_solver **out) {
     A(dalloc(&w.half_col, w.cap_half));
     A(dalloc(&w.half_begin, w.cap_half));
     A(dalloc(&w.half_end, w.cap_half));
+    A(dalloc(&w.half_scene, w.cap_half));
     A(dalloc(&w.half_slot_up, w.cap_half));
     A(dalloc(&w.half_slot_lo, w.cap_half));
     A(dalloc(&w.row_cnt_up, w.cap_nodes));

@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_fill(
     const uint32_t *n2t_offset, const uint32_t *n2t_val, const ushort4 *dense_knn, const uint32_t *row_cols,
     const uint32_t *row_cnts, const uint32_t *pair_first, const uint32_t *entry_first, uint32_t cap_half,
     uint32_t cap_kv, uint32_t *half_row, uint32_t *half_col, uint32_t *half_begin, uint32_t *half_end,
-    uint32_t *row_cnt_lo, uint32_t *pair_val, uint32_t *counts, int *err) {
+    uint32_t *half_scene, uint32_t *row_cnt_lo, uint32_t *pair_val, uint32_t *counts, int *err) {
     __shared__ uint32_t s_col[kRowWarps][kRowPairsMax], s_next[kRowWarps][kRowPairsMax];
     __shared__ uint32_t st_col[kRowWarps][kRowStage], st_term[kRowWarps][kRowStage];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -405,6 +405,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_fill(
     const uint32_t warps = gridDim.x * kRowWarps;
     for (uint32_t row = blockIdx.x * kRowWarps + wib; row < total_nodes; row += warps) {
         const uint32_t h0 = pair_first[row], n_cols = pair_first[row + 1] - h0;
+        const uint32_t s = node_scene[row];
         // the row's pairs: columns ascending, entry ranges one after another from the row's first
         uint32_t carry = entry_first[row];
         for (uint32_t k0 = 0; k0 < n_cols; k0 += 32) {
@@ -423,13 +424,13 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_fill(
                     half_col[h] = c;
                     half_begin[h] = begin;
                     half_end[h] = begin + n;
+                    half_scene[h] = s;
                     atomicAdd(&row_cnt_lo[c], 1u);
                 }
             }
         }
         __syncwarp();
         if (n_cols == 0) continue;
-        const uint32_t s = node_scene[row];
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t beg = n2t_offset[row], end = n2t_offset[row + 1];
@@ -615,7 +616,8 @@ static void pair_index(Workspace &w, cudaStream_t st) {
     k_pair_rows_fill<<<grid, 32 * kRowWarps, 0, st>>>(w.scenes, w.plan, w.node_scene, N, w.n2t_offset,
                                                      w.n2t_sorted_val, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
                                                      w.row_pair_first, w.row_entry_first, w.cap_half, w.cap_pair_kv,
-                                                     w.half_row, w.half_col, w.half_begin, w.half_end, w.row_cnt_lo,
+                                                     w.half_row, w.half_col, w.half_begin, w.half_end, w.half_scene,
+                                                     w.row_cnt_lo,
                                                      w.pair_val, w.counts, w.error_flag);
     w.pair_sorted_val = w.pair_val;
     count_launch(w, 1 + 3 + 3 + 1);

@@ -673,9 +673,9 @@ __device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, c
 
 template <int NT, int C>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
-    const Scene *scenes, const Plan *plan, const uint32_t *node_scene, const uint32_t *counts,
+    const Scene *scenes, const Plan *plan, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
-    const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
+    const uint32_t *half_scene, const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
     const float4 *centers, int centred, float *sym_blocks, int *err) {
     constexpr int kSlot = kSlotWordsF32;   // per-lane partial sums at the end
     static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
@@ -692,10 +692,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
     float *mine = slots + lane * kSlot;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nhalf = counts[kCntHalf];
+    // grid-stride: at any time the warps work on neighbouring pairs, whose term records overlap,
+    // so the records are read from DRAM about once and then from L2
     for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < nhalf; h += warps) {
-        if (slot_up[h] == kInvalidIndex) continue;   // capacity overflow, already flagged
-        const uint32_t row = half_row[h], col = half_col[h], beg = half_begin[h], end = half_end[h];
-        const uint32_t s = node_scene[row];
+        // the pair's words in one round of loads (its scene among them), then its slot check
+        const uint32_t slot = slot_up[h], row = half_row[h], col = half_col[h], beg = half_begin[h],
+                       end = half_end[h], s = half_scene[h];
+        if (slot == kInvalidIndex) continue;   // capacity overflow, already flagged
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges;
@@ -2148,7 +2151,8 @@ void gn_assemble_node(Workspace &w, cudaStream_t st) {
 template <int NT, int C>
 static void launch_assemble_pair_c(Workspace &w, cudaStream_t st) {
     k_assemble_pair<NT, C><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
-        w.scenes, w.plan, w.node_scene, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.pair_sorted_val,
+        w.scenes, w.plan, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_scene,
+        w.pair_sorted_val,
         w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.sym_blocks,
         w.error_flag);
 }

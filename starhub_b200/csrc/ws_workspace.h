@@ -76,6 +76,7 @@ struct Workspace {
     const uint32_t *pair_sorted_val = nullptr;
     uint32_t *half_row = nullptr, *half_col = nullptr;       // [cap_half]
     uint32_t *half_begin = nullptr, *half_end = nullptr;
+    uint32_t *half_scene = nullptr;                          // [cap_half] scene of the pair's nodes
     uint32_t *half_slot_up = nullptr, *half_slot_lo = nullptr;
 
     // block CSR
