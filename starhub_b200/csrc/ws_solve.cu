@@ -2201,10 +2201,13 @@ static PcgArgs pcg_args(Workspace &w, int pcg_iters) {
     a.split_group = pcg_split_group(w);
     a.tickets = w.pcg_tickets;
     {
-        // about kPcgBUnitsPerWarp units per warp: two row groups each on the large batches, one on
-        // problems with a warp per group or so
+        // about kPcgBUnitsPerWarp units per warp on problems with a warp per group or so (one row
+        // group each); on the large batches units of whole steps, at least two (64 rows): a unit's
+        // wait, publication and ticket then serve twice the rows
         const uint64_t slots = (uint64_t)kPcgBUnitsPerWarp * pcg_launch_blocks(w) * pcg_warps_per_block();
         a.bunit_groups = (uint32_t)std::max<uint64_t>(1, (w.total_chunks + slots - 1) / slots);
+        const uint32_t step = (uint32_t)kGroupsPerStep;
+        if (a.bunit_groups >= step) a.bunit_groups = std::max(2 * step, (a.bunit_groups + step - 1) / step * step);
     }
     a.sym_blocks = w.sym_blocks;
     a.inv_diag = w.inv_diag;
