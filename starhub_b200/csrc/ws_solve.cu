@@ -851,7 +851,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
 //
 // Rows (nodes) are grouped in scene-aligned groups of kRowsPerGroup.  Phase A (the SpMV) works on
 // units, contiguous ranges of groups balanced by stored blocks (kPcgUnitsPerWarp per warp);
-// phase B on units of bunit_groups row groups (about kPcgBUnitsPerWarp per warp).  The scenes are
+// phase B on units of bunit_groups row groups (about kPcgBUnitsPerWarp per warp on small problems,
+// whole steps of at least 64 rows on large batches).  The scenes are
 // split at a scene boundary into two halves, X and Y, that run half a phase apart: step k of the
 // schedule holds X's phase A of iteration k/2 with Y's phase B of iteration k/2 - 1 (k even), or
 // X's phase B with Y's phase A of iteration (k-1)/2 (k odd), the two parts' units interleaved in
