@@ -460,7 +460,7 @@ template <class DAcc, int NT, int C>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_node(const Scene *scenes, const Plan *plan,
                                                                      const uint32_t *node_scene, uint32_t total_nodes,
                                                                      const uint32_t *n2t_offset, const uint32_t *n2t_val,
-                                                                     const float *drec, const float *rrec,
+                                                                     uint32_t cap_n2t, const float *drec, const float *rrec,
                                                                      const float *se3, const float4 *centers,
                                                                      const uint32_t *item_ptr, uint32_t cap_items,
                                                                      float *sym_blocks, double *diag64, float *jtr,
@@ -482,6 +482,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_node(const Scene *sc
         const uint32_t s = node_scene[g];
         const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
         const float4 c4 = centers[g];
+        if (lane == 0 && end > beg + 32u * kTPL) {
+            // the list past the first batch, into L2 ahead of the later batches' reads (one bulk
+            // prefetch from the 16-byte boundary at or below it, kept inside the list's allocation)
+            const uint32_t a = (beg + 32u * kTPL) & ~3u, stop = min(end, cap_n2t);
+            const uint32_t words = stop > a ? ((stop - a + 3u) & ~3u) : 0u;
+            if (words > 0 && a + words <= cap_n2t)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(n2t_val + a), "r"(4u * words) : "memory");
+        }
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
@@ -1546,6 +1554,51 @@ __device__ __forceinline__ NodeStep node_step(const PcgArgs &A, uint32_t g, uint
     return n;
 }
 
+// Twist update of one node from its PCG step x (ApplyWarpFieldUpdateKernel,
+// examples/mono_star/opt/SolverIterationData.cu:19-74).
+__device__ __forceinline__ void twist_update_row(const PcgArgs &A, uint32_t row, const float *x) {
+    float xv[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) xv[c] = x[c];
+    if (A.fp64) {
+        // node-centred twist -> origin twist: t = t' + c x w
+        const float4 c4 = A.centers[row];
+        const float3 cw = cross3(f3(c4.x, c4.y, c4.z), f3(xv[0], xv[1], xv[2]));
+        xv[3] += cw.x;
+        xv[4] += cw.y;
+        xv[5] += cw.z;
+    }
+    const float3 w = f3(xv[0], xv[1], xv[2]);
+    SE3f inc;
+    if (fabsf(w.x) + fabsf(w.y) + fabsf(w.z) < 1e-4f) {
+        inc.rot = M33{{{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}}};
+    } else {
+        const float angle = sqrtf(w.x * w.x + w.y * w.y + w.z * w.z);
+        const float3 ax = (1.0f / angle) * w;
+        const float c = cosf(angle), sn = sinf(angle), t = 1.0f - c;
+        inc.rot.m[0][0] = t * ax.x * ax.x + c;
+        inc.rot.m[0][1] = t * ax.x * ax.y - ax.z * sn;
+        inc.rot.m[0][2] = t * ax.x * ax.z + ax.y * sn;
+        inc.rot.m[1][0] = t * ax.x * ax.y + ax.z * sn;
+        inc.rot.m[1][1] = t * ax.y * ax.y + c;
+        inc.rot.m[1][2] = t * ax.y * ax.z - ax.x * sn;
+        inc.rot.m[2][0] = t * ax.x * ax.z - ax.y * sn;
+        inc.rot.m[2][1] = t * ax.y * ax.z + ax.x * sn;
+        inc.rot.m[2][2] = t * ax.z * ax.z + c;
+    }
+    inc.t = f3(xv[3], xv[4], xv[5]);
+    const SE3f prev = dq_to_mat34(load_dq(A.se3 + 8ull * row));
+    SE3f nw;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            nw.rot.m[i][j] = inc.rot.m[i][0] * prev.rot.m[0][j] + inc.rot.m[i][1] * prev.rot.m[1][j] +
+                             inc.rot.m[i][2] * prev.rot.m[2][j];
+    nw.t = mul(inc.rot, prev.t) + inc.t;
+    store_dq(A.se3 + 8ull * row, dq_from_mat34(nw));
+}
+
 __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
     extern __shared__ __align__(16) float pcg_smem[];
     const int lane = threadIdx.x & 31;
@@ -1663,6 +1716,9 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
                     store6(A.x + 8ull * n.node, xv);
                     store6(A.r + 8ull * n.node, rv);
                     store6(sd_new + (size_t)kSdStride * n.node, sv);
+                    // x is final after the last iteration: the node's twist update
+                    // (ApplyWarpFieldUpdateKernel, SolverIterationData.cu:19-74) follows at once
+                    if (it + 1 == A.pcg_iters) twist_update_row(A, n.node, xv);
                 }
                 const double part = node_dot_group(A, rv, sv, n.valid);
                 if (lane % kRowsPerGroup == 0 && n.group_ok) A.group_partial[n.gg] = part;
@@ -1672,51 +1728,15 @@ __global__ void __launch_bounds__(kPcgThreads, 3) k_pcg(PcgArgs A) {
         if (lane == 0) ticket = atomicAdd(A.tickets, 1u);
         ticket = __shfl_sync(0xffffffffu, ticket, 0);
     }
-    // x of the warp's rows was last written by whichever warps took their phase-B units
-    if (!wait_scenes(A, b_begin, b_end, 1, (uint32_t)A.pcg_iters + 1u, lane)) return;
-    // ---- twist update of every owned node (ApplyWarpFieldUpdateKernel,
-    //      examples/mono_star/opt/SolverIterationData.cu:19-74) ----
+    // the twist update runs in the last iteration's phase-B units (below, as x is final); with
+    // no PCG iteration it follows init here
+    if (A.pcg_iters > 0) return;
+    if (!wait_scenes(A, b_begin, b_end, 1, 1u, lane)) return;
     for (uint32_t row = br_begin + lane; row < br_end; row += 32) {
         float xv[6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) xv[c] = ldcg(A.x + 8ull * row + c);
-        if (A.fp64) {
-            // node-centred twist -> origin twist: t = t' + c x w
-            const float4 c4 = A.centers[row];
-            const float3 cw = cross3(f3(c4.x, c4.y, c4.z), f3(xv[0], xv[1], xv[2]));
-            xv[3] += cw.x;
-            xv[4] += cw.y;
-            xv[5] += cw.z;
-        }
-        const float3 w = f3(xv[0], xv[1], xv[2]);
-        SE3f inc;
-        if (fabsf(w.x) + fabsf(w.y) + fabsf(w.z) < 1e-4f) {
-            inc.rot = M33{{{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}}};
-        } else {
-            const float angle = sqrtf(w.x * w.x + w.y * w.y + w.z * w.z);
-            const float3 ax = (1.0f / angle) * w;
-            const float c = cosf(angle), sn = sinf(angle), t = 1.0f - c;
-            inc.rot.m[0][0] = t * ax.x * ax.x + c;
-            inc.rot.m[0][1] = t * ax.x * ax.y - ax.z * sn;
-            inc.rot.m[0][2] = t * ax.x * ax.z + ax.y * sn;
-            inc.rot.m[1][0] = t * ax.x * ax.y + ax.z * sn;
-            inc.rot.m[1][1] = t * ax.y * ax.y + c;
-            inc.rot.m[1][2] = t * ax.y * ax.z - ax.x * sn;
-            inc.rot.m[2][0] = t * ax.x * ax.z - ax.y * sn;
-            inc.rot.m[2][1] = t * ax.y * ax.z + ax.x * sn;
-            inc.rot.m[2][2] = t * ax.z * ax.z + c;
-        }
-        inc.t = f3(xv[3], xv[4], xv[5]);
-        const SE3f prev = dq_to_mat34(load_dq(A.se3 + 8ull * row));
-        SE3f nw;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-                nw.rot.m[i][j] = inc.rot.m[i][0] * prev.rot.m[0][j] + inc.rot.m[i][1] * prev.rot.m[1][j] +
-                                 inc.rot.m[i][2] * prev.rot.m[2][j];
-        nw.t = mul(inc.rot, prev.t) + inc.t;
-        store_dq(A.se3 + 8ull * row, dq_from_mat34(nw));
+        twist_update_row(A, row, xv);
     }
 }
 
@@ -2118,7 +2138,7 @@ void gn_eval(Workspace &w, cudaStream_t st) {
 template <class DAcc, int NT, int C>
 static void launch_assemble_node_c(Workspace &w, cudaStream_t st) {
     k_assemble_node<DAcc, NT, C><<<grid_for(w.total_nodes * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
-        w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.d_record, w.r_record, w.se3,
+        w.scenes, w.plan, w.node_scene, w.total_nodes, w.n2t_offset, w.n2t_sorted_val, w.cap_n2t, w.d_record, w.r_record, w.se3,
         w.centers, w.item_ptr, w.cap_items, w.sym_blocks, w.diag64, w.jtr, w.error_flag);
 }
 
