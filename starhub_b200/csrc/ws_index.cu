@@ -240,6 +240,15 @@ constexpr int kRowWarps = 4;         // warps per block of the two row passes
 constexpr int kRowLanesEntries = 4;  // list entries per lane and pass (loads in flight)
 constexpr int kRowChunk = 32 * kRowLanesEntries;   // list entries per pass
 constexpr int kRowStage = 3 * kRowChunk;           // their candidates (at most 3 each)
+
+// One lane asks L2 for entries [from, to) of a node->term list of `cap` words: one bulk prefetch
+// from the 16-byte boundary at or below `from`, kept inside the allocation.
+__device__ __forceinline__ void l2_prefetch_list(const uint32_t *list, uint32_t from, uint32_t to, uint32_t cap) {
+    const uint32_t a = from & ~3u, stop = min(to, cap);
+    const uint32_t words = stop > a ? ((stop - a + 3u) & ~3u) : 0u;
+    if (words > 0 && a + words <= cap)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(list + a), "r"(4u * words) : "memory");
+}
 constexpr uint32_t kNoCol = 0xFFFFFFFFu;
 
 // The columns above `row` that list entry `t` (scene-local term id) adds to row `row`'s pairs, in
@@ -307,7 +316,7 @@ __device__ __forceinline__ uint32_t col_hash(uint32_t c) { return (c * 265443576
 
 __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_count(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, uint32_t total_nodes,
-    const uint32_t *n2t_offset, const uint32_t *n2t_val, const ushort4 *dense_knn, uint32_t *row_cols,
+    const uint32_t *n2t_offset, const uint32_t *n2t_val, uint32_t cap_n2t, const ushort4 *dense_knn, uint32_t *row_cols,
     uint32_t *row_cnts, uint32_t *row_pairs, uint32_t *row_entries, int *err) {
     static_assert(kRowHash == 128, "col_hash gives 7 bits");
     __shared__ uint32_t hkey[kRowWarps][kRowHash], hcnt[kRowWarps][kRowHash];
@@ -327,6 +336,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_count(
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t beg = n2t_offset[row], end = n2t_offset[row + 1];
+        if (lane == 0 && end > beg + kRowChunk) l2_prefetch_list(n2t_val, beg + kRowChunk, end, cap_n2t);
         bool full = false;
         for (uint32_t base = beg; base < end; base += kRowChunk) {
             const uint32_t total =
@@ -390,7 +400,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_count(
 
 __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_fill(
     const Scene *scenes, const Plan *plan, const uint32_t *node_scene, uint32_t total_nodes,
-    const uint32_t *n2t_offset, const uint32_t *n2t_val, const ushort4 *dense_knn, const uint32_t *row_cols,
+    const uint32_t *n2t_offset, const uint32_t *n2t_val, uint32_t cap_n2t, const ushort4 *dense_knn, const uint32_t *row_cols,
     const uint32_t *row_cnts, const uint32_t *pair_first, const uint32_t *entry_first, uint32_t cap_half,
     uint32_t cap_kv, uint32_t *half_row, uint32_t *half_col, uint32_t *half_begin, uint32_t *half_end,
     uint32_t *half_scene, uint32_t *row_cnt_lo, uint32_t *pair_val, uint32_t *counts, int *err) {
@@ -434,6 +444,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_pair_rows_fill(
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t beg = n2t_offset[row], end = n2t_offset[row + 1];
+        if (lane == 0 && end > beg + kRowChunk) l2_prefetch_list(n2t_val, beg + kRowChunk, end, cap_n2t);
         for (uint32_t base = beg; base < end; base += kRowChunk) {
             const uint32_t total =
                 stage_row_candidates(sc, p, dense_knn, n2t_val, row, base, end, st_col[wib], st_term[wib], lane, err);
@@ -608,13 +619,13 @@ static void pair_index(Workspace &w, cudaStream_t st) {
     const uint32_t N = w.total_nodes;
     const int grid = grid_for(N * 32u, 32 * kRowWarps, w.num_sms);
     k_pair_rows_count<<<grid, 32 * kRowWarps, 0, st>>>(w.scenes, w.plan, w.node_scene, N, w.n2t_offset,
-                                                      w.n2t_sorted_val, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
+                                                      w.n2t_sorted_val, w.cap_n2t, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
                                                       w.row_cnt_up, w.row_entry_first, w.error_flag);
     exclusive_scan(w.row_cnt_up, w.row_pair_first, nullptr, N, w.cap_nodes, w.scan_tmp, st);
     exclusive_scan(w.row_entry_first, w.row_entry_first, nullptr, N, w.cap_nodes, w.scan_tmp, st);
     cudaMemsetAsync(w.row_cnt_lo, 0, sizeof(uint32_t) * w.cap_nodes, st);
     k_pair_rows_fill<<<grid, 32 * kRowWarps, 0, st>>>(w.scenes, w.plan, w.node_scene, N, w.n2t_offset,
-                                                     w.n2t_sorted_val, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
+                                                     w.n2t_sorted_val, w.cap_n2t, w.d_knn, w.row_pair_cols, w.row_pair_cnts,
                                                      w.row_pair_first, w.row_entry_first, w.cap_half, w.cap_pair_kv,
                                                      w.half_row, w.half_col, w.half_begin, w.half_end, w.half_scene,
                                                      w.row_cnt_lo,
