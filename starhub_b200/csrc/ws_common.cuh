@@ -78,6 +78,15 @@ struct Plan {
     uint32_t pad[2];
 };
 
+// One lane asks L2 for entries [from, to) of a list of `cap` 4-byte words (a term list): one bulk
+// prefetch from the 16-byte boundary at or below `from`, kept inside the list's allocation.
+__device__ __forceinline__ void l2_prefetch_list(const uint32_t *list, uint32_t from, uint32_t to, uint32_t cap) {
+    const uint32_t a = from & ~3u, stop = min(to, cap);
+    const uint32_t words = stop > a ? ((stop - a + 3u) & ~3u) : 0u;
+    if (words > 0 && a + words <= cap)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(list + a), "r"(4u * words) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Small math (FP32 as in the reference; libs/star/math/*).
 // ---------------------------------------------------------------------------

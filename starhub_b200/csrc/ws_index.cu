@@ -241,14 +241,6 @@ constexpr int kRowLanesEntries = 4;  // list entries per lane and pass (loads in
 constexpr int kRowChunk = 32 * kRowLanesEntries;   // list entries per pass
 constexpr int kRowStage = 3 * kRowChunk;           // their candidates (at most 3 each)
 
-// One lane asks L2 for entries [from, to) of a node->term list of `cap` words: one bulk prefetch
-// from the 16-byte boundary at or below `from`, kept inside the allocation.
-__device__ __forceinline__ void l2_prefetch_list(const uint32_t *list, uint32_t from, uint32_t to, uint32_t cap) {
-    const uint32_t a = from & ~3u, stop = min(to, cap);
-    const uint32_t words = stop > a ? ((stop - a + 3u) & ~3u) : 0u;
-    if (words > 0 && a + words <= cap)
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(list + a), "r"(4u * words) : "memory");
-}
 constexpr uint32_t kNoCol = 0xFFFFFFFFu;
 
 // The columns above `row` that list entry `t` (scene-local term id) adds to row `row`'s pairs, in

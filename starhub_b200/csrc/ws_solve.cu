@@ -482,14 +482,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_node(const Scene *sc
         const uint32_t s = node_scene[g];
         const uint32_t beg = n2t_offset[g], end = n2t_offset[g + 1];
         const float4 c4 = centers[g];
-        if (lane == 0 && end > beg + 32u * kTPL) {
-            // the list past the first batch, into L2 ahead of the later batches' reads (one bulk
-            // prefetch from the 16-byte boundary at or below it, kept inside the list's allocation)
-            const uint32_t a = (beg + 32u * kTPL) & ~3u, stop = min(end, cap_n2t);
-            const uint32_t words = stop > a ? ((stop - a + 3u) & ~3u) : 0u;
-            if (words > 0 && a + words <= cap_n2t)
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(n2t_val + a), "r"(4u * words) : "memory");
-        }
+        // the list past the first batch, into L2 ahead of the later batches' reads
+        if (lane == 0 && end > beg + 32u * kTPL) l2_prefetch_list(n2t_val, beg + 32u * kTPL, end, cap_n2t);
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
         const uint32_t nd = p.dense_count, ne = sc.num_edges, nn = sc.num_nodes;
@@ -683,7 +677,7 @@ template <int NT, int C>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *counts,
     const uint32_t *half_row, const uint32_t *half_col, const uint32_t *half_begin, const uint32_t *half_end,
-    const uint32_t *half_scene, const uint32_t *pair_val, const uint32_t *slot_up, const float *drec, const float *rrec,
+    const uint32_t *half_scene, const uint32_t *pair_val, uint32_t cap_kv, const uint32_t *slot_up, const float *drec, const float *rrec,
     const float4 *centers, int centred, float *sym_blocks, int *err) {
     constexpr int kSlot = kSlotWordsF32;   // per-lane partial sums at the end
     static_assert(kSlot >= 36, "a slot holds one lane's 36 partial sums");
@@ -706,6 +700,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
         // the pair's words in one round of loads (its scene among them), then its slot check
         const uint32_t slot = slot_up[h], row = half_row[h], col = half_col[h], beg = half_begin[h],
                        end = half_end[h], s = half_scene[h];
+        // the term list of this warp's next pair, into L2 a pair ahead (its bounds come with this
+        // pair's words)
+        uint32_t next_beg = 0, next_end = 0;
+        if (lane == 0 && h + warps < nhalf) {
+            next_beg = half_begin[h + warps];
+            next_end = half_end[h + warps];
+        }
+        if (lane == 0 && next_end > next_beg) l2_prefetch_list(pair_val, next_beg, next_end, cap_kv);
         if (slot == kInvalidIndex) continue;   // capacity overflow, already flagged
         const Scene &sc = scenes[s];
         const Plan &p = plan[s];
@@ -2173,7 +2175,7 @@ template <int NT, int C>
 static void launch_assemble_pair_c(Workspace &w, cudaStream_t st) {
     k_assemble_pair<NT, C><<<grid_for(w.cap_half * 32u, NT, w.num_sms, 32 * 128 / NT), NT, 0, st>>>(
         w.scenes, w.plan, w.counts, w.half_row, w.half_col, w.half_begin, w.half_end, w.half_scene,
-        w.pair_sorted_val,
+        w.pair_sorted_val, w.cap_pair_kv,
         w.half_slot_up, w.d_record, w.r_record, w.centers, w.precision == WS_PREC_MIXED ? 1 : 0, w.sym_blocks,
         w.error_flag);
 }
