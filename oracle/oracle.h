@@ -148,6 +148,17 @@ int orc_render_solver_maps(const float *vertex_confid4, const float *normal_radi
                            const float *world2camera, float max_depth, float current_time,
                            float conf_threshold, float time_threshold, int footprint, uint32_t *index_map,
                            float *vertex4, float *normal4, float *rgbd4);
+/* The observation-map pass (Renderer::DrawObservationMaps, libs/star/geometry/render/
+ * RendererDraw.cu:353-394, shaders/geometry.vert:40-86 and observation_map.frag:13-17): the same
+ * camera transform, confidence/time cull and depth rule as the solver-map pass (drawn iff
+ * 0 < z < max depth), but each surfel is a GL point whose size is the smaller image extent of its
+ * disk (four points v_cam +- x1, +- y1 of radius * 1.41421356 mm), clamped to [1, 2047]; it covers
+ * the pixels i with u - S/2 < i <= u + S/2 around u = f x / z + c (rows likewise).  Outputs
+ * width*height texels: index (0xFFFFFFFF = none) and rgbd ((colour / 255) * 2 - 1, 1 / z). */
+int orc_render_observation_maps(const float *vertex_confid4, const float *normal_radius4, const float *color_time4,
+                                int n, int width, int height, float fx, float fy, float cx, float cy,
+                                const float *world2camera, float max_depth, float current_time,
+                                float conf_threshold, float time_threshold, uint32_t *index_map, float *rgbd4);
 
 #ifdef __cplusplus
 }

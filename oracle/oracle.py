@@ -368,6 +368,24 @@ def render_solver_maps(vertex_confid, normal_radius, color_time, cam, world2came
     return idx, vert, nrm, rgbd
 
 
+def render_observation_maps(vertex_confid, normal_radius, color_time, cam, world2camera, max_depth, current_time,
+                            conf_threshold=1.0, time_threshold=3.0):
+    """orc_render_observation_maps: (index (H, W) uint32, rgbd (H, W, 4) float32)."""
+    vc = _c(vertex_confid, np.float32)
+    nr = _c(normal_radius, np.float32)
+    ct = _c(color_time, np.float32) if color_time is not None else None
+    m = _c(np.asarray(world2camera, np.float32).reshape(16), np.float32)
+    h, w = cam.height, cam.width
+    idx = np.zeros((h, w), np.uint32)
+    rgbd = np.zeros((h, w, 4), np.float32)
+    rc = lib().orc_render_observation_maps(_p(vc), _p(nr), _p(ct), C.c_int(vc.shape[0]), C.c_int(w), C.c_int(h),
+                                           C.c_float(cam.fx), C.c_float(cam.fy), C.c_float(cam.cx),
+                                           C.c_float(cam.cy), _p(m), C.c_float(max_depth), C.c_float(current_time),
+                                           C.c_float(conf_threshold), C.c_float(time_threshold), _p(idx), _p(rgbd))
+    assert rc == 0
+    return idx, rgbd
+
+
 def measure_maps(depth_mm, fx, fy, cx, cy, clip_near=0.1, clip_far=3.0, radius_scale=1.0):
     """orc_measure_maps: vertex and normal/radius maps, two (H, W, 4) float32 arrays."""
     d = _c(depth_mm, np.uint16)

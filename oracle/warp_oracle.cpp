@@ -1613,3 +1613,115 @@ int orc_render_solver_maps(const float *vc4, const float *nr4, const float *ct4,
     }
     return 0;
 }
+
+// Renderer::DrawObservationMaps (libs/star/geometry/render/RendererDraw.cu:353-394): every surfel
+// drawn as a GL point with shaders/geometry.vert:40-86 and observation_map.frag:13-17, with
+// GL_PROGRAM_POINT_SIZE on (Renderer.cu:87-90), so each surfel's point size comes from its disk.
+// Restated per surfel, every operation rounded as written:
+//   * v_cam = world2camera (v, 1) as in the solver-map pass; culled when z > max depth or z < 0
+//     (geometry.vert:42-44) or unstable and not recent; z = 0 projects to infinity and z = max
+//     depth fails the depth test against the far plane, so a surfel is drawn iff 0 < z < max depth;
+//   * n_c = normalize(R n) with R the rotation rows of world2camera (mat3(world2camera)), where
+//     normalize(a) = a / sqrt((a.x a.x + a.y a.y) + a.z a.z);
+//   * x1 = ((normalize(n_c.y - n_c.z, -n_c.x, n_c.x) * radius) * 1.41421356) * 0.001, y1 = n_c x x1;
+//     the four points v_cam + x1, v_cam + y1, v_cam - y1, v_cam - x1 in image coordinates
+//     ((f p.x) / p.z + c); the point size is min(x extent, y extent), at least 0 (a non-finite
+//     extent counts as 0), clamped to GL's aliased point-size range [1, 2047];
+//   * window position u = (f x) / z + c plus the shader's 0.5 shift; a pixel is covered when its
+//     centre lies in the point's square, taken half-open so that a unit point covers exactly the
+//     solver-map pixel floor(u + 0.5): columns i with u - S/2 < i <= u + S/2, rows likewise;
+//   * nearest z wins, equal z keeps the lower id (GL_LESS, drawn in id order);
+//   * outputs: index (surfel id, clear 0xFFFFFFFF) and rgbd = ((colour byte / 255) * 2 - 1 for
+//     r, g, b; 1 / z), clear zeros (GLClearValues.h:14-33).
+static inline void obs_normalize(const float a[3], float out[3]) {
+    const float len = std::sqrt((a[0] * a[0] + a[1] * a[1]) + a[2] * a[2]);
+    out[0] = a[0] / len;
+    out[1] = a[1] / len;
+    out[2] = a[2] / len;
+}
+
+int orc_render_observation_maps(const float *vc4, const float *nr4, const float *ct4, int n, int W, int H, float fx,
+                                float fy, float cx, float cy, const float *m, float max_depth, float current_time,
+                                float conf_threshold, float time_threshold, uint32_t *index_map, float *rgbd4) {
+    if (n < 0 || W <= 0 || H <= 0) return -1;
+    const size_t npix = (size_t)W * H;
+    std::vector<float> best_z(npix, 0.f);
+    std::vector<int64_t> best_id(npix, -1);
+    std::vector<float> surfel_z((size_t)std::max(n, 1), 0.f);
+    for (int i = 0; i < n; ++i) {
+        const float *v = vc4 + 4ull * i;
+        const float x = ((m[0] * v[0] + m[1] * v[1]) + m[2] * v[2]) + m[3];
+        const float y = ((m[4] * v[0] + m[5] * v[1]) + m[6] * v[2]) + m[7];
+        const float z = ((m[8] * v[0] + m[9] * v[1]) + m[10] * v[2]) + m[11];
+        surfel_z[i] = z;
+        if (!(z > 0.f) || !(z < max_depth)) continue;
+        const float t = ct4 ? ct4[4ull * i + 2] : current_time;
+        if (v[3] < conf_threshold && std::fabs(t - current_time) >= time_threshold) continue;
+        // the point size from the surfel's disk (geometry.vert:64-78)
+        const float *nw = nr4 + 4ull * i;
+        const float rn[3] = {(m[0] * nw[0] + m[1] * nw[1]) + m[2] * nw[2], (m[4] * nw[0] + m[5] * nw[1]) + m[6] * nw[2],
+                             (m[8] * nw[0] + m[9] * nw[1]) + m[10] * nw[2]};
+        float nc[3], dir[3];
+        obs_normalize(rn, nc);
+        const float d0[3] = {nc[1] - nc[2], -nc[0], nc[0]};
+        obs_normalize(d0, dir);
+        float x1[3], y1[3];
+        for (int k = 0; k < 3; ++k) x1[k] = ((dir[k] * nw[3]) * 1.41421356f) * 0.001f;
+        y1[0] = nc[1] * x1[2] - nc[2] * x1[1];
+        y1[1] = nc[2] * x1[0] - nc[0] * x1[2];
+        y1[2] = nc[0] * x1[1] - nc[1] * x1[0];
+        const float vcam[3] = {x, y, z};
+        float px[4], py[4];
+        for (int k = 0; k < 4; ++k) {
+            const float *off = (k == 0 || k == 3) ? x1 : y1;
+            const float sgn = (k == 0 || k == 1) ? 1.f : -1.f;
+            const float p0 = sgn > 0.f ? vcam[0] + off[0] : vcam[0] - off[0];
+            const float p1 = sgn > 0.f ? vcam[1] + off[1] : vcam[1] - off[1];
+            const float p2 = sgn > 0.f ? vcam[2] + off[2] : vcam[2] - off[2];
+            px[k] = (fx * p0) / p2 + cx;
+            py[k] = (fy * p1) / p2 + cy;
+        }
+        float xmin = px[0], xmax = px[0], ymin = py[0], ymax = py[0];
+        for (int k = 1; k < 4; ++k) {
+            xmin = std::min(xmin, px[k]);
+            xmax = std::max(xmax, px[k]);
+            ymin = std::min(ymin, py[k]);
+            ymax = std::max(ymax, py[k]);
+        }
+        const float xd = std::fabs(xmax - xmin), yd = std::fabs(ymax - ymin);
+        float size = xd < yd ? xd : yd;
+        if (!(size > 0.f)) size = 0.f;   // a non-finite or negative extent
+        size = std::min(std::max(size, 1.f), 2047.f);
+        const float half = 0.5f * size;
+        const float u = (fx * x) / z + cx, w = (fy * y) / z + cy;
+        const float lo_x = std::floor(u - half) + 1.f, hi_x = std::floor(u + half);
+        const float lo_y = std::floor(w - half) + 1.f, hi_y = std::floor(w + half);
+        if (!(hi_x >= 0.f && lo_x <= (float)(W - 1) && hi_y >= 0.f && lo_y <= (float)(H - 1))) continue;
+        const int x0 = (int)std::max(lo_x, 0.f), x1i = (int)std::min(hi_x, (float)(W - 1));
+        const int y0 = (int)std::max(lo_y, 0.f), y1i = (int)std::min(hi_y, (float)(H - 1));
+        for (int qy = y0; qy <= y1i; ++qy)
+            for (int qx = x0; qx <= x1i; ++qx) {
+                const size_t q = (size_t)qy * W + qx;
+                if (best_id[q] < 0 || z < best_z[q]) { best_z[q] = z; best_id[q] = i; }
+            }
+    }
+    for (size_t q = 0; q < npix; ++q) {
+        float *ro = rgbd4 ? rgbd4 + 4 * q : nullptr;
+        if (best_id[q] < 0) {
+            index_map[q] = 0xFFFFFFFFu;
+            if (ro) ro[0] = ro[1] = ro[2] = ro[3] = 0.f;
+            continue;
+        }
+        const size_t id = (size_t)best_id[q];
+        index_map[q] = (uint32_t)id;
+        if (ro) {
+            int32_t enc = 0;
+            if (ct4) std::memcpy(&enc, ct4 + 4 * id, 4);   // floatBitsToInt(color_time.x)
+            ro[0] = ((float)((enc & 0x00FF0000) >> 16) / 255.f) * 2.0f - 1.0f;
+            ro[1] = ((float)((enc & 0x0000FF00) >> 8) / 255.f) * 2.0f - 1.0f;
+            ro[2] = ((float)(enc & 0x000000FF) / 255.f) * 2.0f - 1.0f;
+            ro[3] = 1.0f / surfel_z[id];
+        }
+    }
+    return 0;
+}

@@ -289,3 +289,41 @@ def test_render_solver_maps_rules(orc):
     idx2, _, _, _ = orc.render_solver_maps(vc, nr, ct, cam, np.eye(4), max_depth=2.0, current_time=10.0,
                                            time_threshold=-1.0)
     assert (idx2 != 0xFFFFFFFF).sum() == 1
+
+
+def test_render_observation_maps_rules(orc):
+    """The oracle's restatement of the observation-map pass (geometry.vert:40-86 with
+    observation_map.frag:13-17): a surfel facing the camera is a point as wide as its disk's image
+    (radius 106 mm at 1 m and f = 10: about 3 pixels, so a 3 x 3 square), a tiny surfel still draws
+    one pixel (GL's minimum point size), the nearer surfel wins, the culls are the solver map's,
+    and the colour is (byte / 255) * 2 - 1 with 1 / z beside it."""
+    from starhub_b200.scenes import Camera
+    cam = Camera(16, 12, 10.0, 10.0, 8.0, 6.0)
+    vc = np.array([[0.0, 0.0, 1.0, 5.0],      # 0: 3 x 3 square around pixel (8, 6)
+                   [0.2, 0.0, 1.0, 5.0],      # 1: tiny, pixel (10, 6)
+                   [0.0, 0.0, 0.5, 5.0],      # 2: tiny and nearer: wins (8, 6)
+                   [0.0, 0.0, -1.0, 5.0],     # 3: behind the camera: culled
+                   [0.1, 0.0, 3.0, 5.0],      # 4: z = max depth: culled
+                   [-0.3, 0.0, 1.0, 0.5],     # 5: unstable, observed at t = 2: culled
+                   [0.3, 0.2, 1.0, 0.5]],     # 6: unstable, observed at t = 9: pixel (11, 8)
+                  np.float32)
+    nr = np.tile(np.array([[0, 0, -1, 1.0]], np.float32), (len(vc), 1))
+    nr[0, 3] = 106.0
+    ct = np.zeros((len(vc), 4), np.float32)
+    ct[:, 2] = [10, 10, 10, 10, 10, 2, 9]
+    ct[0, 0] = np.array([0x00FF0080], np.int32).view(np.float32)[0]   # colour bytes (255, 0, 128)
+    idx, rgbd = orc.render_observation_maps(vc, nr, ct, cam, np.eye(4), max_depth=3.0, current_time=10.0)
+    want = np.full((12, 16), 0xFFFFFFFF, np.uint32)
+    want[5:8, 7:10] = 0
+    want[6, 8] = 2
+    want[6, 10] = 1
+    want[8, 11] = 6
+    np.testing.assert_array_equal(idx, want)
+    third = np.float32(np.float32(128) / np.float32(255)) * np.float32(2) - np.float32(1)
+    np.testing.assert_array_equal(rgbd[5, 7], np.array([1.0, -1.0, third, 1.0], np.float32))
+    assert rgbd[6, 8, 3] == np.float32(2.0)
+    assert (rgbd[idx == 0xFFFFFFFF] == 0).all()
+    # without the recent-observation pass the unstable surfel 6 goes too
+    idx2, _ = orc.render_observation_maps(vc, nr, ct, cam, np.eye(4), max_depth=3.0, current_time=10.0,
+                                          time_threshold=-1.0)
+    assert idx2[8, 11] == 0xFFFFFFFF and (idx2 != 0xFFFFFFFF).sum() == 10
