@@ -272,6 +272,20 @@ typedef struct ws_render_params {
 int ws_render_solver_maps(const float *vertex_confid, const float *normal_radius, const float *color_time,
                           int num_surfels, const ws_render_params *params, uint32_t *index_map, float *vertex_map,
                           float *normal_map, float *rgbd_map, void *stream);
+/* Observation maps as Renderer::DrawObservationMaps (libs/star/geometry/render/RendererDraw.cu:353-394)
+ * draws them with shaders/geometry.vert:40-86 and observation_map.frag:13-17, with
+ * GL_PROGRAM_POINT_SIZE on (Renderer.cu:87-90).  Same inputs, transform, culls and depth rule as
+ * ws_render_solver_maps (drawn iff 0 < z < max_depth and not an unstable surfel outside the time
+ * threshold; nearest z, equal depths to the lower id), but normal_radius is required and each
+ * surfel is a point as wide as its disk's image: the smaller image extent of the four points
+ * v_cam +- x1, v_cam +- y1 (x1 = normalize(n.y - n.z, -n.x, n.x) * radius * 1.41421356 mm in the
+ * camera frame, y1 = n x x1), clamped to [1, 2047]; it covers the pixels i with
+ * u - S/2 < i <= u + S/2 around u = f x / z + c (rows likewise).  params->footprint is unused.
+ * Writes width*height texels: index (surfel id, 0xFFFFFFFF = none) and, when rgbd_map is not
+ * NULL, rgbd = ((colour byte / 255) * 2 - 1 for r, g, b; 1 / z); empty texels are zero. */
+int ws_render_observation_maps(const float *vertex_confid, const float *normal_radius, const float *color_time,
+                               int num_surfels, const ws_render_params *params, uint32_t *index_map, float *rgbd_map,
+                               void *stream);
 /* Measurement maps from a depth image in millimetres (device, `pitch` elements per row):
  * createVertexConfidMapKernel (libs/star/img_proc/vertex_map.cu:13-33), the depth clip of
  * filterAndScaleVertexKernel (libs/star/geometry/geometry_map/SurfelMapInitializer.cu:107-137,

@@ -37,6 +37,7 @@ EXPORTED = [
     "ws_server_remove_scene", "ws_submit", "ws_poll", "ws_wait", "ws_server_forget", "ws_server_get_warp",
     "ws_server_copy_warp", "ws_server_set_warp", "ws_server_get_stats", "ws_spmv", "ws_spmv_matrix_free", "ws_autotune",
     "ws_selftest_wait_timeout", "ws_selftest_grid_barrier_timeout", "ws_render_solver_maps",
+    "ws_render_observation_maps",
     "ws_build_node_graph_ex", "ws_skinning_ex", "ws_skinning_incremental",
     "ws_set_tuning",
 ]
@@ -185,6 +186,7 @@ def load() -> C.CDLL:
         "ws_selftest_wait_timeout": (i, [vp]),
         "ws_selftest_grid_barrier_timeout": (i, [vp]),
         "ws_render_solver_maps": (i, [vp, vp, vp, i, C.POINTER(WsRenderParams), vp, vp, vp, vp, vp]),
+        "ws_render_observation_maps": (i, [vp, vp, vp, i, C.POINTER(WsRenderParams), vp, vp, vp]),
         "ws_build_node_graph_ex": (i, [vp, vp, i, i, f, i, vp, vp, vp, vp]),
         "ws_skinning_ex": (i, [vp, vp, i, vp, i, f, i, vp, vp, vp, vp]),
         "ws_skinning_incremental": (i, [vp, vp, i, i, vp, i, i, f, i, vp, vp, vp, vp]),

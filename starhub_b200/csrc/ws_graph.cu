@@ -17,6 +17,7 @@
 
 #include "../../include/warpsolve.h"
 #include "ws_common.cuh"
+#include "ws_obs_point.cuh"
 #include "ws_prims.cuh"
 
 namespace ws {
@@ -681,6 +682,48 @@ __global__ void k_render_resolve(const unsigned long long *zbuf, int npix, const
     }
 }
 
+// ---- Observation maps as the reference's observation-map pass draws them ----------------------
+// Renderer::DrawObservationMaps (libs/star/geometry/render/RendererDraw.cu:353-394) with
+// shaders/geometry.vert:40-86 and observation_map.frag:13-17: the same transform, culls and depth
+// rule as the solver-map pass, but each surfel is a GL point as wide as its disk's image
+// (obs_point in ws_obs_point.cuh, shared with the host check of the tests).  One thread per
+// surfel offers its (z bits, id) key to every pixel of its clipped rectangle; the smallest key
+// wins, so the nearest z wins and equal depths keep the lower id (GL_LESS in draw order).
+__global__ void k_obs_keys(const float4 *vc, const float4 *nr, const float4 *ct, int n, RenderArgs a,
+                           unsigned long long *zbuf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 v4 = vc[i], n4 = nr[i];
+        const float v[4] = {v4.x, v4.y, v4.z, v4.w}, nw[4] = {n4.x, n4.y, n4.z, n4.w};
+        const float t = ct ? ct[i].z : a.current_time;
+        const ObsCover c = obs_point(v, nw, t, a.m, a.fx, a.fy, a.cx, a.cy, a.W, a.H, a.max_depth, a.current_time,
+                                     a.conf_threshold, a.time_threshold);
+        if (!c.drawn) continue;
+        // z > 0 here, so its bits order like its value
+        const unsigned long long key = ((unsigned long long)__float_as_uint(c.z) << 32) | (unsigned)i;
+        for (int qy = c.y0; qy <= c.y1; ++qy)   // inside the image: obs_point clips the rectangle
+            for (int qx = c.x0; qx <= c.x1; ++qx) atomicMin(zbuf + (size_t)qy * a.W + qx, key);
+    }
+}
+
+__global__ void k_obs_resolve(const unsigned long long *zbuf, int npix, const float4 *ct, uint32_t *index,
+                              float4 *rgbd) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const unsigned long long k = zbuf[p];
+        if (k == ~0ull) {   // the clear values (GLClearValues.h:26-33)
+            index[p] = kInvalidIndex;
+            if (rgbd) rgbd[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const uint32_t id = (uint32_t)(k & 0xffffffffu);
+        index[p] = id;
+        if (rgbd) {
+            float o[4];
+            obs_rgbd(ct ? __float_as_int(ct[id].x) : 0, __uint_as_float((uint32_t)(k >> 32)), o);
+            rgbd[p] = make_float4(o[0], o[1], o[2], o[3]);
+        }
+    }
+}
+
 // Scratch of ws_splat_maps_noalloc: one depth/id key per pixel of the largest supported
 // image, in the module's static device memory (no allocation at call time).
 static __device__ __align__(256) unsigned long long g_noalloc_zbuf[WS_NOALLOC_MAX_PIXELS];
@@ -1055,6 +1098,38 @@ int ws_render_solver_maps(const float *vertex_confid, const float *normal_radius
     ws::k_render_resolve<<<ws::grid_of((long long)npix, 256), 256, 0, st>>>(
         zbuf, (int)npix, vc, reinterpret_cast<const float4 *>(normal_radius), ct, index_map,
         reinterpret_cast<float4 *>(vertex_map), reinterpret_cast<float4 *>(normal_map), reinterpret_cast<float4 *>(rgbd_map));
+    cudaFreeAsync(zbuf, st);
+    return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+}
+
+
+int ws_render_observation_maps(const float *vertex_confid, const float *normal_radius, const float *color_time,
+                               int num_surfels, const ws_render_params *params, uint32_t *index_map, float *rgbd_map,
+                               void *stream) {
+    if (!params || !vertex_confid || !normal_radius || num_surfels < 0 || !index_map) return WS_ERR_INVALID_ARGUMENT;
+    const ws_render_params &p = *params;
+    if (p.width <= 0 || p.height <= 0 || !(p.max_depth > 0.f)) return WS_ERR_INVALID_ARGUMENT;
+    ws::RenderArgs a;
+    a.W = p.width; a.H = p.height; a.fp = 0;
+    a.fx = p.fx; a.fy = p.fy; a.cx = p.cx; a.cy = p.cy;
+    a.max_depth = p.max_depth; a.current_time = p.current_time;
+    a.conf_threshold = p.confidence_threshold; a.time_threshold = p.time_threshold;
+    for (int q = 0; q < 12; ++q) a.m[q] = p.world2camera[q];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t npix = (size_t)p.width * p.height;
+    unsigned long long *zbuf = nullptr;
+    if (cudaMallocAsync(&zbuf, 8 * npix, st) != cudaSuccess) return WS_ERR_CUDA;
+    if (cudaMemsetAsync(zbuf, 0xff, 8 * npix, st) != cudaSuccess) {
+        cudaFreeAsync(zbuf, st);
+        return WS_ERR_CUDA;
+    }
+    const float4 *ct = reinterpret_cast<const float4 *>(color_time);
+    if (num_surfels > 0)
+        ws::k_obs_keys<<<ws::grid_of(num_surfels, 256), 256, 0, st>>>(
+            reinterpret_cast<const float4 *>(vertex_confid), reinterpret_cast<const float4 *>(normal_radius), ct,
+            num_surfels, a, zbuf);
+    ws::k_obs_resolve<<<ws::grid_of((long long)npix, 256), 256, 0, st>>>(zbuf, (int)npix, ct, index_map,
+                                                                          reinterpret_cast<float4 *>(rgbd_map));
     cudaFreeAsync(zbuf, st);
     return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
 }

@@ -461,6 +461,26 @@ class GpuGeometry:
               "ws_render_solver_maps")
         return (idx.cpu().numpy().view(np.uint32),) + tuple(m.cpu().numpy() for m in maps)
 
+    def render_observation_maps(self, vertex_confid, normal_radius, color_time, cam, world2camera, max_depth,
+                                current_time, conf_threshold=1.0, time_threshold=3.0):
+        """ws_render_observation_maps: (index (H, W) uint32, rgbd (H, W, 4) float32)."""
+        from ._lib import WsRenderParams
+        vc = _dev(vertex_confid, self.device, torch.float32)
+        nr = _dev(normal_radius, self.device, torch.float32)
+        ct = _dev(color_time, self.device, torch.float32)
+        p = WsRenderParams()
+        p.width, p.height = cam.width, cam.height
+        p.fx, p.fy, p.cx, p.cy = cam.fx, cam.fy, cam.cx, cam.cy
+        p.world2camera[:] = [float(v) for v in np.asarray(world2camera, np.float32).reshape(-1)]
+        p.max_depth, p.current_time = max_depth, current_time
+        p.confidence_threshold, p.time_threshold, p.footprint = conf_threshold, time_threshold, 0
+        idx = torch.empty((cam.height, cam.width), dtype=torch.int32, device=self.device)
+        rgbd = torch.empty((cam.height, cam.width, 4), dtype=torch.float32, device=self.device)
+        check(self.lib.ws_render_observation_maps(_ptr(vc), _ptr(nr), _ptr(ct), int(vc.shape[0]), C.byref(p),
+                                                  _ptr(idx), _ptr(rgbd), self._stream()),
+              "ws_render_observation_maps")
+        return idx.cpu().numpy().view(np.uint32), rgbd.cpu().numpy()
+
     def splat(self, verts, cam, footprint):
         v = _dev(verts, self.device, torch.float32)
         idx = torch.empty((cam.height, cam.width), dtype=torch.int32, device=self.device)
