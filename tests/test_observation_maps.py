@@ -71,7 +71,7 @@ def _run_host(lib, vc, nr, ct, cam, w2c, max_depth, now, conf, tthr):
     idx = np.zeros((h, w), np.uint32)
     rgbd = np.zeros((h, w, 4), np.float32)
     m = np.ascontiguousarray(np.asarray(w2c, np.float32).reshape(16))
-    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
     rc = lib.obs_maps_host(p(vc), p(nr), p(ct), C.c_int(len(vc)), C.c_int(w), C.c_int(h), C.c_float(cam.fx),
                            C.c_float(cam.fy), C.c_float(cam.cx), C.c_float(cam.cy), p(m), C.c_float(max_depth),
                            C.c_float(now), C.c_float(conf), C.c_float(tthr), p(idx), p(rgbd))
@@ -82,7 +82,8 @@ def _run_host(lib, vc, nr, ct, cam, w2c, max_depth, now, conf, tthr):
 @pytest.mark.parametrize("kind", ["torus", "cloud"])
 def test_kernel_arithmetic_matches_the_oracle_on_the_host(orc, small_scene, tmp_path, kind):
     """The kernel's per-surfel arithmetic, built for the host, equals the oracle's restatement of
-    the shader bit for bit (index and rgbd maps), with and without the recent-observation pass."""
+    the shader bit for bit (index and rgbd maps), with and without the recent-observation pass and
+    without colour and time."""
     lib = _host_build(tmp_path)
     args = _inputs(kind, small_scene)
     for tthr in (3.0, -1.0):
@@ -92,13 +93,19 @@ def test_kernel_arithmetic_matches_the_oracle_on_the_host(orc, small_scene, tmp_
         np.testing.assert_array_equal(hi, oi)
         np.testing.assert_array_equal(hr.view(np.uint32), orgbd.view(np.uint32))
         assert 100 < (oi != 0xFFFFFFFF).sum() < oi.size
+    # without colour and time: every surfel observed now, colour bytes zero
+    a = (args[0], args[1], None) + args[3:]
+    hi, hr = _run_host(lib, np.ascontiguousarray(a[0]), np.ascontiguousarray(a[1]), None, *a[3:])
+    oi, orgbd = orc.render_observation_maps(*a)
+    np.testing.assert_array_equal(hi, oi)
+    np.testing.assert_array_equal(hr.view(np.uint32), orgbd.view(np.uint32))
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["torus", "cloud"])
 def test_observation_maps_match_the_oracle(ws, orc, small_scene, kind):
     """ws_render_observation_maps against the oracle's restatement, bit for bit, with and without
-    the recent-observation pass, twice in a row on the same inputs."""
+    the recent-observation pass, twice in a row on the same inputs, and without colour and time."""
     from starhub_b200.solver import GpuGeometry
     geo = GpuGeometry()
     args = _inputs(kind, small_scene)
@@ -108,3 +115,8 @@ def test_observation_maps_match_the_oracle(ws, orc, small_scene, kind):
         oi, orgbd = orc.render_observation_maps(*a)
         np.testing.assert_array_equal(gi, oi)
         np.testing.assert_array_equal(gr.view(np.uint32), orgbd.view(np.uint32))
+    a = (args[0], args[1], None) + args[3:]   # without colour and time
+    gi, gr = geo.render_observation_maps(*a)
+    oi, orgbd = orc.render_observation_maps(*a)
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(gr.view(np.uint32), orgbd.view(np.uint32))
