@@ -660,19 +660,6 @@ __device__ __forceinline__ float pick6(const float *v, int i) {
     return r;
 }
 
-__device__ __forceinline__ void accumulate_pair_row(float *A, const float *ur, const float *uc, float si, float sj) {
-    float a[6], c[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        a[q] = si * ur[q];
-        c[q] = sj * uc[q];
-    }
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = 0; j < 6; ++j) A[6 * i + j] += a[i] * c[j];
-}
-
 template <int NT, int C>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_assemble_pair(
     const Scene *scenes, const Plan *plan, const uint32_t *counts,
